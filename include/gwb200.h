@@ -1,0 +1,144 @@
+/*
+ * gwb200.h -- C ABI of the B200-native G0W0 screening / self-energy backend.
+ *
+ * One library (libgwb200.so) with plain pointers and sizes.  Host buffers are
+ * borrowed for the duration of a call; device memory belongs to the handle.
+ * One host thread per handle.  No exception crosses this boundary: every entry
+ * point returns a gwb200_status and gwb200_last_error() gives a thread-local
+ * message.  There is no CPU fallback: when the CUDA device or the sm_100a code
+ * is unavailable the calls fail with GWB200_CUDA_ERROR.
+ *
+ * Layout contract (the reference's, include/types.hpp:15-192): every matrix is
+ * row-major (C order); complex numbers are interleaved (re, im) doubles, i.e.
+ * std::complex<double> / double _Complex; eri is eri_mo[p,q,r,s] in C order
+ * (include/gw/integrals.hpp:28-32); states are 0-based MO indices.
+ *
+ * Each declaration names the reference interface it replaces (file:line in
+ * scnlong/miniGW).
+ */
+#ifndef GWB200_H
+#define GWB200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum gwb200_status {
+    GWB200_OK = 0,
+    GWB200_BAD_SHAPE = 1,        /* nmo/nocc/nfreq/state out of range (reference: std::runtime_error) */
+    GWB200_ETA_NONZERO = 2,      /* eta != 0: eps(iw) is not SPD; this backend requires eta == 0 */
+    GWB200_NOT_SPD = 3,          /* Cholesky pivot <= 0; gwb200_stats.info = 1-based pivot row */
+    GWB200_OOM = 4,              /* device allocation failed */
+    GWB200_DEVICE_TIMEOUT = 5,   /* a bounded device wait gave up */
+    GWB200_CUDA_ERROR = 6,       /* CUDA runtime error, or no usable sm_100 device */
+    GWB200_BAD_ARGUMENT = 7,     /* null pointer, unknown precision, bad handle */
+    GWB200_NO_SYSTEM = 8,        /* sigma/qp requested before gwb200_load_system */
+    GWB200_IO_ERROR = 9,         /* gw_input.h5 missing, malformed or unsupported */
+    GWB200_NONPOSITIVE_GAP = 10  /* some e_a - e_i <= 0: chi0(iw) is not negative definite */
+} gwb200_status;
+
+typedef enum gwb200_precision {
+    GWB200_FP64 = 0,             /* plain form: FP64 throughout (the drop-in) */
+    GWB200_MIXED = 1             /* mixed form (FP32 factor + FP64 correction) */
+} gwb200_precision;
+
+typedef struct gwb200_stats {
+    double device_ms_total;      /* CUDA-event time of the whole call */
+    double device_ms_gather;     /* V_ph / panel gathers */
+    double device_ms_screening;  /* eps build + Cholesky + panel solve (all frequency chunks) */
+    double device_ms_contract;   /* G0-weighted frequency contraction */
+    double flops_screening;      /* algorithmic flops n^3/3 + n^2 m + 3 n m per frequency, summed */
+    int64_t frequency_chunks;    /* frequency chunks the screening was split into (HBM budget) */
+    int64_t kernel_launches;     /* kernels this call launched */
+    int64_t info;                /* NOT_SPD: 1-based failing pivot; else 0 */
+    int64_t nph;                 /* n = nocc * nvir */
+    int64_t ncols;               /* m = nstates * nmo */
+} gwb200_stats;
+
+typedef struct gwb200_handle gwb200_handle;
+
+/* Thread-local description of the last failure on this thread ("" if none). */
+const char* gwb200_last_error(void);
+
+/* Library / build information, e.g. "gwb200 sm_100a fp64-dmma". */
+const char* gwb200_version(void);
+
+/* Create a handle bound to CUDA device `device` (it owns a stream and device buffers).
+ * Replaces: gw::workspace::DeviceScreeningWorkspace construction and the device
+ * selection gw::linalg::set_cuda_device_for_local_rank
+ * (include/workspace/device_screening_workspace.hpp:27-59, src/linalg/linalg_cublas.cu:393-405). */
+int gwb200_create(int device, gwb200_handle** out);
+
+/* Release every device buffer of the handle.  Safe on NULL. */
+int gwb200_destroy(gwb200_handle* h);
+
+/* Upload one molecular system and build its resident device state: the occupied-virtual
+ * index map, the V_ph=(jb|ia) gather and the exchange diagonal.  eri (nmo^4), mo_energy
+ * (nmo) and vxc (nmo^2) are borrowed for the call.
+ * Replaces: gw::OrbitalSpace / gw::ParticleHoleBasis (include/gw/orbital_space.hpp:10-70,
+ * include/gw/particle_hole.hpp:18-59), gw::calculate_v_ph_matrix (src/gw/sigma.cpp:56-71),
+ * gw::workspace::DeviceScreeningWorkspace(v_ph) (src/workspace/device_screening_workspace.cu:288-310)
+ * and gw::workspace::DevicePqPhPanelView (src/workspace/device_pq_ph_panel.cu:168-237). */
+int gwb200_load_system(gwb200_handle* h, int64_t nmo, int64_t nocc, const double* mo_energy,
+                       const double* eri, const double* vxc, double fermi_energy);
+
+/* Correlation self-energy Sigma_c(i w_n) on the imaginary grid for the requested states.
+ * sigma_out is nmo x nfreq complex, row-major (gw::MatrixComplex); rows of states not
+ * requested are set to zero.  eta must be 0 (GWB200_ETA_NONZERO otherwise).
+ * Replaces: gw::compute_sigma_c_with_backend (src/gw/sigma_c_driver.cpp:451-592) with the
+ * device branch (:471-514): compute_w_c (src/workspace/device_screening_workspace.cu:337-374),
+ * fill_panel (src/workspace/device_pq_ph_panel.cu:284), quadratic_forms_panel (:376-417) and the
+ * Sigma accumulation (src/gw/sigma_c_driver.cpp:186-222). */
+int gwb200_sigma_c(gwb200_handle* h, const double* omega, const double* weight, int64_t nfreq,
+                   const int64_t* states, int64_t nstates, double eta, int precision,
+                   double* sigma_out, gwb200_stats* stats);
+
+/* Screened quadratic forms Q[f, s, k] = x_{p_s k}^T W_c(i w_f) x_{p_s k} (real, <= 0), layout
+ * [nfreq][nstates][nmo].  The per-frequency quantity the reference computes as
+ * quadratic_forms_panel (src/workspace/screening_workspace.cpp:69-102); exported for checking. */
+int gwb200_screened_forms(gwb200_handle* h, const double* omega, int64_t nfreq, const int64_t* states,
+                          int64_t nstates, double eta, int precision, double* q_out, gwb200_stats* stats);
+
+/* Diagonal of the exchange self-energy, Sigma_x[p,p] = -sum_{i<nocc} (p i | p i), out[nmo].
+ * Replaces: gw::calculate_exchange (src/gw/sigma.cpp:22-39) (only its diagonal is consumed,
+ * src/gw/qp_solver.cpp:36 and src/io.cpp:110-126). */
+int gwb200_sigma_x_diag(gwb200_handle* h, double* out);
+
+/* Quasiparticle energies by Pade continuation of Sigma_c and the fixed-point update, on the
+ * device in FP64.  sigma is nmo x nfreq complex (as returned by gwb200_sigma_c), qp_out[nmo]
+ * is NaN for states not requested.
+ * Replaces: gw::solve_qp_energies (src/gw/qp_solver.cpp:10-47) with
+ * get_pade_coefficients_continued_fraction / evaluate_pade_continued_fraction (src/gw/pade.cpp:10-101). */
+int gwb200_qp(gwb200_handle* h, const double* omega, int64_t nfreq, const double* sigma, int64_t npade,
+              const int64_t* states, int64_t nstates, double* qp_out);
+
+/* Pade continuation of one state's Sigma_c(iw) (sigma_row: nfreq complex) evaluated on the real
+ * axis at e_i = x_start + i*interval - fermi, i < npts; out is npts x 3: (e_i+fermi)*Ha->eV, Re, Im.
+ * Replaces: gw::output_self_energy_after_pade's sweep (src/io.cpp:94-108). */
+int gwb200_pade_sweep(gwb200_handle* h, const double* omega, int64_t nfreq, const double* sigma_row,
+                      int64_t npade, int64_t npts, double fermi, double x_start, double interval,
+                      double* out);
+
+/* Transformed Gauss-Legendre grid (host, FP64, same arithmetic as the reference).
+ * Replaces: gw::generate_transformed_legendre_grid (src/gw/frequency_grids.cpp:62-93). */
+int gwb200_grid(int64_t nfreq, double* omega, double* weight);
+
+/* Minimal reader for gw_input.h5 (HDF5 superblock v0/v1, v1 object headers, symbol-table groups,
+ * contiguous or compact float64 datasets, scalar attributes).  Call with eri/mo/vxc NULL to query
+ * nmo, nocc and fermi; then with buffers of nmo^4, nmo and nmo^2 doubles.
+ * Replaces: gw::read_gw_input_hdf5 (src/hdf5_input.cpp:192-212). */
+int gwb200_read_input_h5(const char* path, int64_t* nmo, int64_t* nocc, double* fermi_energy,
+                         double* mo_energy, double* eri, double* vxc);
+
+/* Measured FP64 tensor (DMMA) throughput of this device in TFLOP/s, from a short
+ * microbenchmark of mma.sync f64 (used as the roofline denominator of the plain form). */
+int gwb200_fp64_peak_tflops(gwb200_handle* h, double* tflops);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* GWB200_H */

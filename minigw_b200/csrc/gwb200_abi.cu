@@ -1,0 +1,416 @@
+// gwb200_abi.cu -- the C ABI (include/gwb200.h): handle, resident device state, frequency
+// chunking by HBM budget, and the orchestration of the screening kernels.
+#include "internal.cuh"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <limits>
+#include <new>
+#include <string>
+#include <vector>
+
+using namespace gwb200;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+// Grow-only device buffer.
+struct DevBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+    void ensure(size_t want) {
+        if (want <= bytes) return;
+        release();
+        GWB_CUDA(cudaMalloc(&p, want));
+        bytes = want;
+    }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        bytes = 0;
+    }
+    template <class T>
+    T* as() const {
+        return static_cast<T*>(p);
+    }
+};
+
+template <class F>
+int guarded(F&& body) {
+    try {
+        body();
+        g_last_error.clear();
+        return GWB200_OK;
+    } catch (const Failure& e) {
+        g_last_error = e.what();
+        return e.code;
+    } catch (const std::bad_alloc&) {
+        g_last_error = "host allocation failed";
+        return GWB200_OOM;
+    } catch (const std::exception& e) {
+        g_last_error = e.what();
+        return GWB200_CUDA_ERROR;
+    }
+}
+
+} // namespace
+
+struct gwb200_handle {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev[6] = {};
+    // resident system
+    bool loaded = false;
+    int64_t nmo = 0, nocc = 0, n = 0;
+    double fermi = 0.0;
+    bool bad_gap = false;
+    DevBuf eri, mo, vxc_diag, delta, v, sigx, flag;
+    // per-call workspaces (grow-only, reused across calls)
+    DevBuf xt, dvec, a, linv, qacc, qall, sigma, omega, weight, states, err, qp;
+};
+
+namespace {
+
+void check_handle(gwb200_handle* h) {
+    if (!h) fail(GWB200_BAD_ARGUMENT, "null gwb200_handle");
+    GWB_CUDA(cudaSetDevice(h->device));
+}
+
+void check_system(gwb200_handle* h) {
+    check_handle(h);
+    if (!h->loaded) fail(GWB200_NO_SYSTEM, "no system loaded: call gwb200_load_system first");
+}
+
+void check_states(const gwb200_handle* h, const int64_t* states, int64_t nstates) {
+    if (nstates <= 0 || !states) fail(GWB200_BAD_SHAPE, "at least one state is required");
+    std::vector<int64_t> seen(states, states + nstates);
+    for (int64_t s : seen)
+        if (s < 0 || s >= h->nmo) fail(GWB200_BAD_SHAPE, "Selected state is out of range");
+    std::sort(seen.begin(), seen.end());
+    if (std::adjacent_find(seen.begin(), seen.end()) != seen.end()) fail(GWB200_BAD_SHAPE, "duplicate state in the state list");
+}
+
+float elapsed(cudaEvent_t a, cudaEvent_t b) {
+    float ms = 0.f;
+    GWB_CUDA(cudaEventElapsedTime(&ms, a, b));
+    return ms;
+}
+
+// Screened quadratic forms for all requested frequencies into h->qall ([nfreq][m] doubles,
+// x^T W_c x <= 0).  Records ev[0] (start), ev[1] (after gather), ev[2] (after screening).
+void compute_forms(gwb200_handle* h, const double* omega, int64_t nfreq, const int64_t* states, int64_t nstates,
+                   double eta, int precision, gwb200_stats* st) {
+    if (!omega) fail(GWB200_BAD_ARGUMENT, "null omega");
+    if (nfreq <= 0) fail(GWB200_BAD_SHAPE, "--freq-points must be positive");
+    check_states(h, states, nstates);
+    if (eta != 0.0)
+        fail(GWB200_ETA_NONZERO, "the b200 backend factors the SPD form of eps(iw) and requires eta == 0");
+    if (precision != GWB200_FP64 && precision != GWB200_MIXED) fail(GWB200_BAD_ARGUMENT, "unknown precision");
+    if (precision == GWB200_MIXED) fail(GWB200_BAD_ARGUMENT, "the mixed-precision form is not built in this library");
+    if (h->bad_gap)
+        fail(GWB200_NONPOSITIVE_GAP, "some e_a - e_i <= 0: chi0(iw) is not negative definite, eps(iw) is not SPD");
+    for (int64_t f = 0; f < nfreq; ++f)
+        if (!(std::isfinite(omega[f]))) fail(GWB200_BAD_ARGUMENT, "non-finite frequency");
+
+    cudaStream_t s = h->stream;
+    const int64_t m = nstates * h->nmo;
+    const TallGeometry g = make_geometry(h->n, m);
+    int64_t launches = 0;
+
+    h->omega.ensure(sizeof(double) * nfreq);
+    h->states.ensure(sizeof(int64_t) * nstates);
+    h->xt.ensure(sizeof(double) * (size_t)m * h->n);
+    h->qall.ensure(sizeof(double) * (size_t)nfreq * g.m_pad);
+    h->err.ensure(sizeof(unsigned long long));
+    GWB_CUDA(cudaMemcpyAsync(h->omega.p, omega, sizeof(double) * nfreq, cudaMemcpyHostToDevice, s));
+    GWB_CUDA(cudaMemcpyAsync(h->states.p, states, sizeof(int64_t) * nstates, cudaMemcpyHostToDevice, s));
+    GWB_CUDA(cudaMemsetAsync(h->err.p, 0xFF, sizeof(unsigned long long), s));
+
+    // Frequency chunk size from the HBM budget: tall matrices + scale vectors + 64x64 inverses.
+    const size_t per_freq = sizeof(double) * ((size_t)g.stride + g.n_pad + kNb * kNb + g.m_pad);
+    size_t free_b = 0, total_b = 0;
+    GWB_CUDA(cudaMemGetInfo(&free_b, &total_b));
+    const size_t have = h->a.bytes + h->dvec.bytes + h->linv.bytes + h->qacc.bytes;
+    const size_t budget = (size_t)((double)(free_b + have) * 0.85);
+    int64_t fc = (int64_t)std::min<size_t>((size_t)nfreq, std::max<size_t>(1, budget / per_freq));
+    if ((size_t)fc * per_freq > free_b + have) fail(GWB200_OOM, "not enough device memory for one frequency of eps(iw)");
+    h->a.ensure(sizeof(double) * (size_t)fc * g.stride);
+    h->dvec.ensure(sizeof(double) * (size_t)fc * g.n_pad);
+    h->linv.ensure(sizeof(double) * (size_t)fc * kNb * kNb);
+    h->qacc.ensure(sizeof(double) * (size_t)fc * g.m_pad);
+
+    GWB_CUDA(cudaEventRecord(h->ev[0], s));
+    launches += launch_gather_panel(h->eri.as<double>(), h->nmo, h->nocc, h->states.as<int64_t>(), nstates,
+                                    h->xt.as<double>(), s);
+    GWB_CUDA(cudaEventRecord(h->ev[1], s));
+    int64_t chunks = 0;
+    for (int64_t f0 = 0; f0 < nfreq; f0 += fc) {
+        const int64_t nf = std::min(fc, nfreq - f0);
+        launches += launch_scale_vectors(h->delta.as<double>(), g.n, g.n_pad, h->omega.as<double>() + f0, nf,
+                                         h->dvec.as<double>(), s);
+        launches += launch_build_tall(g, h->v.as<double>(), h->xt.as<double>(), h->dvec.as<double>(), nf,
+                                      h->a.as<double>(), s);
+        GWB_CUDA(cudaMemsetAsync(h->qacc.p, 0, sizeof(double) * (size_t)nf * g.m_pad, s));
+        for (int64_t k = 0; k < g.n_pad; k += kNb)
+            launches += launch_cholesky_step(g, k, nf, h->a.as<double>(), h->linv.as<double>(), h->qacc.as<double>(),
+                                             h->err.as<unsigned long long>(), s);
+        launches += launch_negate_copy(h->qacc.as<double>(), nf, m, g.m_pad, h->qall.as<double>() + f0 * g.m_pad,
+                                       g.m_pad, s);
+        ++chunks;
+    }
+    GWB_CUDA(cudaEventRecord(h->ev[2], s));
+    if (st) {
+        const double nd = (double)g.n, md = (double)m;
+        st->flops_screening = (double)nfreq * (nd * nd * nd / 3.0 + nd * nd * md + 3.0 * nd * md);
+        st->frequency_chunks = chunks;
+        st->kernel_launches = launches;
+        st->nph = g.n;
+        st->ncols = m;
+    }
+}
+
+void finish_forms(gwb200_handle* h, gwb200_stats* st) {
+    unsigned long long piv = 0;
+    GWB_CUDA(cudaMemcpyAsync(&piv, h->err.p, sizeof(piv), cudaMemcpyDeviceToHost, h->stream));
+    GWB_CUDA(cudaStreamSynchronize(h->stream));
+    if (piv != std::numeric_limits<unsigned long long>::max()) {
+        if (st) st->info = (int64_t)piv;
+        fail(GWB200_NOT_SPD, "eps(iw) is not positive definite: Cholesky pivot " + std::to_string(piv) + " <= 0");
+    }
+    if (st) {
+        st->device_ms_gather = elapsed(h->ev[0], h->ev[1]);
+        st->device_ms_screening = elapsed(h->ev[1], h->ev[2]);
+    }
+}
+
+} // namespace
+
+extern "C" {
+
+const char* gwb200_last_error(void) { return g_last_error.c_str(); }
+
+const char* gwb200_version(void) { return "gwb200 1.0 sm_100a fp64-dmma"; }
+
+int gwb200_create(int device, gwb200_handle** out) {
+    return guarded([&] {
+        if (!out) fail(GWB200_BAD_ARGUMENT, "null output handle pointer");
+        *out = nullptr;
+        int count = 0;
+        const cudaError_t e = cudaGetDeviceCount(&count);
+        if (e != cudaSuccess || count == 0)
+            fail(GWB200_CUDA_ERROR, std::string("no CUDA device available: ") + cudaGetErrorString(e));
+        if (device < 0 || device >= count) fail(GWB200_BAD_ARGUMENT, "device index out of range");
+        int major = 0;
+        GWB_CUDA(cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, device));
+        if (major != 10) fail(GWB200_CUDA_ERROR, "libgwb200 is built for sm_100a (B200); device has compute capability " +
+                                                    std::to_string(major) + ".x");
+        GWB_CUDA(cudaSetDevice(device));
+        auto* h = new gwb200_handle();
+        h->device = device;
+        try {
+            GWB_CUDA(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+            for (auto& e2 : h->ev) GWB_CUDA(cudaEventCreate(&e2));
+        } catch (...) {
+            gwb200_destroy(h);
+            throw;
+        }
+        *out = h;
+    });
+}
+
+int gwb200_destroy(gwb200_handle* h) {
+    if (!h) return GWB200_OK;
+    cudaSetDevice(h->device);
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    for (DevBuf* b : {&h->eri, &h->mo, &h->vxc_diag, &h->delta, &h->v, &h->sigx, &h->flag, &h->xt, &h->dvec, &h->a,
+                      &h->linv, &h->qacc, &h->qall, &h->sigma, &h->omega, &h->weight, &h->states, &h->err, &h->qp})
+        b->release();
+    for (auto& e : h->ev)
+        if (e) cudaEventDestroy(e);
+    if (h->stream) cudaStreamDestroy(h->stream);
+    delete h;
+    return GWB200_OK;
+}
+
+int gwb200_load_system(gwb200_handle* h, int64_t nmo, int64_t nocc, const double* mo_energy, const double* eri,
+                       const double* vxc, double fermi_energy) {
+    return guarded([&] {
+        check_handle(h);
+        if (!mo_energy || !eri || !vxc) fail(GWB200_BAD_ARGUMENT, "null input array");
+        if (nmo <= 0) fail(GWB200_BAD_SHAPE, "OrbitalSpace: empty MO energy vector");
+        if (nocc <= 0 || nocc >= nmo) fail(GWB200_BAD_SHAPE, "OrbitalSpace: invalid number of occupied orbitals");
+        if (nmo > 1024) fail(GWB200_BAD_SHAPE, "nmo > 1024 is not supported");
+        cudaStream_t s = h->stream;
+        h->loaded = false;
+        const size_t n4 = (size_t)nmo * nmo * nmo * nmo;
+        const int64_t n = nocc * (nmo - nocc);
+        h->eri.ensure(sizeof(double) * n4);
+        h->mo.ensure(sizeof(double) * nmo);
+        h->vxc_diag.ensure(sizeof(double) * nmo);
+        h->sigx.ensure(sizeof(double) * nmo);
+        h->delta.ensure(sizeof(double) * n);
+        h->v.ensure(sizeof(double) * (size_t)n * n);
+        h->flag.ensure(sizeof(int));
+        std::vector<double> vd((size_t)nmo);
+        for (int64_t p = 0; p < nmo; ++p) vd[(size_t)p] = vxc[p * nmo + p];
+        GWB_CUDA(cudaMemcpyAsync(h->eri.p, eri, sizeof(double) * n4, cudaMemcpyHostToDevice, s));
+        GWB_CUDA(cudaMemcpyAsync(h->mo.p, mo_energy, sizeof(double) * nmo, cudaMemcpyHostToDevice, s));
+        GWB_CUDA(cudaMemcpyAsync(h->vxc_diag.p, vd.data(), sizeof(double) * nmo, cudaMemcpyHostToDevice, s));
+        GWB_CUDA(cudaMemsetAsync(h->flag.p, 0, sizeof(int), s));
+        launch_delta(h->mo.as<double>(), nmo, nocc, h->delta.as<double>(), h->flag.as<int>(), s);
+        launch_gather_vph(h->eri.as<double>(), nmo, nocc, h->v.as<double>(), s);
+        launch_sigma_x_diag(h->eri.as<double>(), nmo, nocc, h->sigx.as<double>(), s);
+        int bad = 0;
+        GWB_CUDA(cudaMemcpyAsync(&bad, h->flag.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+        GWB_CUDA(cudaStreamSynchronize(s));
+        h->nmo = nmo;
+        h->nocc = nocc;
+        h->n = n;
+        h->fermi = fermi_energy;
+        h->bad_gap = bad != 0;
+        h->loaded = true;
+    });
+}
+
+int gwb200_screened_forms(gwb200_handle* h, const double* omega, int64_t nfreq, const int64_t* states,
+                          int64_t nstates, double eta, int precision, double* q_out, gwb200_stats* stats) {
+    return guarded([&] {
+        check_system(h);
+        if (!q_out) fail(GWB200_BAD_ARGUMENT, "null output array");
+        gwb200_stats local{};
+        gwb200_stats* st = stats ? stats : &local;
+        *st = gwb200_stats{};
+        compute_forms(h, omega, nfreq, states, nstates, eta, precision, st);
+        finish_forms(h, st);
+        const int64_t m = nstates * h->nmo;
+        const int64_t ldq = make_geometry(h->n, m).m_pad;
+        GWB_CUDA(cudaMemcpy2DAsync(q_out, sizeof(double) * m, h->qall.p, sizeof(double) * ldq, sizeof(double) * m,
+                                   (size_t)nfreq, cudaMemcpyDeviceToHost, h->stream));
+        GWB_CUDA(cudaStreamSynchronize(h->stream));
+    });
+}
+
+int gwb200_sigma_c(gwb200_handle* h, const double* omega, const double* weight, int64_t nfreq, const int64_t* states,
+                   int64_t nstates, double eta, int precision, double* sigma_out, gwb200_stats* stats) {
+    return guarded([&] {
+        check_system(h);
+        if (!weight || !sigma_out) fail(GWB200_BAD_ARGUMENT, "null weight or output array");
+        gwb200_stats local{};
+        gwb200_stats* st = stats ? stats : &local;
+        *st = gwb200_stats{};
+        compute_forms(h, omega, nfreq, states, nstates, eta, precision, st);
+        cudaStream_t s = h->stream;
+        const int64_t m = nstates * h->nmo;
+        const int64_t ldq = make_geometry(h->n, m).m_pad;
+        const size_t sig_bytes = sizeof(double) * 2 * (size_t)h->nmo * nfreq;
+        h->weight.ensure(sizeof(double) * nfreq);
+        h->sigma.ensure(sig_bytes);
+        GWB_CUDA(cudaMemcpyAsync(h->weight.p, weight, sizeof(double) * nfreq, cudaMemcpyHostToDevice, s));
+        GWB_CUDA(cudaMemsetAsync(h->sigma.p, 0, sig_bytes, s));
+        st->kernel_launches += launch_sigma_contract(h->qall.as<double>(), nfreq, nstates, h->nmo, ldq,
+                                                     h->states.as<int64_t>(), h->mo.as<double>(), h->fermi,
+                                                     h->omega.as<double>(), h->weight.as<double>(),
+                                                     h->sigma.as<double>(), s);
+        GWB_CUDA(cudaEventRecord(h->ev[3], s));
+        finish_forms(h, st);
+        st->device_ms_contract = elapsed(h->ev[2], h->ev[3]);
+        st->device_ms_total = elapsed(h->ev[0], h->ev[3]);
+        GWB_CUDA(cudaMemcpyAsync(sigma_out, h->sigma.p, sig_bytes, cudaMemcpyDeviceToHost, s));
+        GWB_CUDA(cudaStreamSynchronize(s));
+    });
+}
+
+int gwb200_sigma_x_diag(gwb200_handle* h, double* out) {
+    return guarded([&] {
+        check_system(h);
+        if (!out) fail(GWB200_BAD_ARGUMENT, "null output array");
+        GWB_CUDA(cudaMemcpyAsync(out, h->sigx.p, sizeof(double) * h->nmo, cudaMemcpyDeviceToHost, h->stream));
+        GWB_CUDA(cudaStreamSynchronize(h->stream));
+    });
+}
+
+int gwb200_qp(gwb200_handle* h, const double* omega, int64_t nfreq, const double* sigma, int64_t npade,
+              const int64_t* states, int64_t nstates, double* qp_out) {
+    return guarded([&] {
+        check_system(h);
+        if (!omega || !sigma || !qp_out) fail(GWB200_BAD_ARGUMENT, "null input or output array");
+        if (nfreq <= 0) fail(GWB200_BAD_SHAPE, "nfreq must be positive");
+        if (npade <= 0) fail(GWB200_BAD_SHAPE, "Pade: npar must be positive");
+        check_states(h, states, nstates);
+        cudaStream_t s = h->stream;
+        const size_t sig_bytes = sizeof(double) * 2 * (size_t)h->nmo * nfreq;
+        h->omega.ensure(sizeof(double) * nfreq);
+        h->sigma.ensure(sig_bytes);
+        h->states.ensure(sizeof(int64_t) * nstates);
+        h->qp.ensure(sizeof(double) * h->nmo);
+        std::vector<double> nan((size_t)h->nmo, std::numeric_limits<double>::quiet_NaN());
+        GWB_CUDA(cudaMemcpyAsync(h->omega.p, omega, sizeof(double) * nfreq, cudaMemcpyHostToDevice, s));
+        GWB_CUDA(cudaMemcpyAsync(h->sigma.p, sigma, sig_bytes, cudaMemcpyHostToDevice, s));
+        GWB_CUDA(cudaMemcpyAsync(h->states.p, states, sizeof(int64_t) * nstates, cudaMemcpyHostToDevice, s));
+        GWB_CUDA(cudaMemcpyAsync(h->qp.p, nan.data(), sizeof(double) * h->nmo, cudaMemcpyHostToDevice, s));
+        launch_qp(h->sigma.as<double>(), h->omega.as<double>(), nfreq, h->nmo, h->states.as<int64_t>(), nstates,
+                  npade, h->mo.as<double>(), h->fermi, h->sigx.as<double>(), h->vxc_diag.as<double>(),
+                  h->qp.as<double>(), s);
+        GWB_CUDA(cudaMemcpyAsync(qp_out, h->qp.p, sizeof(double) * h->nmo, cudaMemcpyDeviceToHost, s));
+        GWB_CUDA(cudaStreamSynchronize(s));
+    });
+}
+
+int gwb200_pade_sweep(gwb200_handle* h, const double* omega, int64_t nfreq, const double* sigma_row, int64_t npade,
+                      int64_t npts, double fermi, double x_start, double interval, double* out) {
+    return guarded([&] {
+        check_handle(h);
+        if (!omega || !sigma_row || !out) fail(GWB200_BAD_ARGUMENT, "null input or output array");
+        if (nfreq <= 0 || npts <= 0) fail(GWB200_BAD_SHAPE, "nfreq and npts must be positive");
+        if (npade <= 0) fail(GWB200_BAD_SHAPE, "Pade: npar must be positive");
+        cudaStream_t s = h->stream;
+        DevBuf dom, drow, dout;
+        try {
+            dom.ensure(sizeof(double) * nfreq);
+            drow.ensure(sizeof(double) * 2 * nfreq);
+            dout.ensure(sizeof(double) * 3 * (size_t)npts);
+            GWB_CUDA(cudaMemcpyAsync(dom.p, omega, sizeof(double) * nfreq, cudaMemcpyHostToDevice, s));
+            GWB_CUDA(cudaMemcpyAsync(drow.p, sigma_row, sizeof(double) * 2 * nfreq, cudaMemcpyHostToDevice, s));
+            launch_pade_sweep(drow.as<double>(), dom.as<double>(), nfreq, npade, npts, fermi, x_start, interval,
+                              dout.as<double>(), s);
+            GWB_CUDA(cudaMemcpyAsync(out, dout.p, sizeof(double) * 3 * (size_t)npts, cudaMemcpyDeviceToHost, s));
+            GWB_CUDA(cudaStreamSynchronize(s));
+        } catch (...) {
+            cudaStreamSynchronize(s);
+            dom.release();
+            drow.release();
+            dout.release();
+            throw;
+        }
+        dom.release();
+        drow.release();
+        dout.release();
+    });
+}
+
+int gwb200_grid(int64_t nfreq, double* omega, double* weight) {
+    return guarded([&] {
+        if (!omega || !weight) fail(GWB200_BAD_ARGUMENT, "null output array");
+        transformed_legendre_grid(nfreq, omega, weight);
+    });
+}
+
+int gwb200_read_input_h5(const char* path, int64_t* nmo, int64_t* nocc, double* fermi_energy, double* mo_energy,
+                         double* eri, double* vxc) {
+    return guarded([&] {
+        if (!path || !nmo || !nocc || !fermi_energy) fail(GWB200_BAD_ARGUMENT, "null argument");
+        read_gw_input_h5(path, nmo, nocc, fermi_energy, mo_energy, eri, vxc);
+    });
+}
+
+int gwb200_fp64_peak_tflops(gwb200_handle* h, double* tflops) {
+    return guarded([&] {
+        check_handle(h);
+        if (!tflops) fail(GWB200_BAD_ARGUMENT, "null output");
+        *tflops = measure_fp64_peak_tflops(h->stream);
+    });
+}
+
+} // extern "C"

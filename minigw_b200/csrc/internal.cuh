@@ -1,0 +1,95 @@
+// internal.cuh -- shared declarations of libgwb200 (not part of the C ABI).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <stdexcept>
+#include <string>
+
+#include "../../include/gwb200.h"
+
+namespace gwb200 {
+
+// Error carrying a gwb200_status across the host code; converted to a return code
+// at the C-ABI boundary.
+struct Failure : std::runtime_error {
+    int code;
+    Failure(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+[[noreturn]] inline void fail(int code, const std::string& msg) { throw Failure(code, msg); }
+
+inline void cuda_check(cudaError_t e, const char* what, const char* file, int line) {
+    if (e != cudaSuccess) {
+        const int code = (e == cudaErrorMemoryAllocation) ? GWB200_OOM : GWB200_CUDA_ERROR;
+        fail(code, std::string(what) + ": " + cudaGetErrorString(e) + " (" + file + ":" + std::to_string(line) + ")");
+    }
+}
+#define GWB_CUDA(x) ::gwb200::cuda_check((x), #x, __FILE__, __LINE__)
+#define GWB_LAUNCH(what) ::gwb200::cuda_check(cudaGetLastError(), what, __FILE__, __LINE__)
+
+// Block size of the right-looking Cholesky (rows/cols of one diagonal block) and
+// the square tile edge of every DMMA tile kernel.
+constexpr int kNb = 64;
+// Padded shared-memory row stride (doubles) of a 64-wide tile: 68*8 B rows put the
+// 8 rows touched by one m8n8k4 fragment load on distinct banks.
+constexpr int kLds = 68;
+
+// Geometry of one frequency chunk of the tall screening matrices
+//   A_f = [ eps_f (n_pad x n_pad, lower) ; B_f^T (m_pad x n_pad) ],  row-major, ld = n_pad.
+struct TallGeometry {
+    int64_t n;      // nph
+    int64_t m;      // nstates * nmo (right-hand sides)
+    int64_t n_pad;  // n rounded up to kNb
+    int64_t m_pad;  // m rounded up to kNb
+    int64_t rows;   // n_pad + m_pad
+    int64_t ld;     // n_pad
+    int64_t stride; // rows * ld (elements per frequency)
+};
+
+inline int64_t round_up(int64_t x, int64_t r) { return (x + r - 1) / r * r; }
+
+inline TallGeometry make_geometry(int64_t n, int64_t m) {
+    TallGeometry g{};
+    g.n = n;
+    g.m = m;
+    g.n_pad = round_up(n, kNb);
+    g.m_pad = round_up(m, kNb);
+    g.rows = g.n_pad + g.m_pad;
+    g.ld = g.n_pad;
+    g.stride = g.rows * g.ld;
+    return g;
+}
+
+// ---- kernel launchers (kernels_fp64.cu, kernels_small.cu) ----
+int launch_gather_vph(const double* eri, int64_t nmo, int64_t nocc, double* v, cudaStream_t s);
+int launch_gather_panel(const double* eri, int64_t nmo, int64_t nocc, const int64_t* states, int64_t nstates,
+                        double* xt, cudaStream_t s);
+int launch_sigma_x_diag(const double* eri, int64_t nmo, int64_t nocc, double* out, cudaStream_t s);
+int launch_delta(const double* mo, int64_t nmo, int64_t nocc, double* delta, int* bad_gap, cudaStream_t s);
+int launch_scale_vectors(const double* delta, int64_t n, int64_t n_pad, const double* omega, int64_t nf,
+                         double* dvec, cudaStream_t s);
+int launch_build_tall(const TallGeometry& g, const double* v, const double* xt, const double* dvec, int64_t nf,
+                      double* a, cudaStream_t s);
+// One right-looking step at block column k for nf frequencies; returns launches issued.
+int launch_cholesky_step(const TallGeometry& g, int64_t k, int64_t nf, double* a, double* linv, double* qacc,
+                         unsigned long long* err_pivot, cudaStream_t s);
+int launch_sigma_contract(const double* qall, int64_t nfreq, int64_t nstates, int64_t nmo, int64_t ldq,
+                          const int64_t* states, const double* mo, double fermi, const double* omega,
+                          const double* weight, double* sigma, cudaStream_t s);
+int launch_qp(const double* sigma, const double* omega, int64_t nfreq, int64_t nmo, const int64_t* states,
+              int64_t nstates, int64_t npade, const double* mo, double fermi, const double* sigx,
+              const double* vxc_diag, double* qp, cudaStream_t s);
+int launch_pade_sweep(const double* sigma_row, const double* omega, int64_t nfreq, int64_t npade, int64_t npts,
+                      double fermi, double x_start, double interval, double* out, cudaStream_t s);
+int launch_negate_copy(const double* qacc, int64_t nf, int64_t m, int64_t ldq_in, double* q_out, int64_t ldq_out,
+                       cudaStream_t s);
+double measure_fp64_peak_tflops(cudaStream_t s);
+
+// ---- host helpers (host_grid.cpp, host_h5.cpp) ----
+void transformed_legendre_grid(int64_t n, double* omega, double* weight);
+void read_gw_input_h5(const std::string& path, int64_t* nmo, int64_t* nocc, double* fermi, double* mo, double* eri,
+                      double* vxc);
+
+} // namespace gwb200

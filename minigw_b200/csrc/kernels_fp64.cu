@@ -1,0 +1,416 @@
+// kernels_fp64.cu -- plain-form (FP64) screening kernels for sm_100a.
+//
+// Per frequency f the reference builds eps_left = I - diag(Pi0) V and forms
+// W_c = eps_left^{-1} diag(Pi0) with a complex LU (src/workspace/screening_workspace.cpp:21-66,
+// src/workspace/device_screening_workspace.cu:337-374), then evaluates x^T W_c x per panel
+// (src/workspace/screening_workspace.cpp:69-102).  At eta = 0, Pi0 = -D with
+// D = 4 delta / (w^2 + delta^2) > 0, and
+//     x^T W_c x = -|| L^{-1} D^1/2 x ||^2,   L L^T = eps = I + D^1/2 V D^1/2  (SPD, eigenvalues >= 1).
+// The kernels below factor the tall matrix [eps ; (D^1/2 X)^T] with one right-looking
+// blocked Cholesky: its lower rows become (L^{-1} D^1/2 X)^T, whose row norms are the
+// quadratic forms.  All arithmetic is FP64; the O(n^3) and O(n^2 m) work runs on FP64
+// tensor cores (mma.sync m8n8k4 f64, DMMA).
+#include "internal.cuh"
+
+#include <cmath>
+
+namespace gwb200 {
+namespace {
+
+// ---------------------------------------------------------------------------
+// Gathers (bit-exact copies).
+
+// V[jb, ia] = eri[j, b, i, a]  (src/gw/sigma.cpp:56-71), row-major n x n.
+// blockIdx.y strides over rows jb; threads over ia: for fixed (jb, i) the source run
+// eri[j,b,i,nocc:nmo] is contiguous, so loads coalesce in runs of nvir.
+__global__ void k_gather_vph(const double* __restrict__ eri, int nmo, int nocc, int n, double* __restrict__ v) {
+    const int nvir = nmo - nocc;
+    for (int jb = blockIdx.y; jb < n; jb += gridDim.y) {
+        const int j = jb / nvir, b = nocc + jb % nvir;
+        const size_t base = ((size_t)j * nmo + b) * (size_t)nmo * nmo;
+        for (int ia = blockIdx.x * blockDim.x + threadIdx.x; ia < n; ia += gridDim.x * blockDim.x) {
+            const int i = ia / nvir, a = nocc + ia % nvir;
+            v[(size_t)jb * n + ia] = eri[base + (size_t)i * nmo + a];
+        }
+    }
+}
+
+// Xt[s*nmo + k, ia] = eri[p_s, k, i, a]  (src/workspace/pq_ph_panel.cpp:25-47, transposed so
+// that every right-hand side is a contiguous row), row-major m x n.
+__global__ void k_gather_panel(const double* __restrict__ eri, int nmo, int nocc, int n,
+                               const int64_t* __restrict__ states, int m, double* __restrict__ xt) {
+    const int nvir = nmo - nocc;
+    for (int row = blockIdx.y; row < m; row += gridDim.y) {
+        const int s = row / nmo, k = row % nmo;
+        const size_t p = (size_t)states[s];
+        const size_t base = (p * nmo + k) * (size_t)nmo * nmo;
+        for (int ia = blockIdx.x * blockDim.x + threadIdx.x; ia < n; ia += gridDim.x * blockDim.x) {
+            const int i = ia / nvir, a = nocc + ia % nvir;
+            xt[(size_t)row * n + ia] = eri[base + (size_t)i * nmo + a];
+        }
+    }
+}
+
+// Sigma_x[p,p] = -sum_{i<nocc} eri[p,i,p,i] in the reference's order (src/gw/sigma.cpp:29-36).
+__global__ void k_sigma_x_diag(const double* __restrict__ eri, int nmo, int nocc, double* __restrict__ out) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= nmo) return;
+    double value = 0.0;
+    for (int i = 0; i < nocc; ++i) {
+        value = __dsub_rn(value, eri[(((size_t)p * nmo + i) * nmo + p) * nmo + i]);
+    }
+    out[p] = value;
+}
+
+// delta[ph] = e_a - e_i with ph = i*nvir + a_vir (include/gw/particle_hole.hpp:22-35).
+__global__ void k_delta(const double* __restrict__ mo, int nmo, int nocc, double* __restrict__ delta,
+                        int* __restrict__ bad_gap) {
+    const int nvir = nmo - nocc, n = nocc * nvir;
+    const int ph = blockIdx.x * blockDim.x + threadIdx.x;
+    if (ph >= n) return;
+    const int i = ph / nvir, a = nocc + ph % nvir;
+    const double d = __dsub_rn(mo[a], mo[i]);
+    delta[ph] = d;
+    if (!(d > 0.0)) atomicExch(bad_gap, 1);
+}
+
+// dvec[f, c] = sqrt(D_f[c]) with D = -Pi0(i w_f) = 4 delta / (w^2 + delta^2); zero padding.
+__global__ void k_scale_vectors(const double* __restrict__ delta, int n, int n_pad, const double* __restrict__ omega,
+                                int nf, double* __restrict__ dvec) {
+    const int f = blockIdx.y;
+    const double w = omega[f];
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n_pad; c += gridDim.x * blockDim.x) {
+        double val = 0.0;
+        if (c < n) {
+            const double d = delta[c];
+            val = sqrt(4.0 * d / (w * w + d * d));
+        }
+        dvec[(size_t)f * n_pad + c] = val;
+    }
+}
+
+// Build the tall matrices of nf frequencies.  Thread (r, c): rows r < n_pad hold the lower
+// triangle of eps (c <= r), rows r >= n_pad hold d_c * Xt[r - n_pad, c].  V and Xt are read
+// once per chunk; the loop over frequencies reuses the value from registers.
+__global__ void k_build_tall(int64_t n, int64_t m, int64_t n_pad, int64_t ld, int64_t stride,
+                             const double* __restrict__ v, const double* __restrict__ xt,
+                             const double* __restrict__ dvec, int nf, double* __restrict__ a) {
+    const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= n_pad) return;
+    const int64_t rows = n_pad + ((m + kNb - 1) / kNb) * kNb;
+    for (int64_t r = blockIdx.y; r < rows; r += gridDim.y) {
+    if (r < n_pad) {
+        if (c > r) continue;
+        const bool inside = (r < n) && (c < n);
+        const double vrc = inside ? v[r * n + c] : 0.0;
+        const double diag = (r == c) ? 1.0 : 0.0;
+        for (int f = 0; f < nf; ++f) {
+            const double* d = dvec + (size_t)f * n_pad;
+            a[(size_t)f * stride + r * ld + c] = fma(d[r] * vrc, d[c], diag);
+        }
+    } else {
+        const int64_t j = r - n_pad;
+        const double x = (j < m && c < n) ? xt[j * n + c] : 0.0;
+        for (int f = 0; f < nf; ++f) {
+            a[(size_t)f * stride + r * ld + c] = dvec[(size_t)f * n_pad + c] * x;
+        }
+    }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// DMMA 64x64x64 tile product:  acc += sgn * As(64x64) * Bs(64x64)^T, both in shared memory,
+// row-major with stride kLds.  8 warps; warp w owns rows 16*(w/2)..+15, cols 32*(w%2)..+31,
+// i.e. 2 x 4 fragments of the m8n8k4 f64 MMA.  Fragment layout (PTX ISA, mma.m8n8k4 .f64):
+// A: a = A[lane/4][lane%4]; B: b = B[lane%4][lane/4]; C: {C[lane/4][2*(lane%4)], +1}.
+__device__ __forceinline__ void dmma_8x8x4(double (&c)[2], double a, double b) {
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+                 : "+d"(c[0]), "+d"(c[1])
+                 : "d"(a), "d"(b));
+}
+
+__device__ __forceinline__ void tile_mma_64(const double* __restrict__ As, const double* __restrict__ Bs,
+                                            double (&acc)[2][4][2], double sgn) {
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int g = lane >> 2, t = lane & 3;
+    const int r0 = 16 * (w >> 1), c0 = 32 * (w & 1);
+#pragma unroll 4
+    for (int kk = 0; kk < kNb; kk += 4) {
+        double af[2], bf[4];
+#pragma unroll
+        for (int i = 0; i < 2; ++i) af[i] = sgn * As[(r0 + 8 * i + g) * kLds + kk + t];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) bf[j] = Bs[(c0 + 8 * j + g) * kLds + kk + t];
+#pragma unroll
+        for (int i = 0; i < 2; ++i)
+#pragma unroll
+            for (int j = 0; j < 4; ++j) dmma_8x8x4(acc[i][j], af[i], bf[j]);
+    }
+}
+
+// Copy a 64x64 tile (global row stride ld) into shared memory (stride kLds), 16-byte loads.
+__device__ __forceinline__ void load_tile_64(double* __restrict__ s, const double* __restrict__ gsrc, int64_t ld) {
+    for (int idx = threadIdx.x; idx < 64 * 32; idx += blockDim.x) {
+        const int r = idx >> 5, c2 = idx & 31;
+        const double2 v = *reinterpret_cast<const double2*>(gsrc + (size_t)r * ld + 2 * c2);
+        *reinterpret_cast<double2*>(s + r * kLds + 2 * c2) = v;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Step 1: factor the diagonal block A[k:k+64, k:k+64] of each frequency in shared memory,
+// write L back and its inverse to linv (64x64 row-major, zero above the diagonal).
+// A pivot that is not > 0 (or NaN) records the 1-based global pivot row in *err_pivot
+// (minimum over all frequencies) and is replaced by 1 so the factorisation stays finite.
+__global__ void __launch_bounds__(256) k_potrf_diag(double* __restrict__ a, int64_t ld, int64_t stride, int64_t k,
+                                                    double* __restrict__ linv, unsigned long long* err_pivot) {
+    extern __shared__ double smem[];
+    constexpr int L = kNb + 1;
+    double* T = smem;            // 64 x 65: the block, then L
+    double* Y = smem + kNb * L;  // 64 x 65: L^{-1}
+    double* A = a + (size_t)blockIdx.x * stride + k * ld + k;
+    const int tid = threadIdx.x;
+    for (int idx = tid; idx < kNb * kNb; idx += blockDim.x) {
+        const int i = idx / kNb, j = idx % kNb;
+        T[i * L + j] = (j <= i) ? A[(size_t)i * ld + j] : 0.0;
+    }
+    __syncthreads();
+    for (int j = 0; j < kNb; ++j) {
+        if (tid == 0) {
+            double piv = T[j * L + j];
+            if (!(piv > 0.0)) {
+                atomicMin(err_pivot, (unsigned long long)(k + j + 1));
+                piv = 1.0;
+            }
+            T[j * L + j] = sqrt(piv);
+        }
+        __syncthreads();
+        const double djj = T[j * L + j];
+        for (int i = j + 1 + tid; i < kNb; i += blockDim.x) T[i * L + j] /= djj;
+        __syncthreads();
+        const int rem = kNb - 1 - j;
+        for (int idx = tid; idx < rem * rem; idx += blockDim.x) {
+            const int i = j + 1 + idx / rem, l = j + 1 + idx % rem;
+            if (l <= i) T[i * L + l] -= T[i * L + j] * T[l * L + j];
+        }
+        __syncthreads();
+    }
+    for (int idx = tid; idx < kNb * kNb; idx += blockDim.x) {
+        const int i = idx / kNb, j = idx % kNb;
+        if (j <= i) A[(size_t)i * ld + j] = T[i * L + j];
+    }
+    // Inverse of the lower-triangular block by forward substitution, one column per thread.
+    if (tid < kNb) {
+        const int col = tid;
+        for (int i = 0; i < kNb; ++i) {
+            double y;
+            if (i < col) {
+                y = 0.0;
+            } else if (i == col) {
+                y = 1.0 / T[i * L + i];
+            } else {
+                double s = 0.0;
+                for (int l = col; l < i; ++l) s = fma(T[i * L + l], Y[l * L + col], s);
+                y = -s / T[i * L + i];
+            }
+            Y[i * L + col] = y;
+        }
+    }
+    __syncthreads();
+    double* out = linv + (size_t)blockIdx.x * kNb * kNb;
+    for (int idx = tid; idx < kNb * kNb; idx += blockDim.x) out[idx] = Y[(idx / kNb) * L + idx % kNb];
+}
+
+// Step 2: panel solve.  Rows [k+64, rows) of block column k: P = A[:, k:k+64] * Linv^T, in place.
+// Rows in the right-hand-side block also add their squared norms to qacc (one thread per row,
+// fixed order, so the accumulation is deterministic).
+__global__ void __launch_bounds__(256) k_trsm_panel(double* __restrict__ a, int64_t ld, int64_t stride, int64_t k,
+                                                    int64_t n_pad, int64_t rows, const double* __restrict__ linv,
+                                                    double* __restrict__ qacc, int64_t ldq) {
+    extern __shared__ double smem[];
+    double* Ps = smem;              // 64 x kLds
+    double* Ls = smem + 64 * kLds;  // 64 x kLds
+    const int f = blockIdx.y;
+    const int64_t r0 = k + kNb + (int64_t)blockIdx.x * kNb;
+    if (r0 >= rows) return;
+    double* A = a + (size_t)f * stride;
+    load_tile_64(Ps, A + r0 * ld + k, ld);
+    load_tile_64(Ls, linv + (size_t)f * kNb * kNb, kNb);
+    __syncthreads();
+    double acc[2][4][2] = {};
+    tile_mma_64(Ps, Ls, acc, 1.0);
+    __syncthreads();
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int g = lane >> 2, t = lane & 3;
+    const int rr = 16 * (w >> 1), cc = 32 * (w & 1);
+#pragma unroll
+    for (int i = 0; i < 2; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            Ps[(rr + 8 * i + g) * kLds + cc + 8 * j + 2 * t] = acc[i][j][0];
+            Ps[(rr + 8 * i + g) * kLds + cc + 8 * j + 2 * t + 1] = acc[i][j][1];
+        }
+    __syncthreads();
+    for (int idx = threadIdx.x; idx < 64 * 32; idx += blockDim.x) {
+        const int r = idx >> 5, c2 = idx & 31;
+        *reinterpret_cast<double2*>(A + (size_t)(r0 + r) * ld + k + 2 * c2) =
+            *reinterpret_cast<const double2*>(Ps + r * kLds + 2 * c2);
+    }
+    if (r0 >= n_pad && threadIdx.x < kNb) {
+        const int r = threadIdx.x;
+        double s = 0.0;
+        for (int j = 0; j < kNb; ++j) s = fma(Ps[r * kLds + j], Ps[r * kLds + j], s);
+        qacc[(size_t)f * ldq + (r0 - n_pad + r)] += s;
+    }
+}
+
+// Step 3: trailing update C -= P_i P_j^T over the lower tiles of the remaining square block
+// and all tiles of the right-hand-side rows.  Tile x < t(t+1)/2 is square tile (ti >= tj);
+// beyond that, right-hand-side tile rows follow.
+__global__ void __launch_bounds__(256) k_syrk_update(double* __restrict__ a, int64_t ld, int64_t stride, int64_t k,
+                                                     int64_t t_sq, int64_t t_rhs) {
+    extern __shared__ double smem[];
+    double* Pi = smem;
+    double* Pj = smem + 64 * kLds;
+    const int f = blockIdx.y;
+    const int64_t x = blockIdx.x;
+    const int64_t n_sq = t_sq * (t_sq + 1) / 2;
+    int64_t ti, tj;
+    if (x < n_sq) {
+        ti = (int64_t)((sqrt(8.0 * (double)x + 1.0) - 1.0) * 0.5);
+        while (ti * (ti + 1) / 2 > x) --ti;
+        while ((ti + 1) * (ti + 2) / 2 <= x) ++ti;
+        tj = x - ti * (ti + 1) / 2;
+    } else {
+        const int64_t y = x - n_sq;
+        ti = t_sq + y / t_sq;
+        tj = y % t_sq;
+        if (ti >= t_sq + t_rhs) return;
+    }
+    const int64_t base = k + kNb;
+    const int64_t ri = base + ti * kNb, cj = base + tj * kNb;
+    double* A = a + (size_t)f * stride;
+    load_tile_64(Pi, A + ri * ld + k, ld);
+    load_tile_64(Pj, A + cj * ld + k, ld);
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int g = lane >> 2, t = lane & 3;
+    const int rr = 16 * (w >> 1), cc = 32 * (w & 1);
+    double acc[2][4][2];
+#pragma unroll
+    for (int i = 0; i < 2; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const double2 v = *reinterpret_cast<const double2*>(A + (size_t)(ri + rr + 8 * i + g) * ld + cj + cc + 8 * j + 2 * t);
+            acc[i][j][0] = v.x;
+            acc[i][j][1] = v.y;
+        }
+    __syncthreads();
+    tile_mma_64(Pi, Pj, acc, -1.0);
+#pragma unroll
+    for (int i = 0; i < 2; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            double2 v;
+            v.x = acc[i][j][0];
+            v.y = acc[i][j][1];
+            *reinterpret_cast<double2*>(A + (size_t)(ri + rr + 8 * i + g) * ld + cj + cc + 8 * j + 2 * t) = v;
+        }
+}
+
+// q_out[f, j] = -qacc[f, j]  (x^T W_c x = -||L^{-1} D^1/2 x||^2).
+__global__ void k_negate_copy(const double* __restrict__ qacc, int nf, int m, int64_t ldq_in, double* __restrict__ q,
+                              int64_t ldq_out) {
+    const int f = blockIdx.y;
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < m; j += gridDim.x * blockDim.x)
+        q[(size_t)f * ldq_out + j] = -qacc[(size_t)f * ldq_in + j];
+}
+
+} // namespace
+
+int launch_gather_vph(const double* eri, int64_t nmo, int64_t nocc, double* v, cudaStream_t s) {
+    const int n = (int)(nocc * (nmo - nocc));
+    dim3 grid((unsigned)std::min<int64_t>((n + 255) / 256, 64), (unsigned)std::min(n, 65535));
+    k_gather_vph<<<grid, 256, 0, s>>>(eri, (int)nmo, (int)nocc, n, v);
+    GWB_LAUNCH("k_gather_vph");
+    return 1;
+}
+
+int launch_gather_panel(const double* eri, int64_t nmo, int64_t nocc, const int64_t* states, int64_t nstates,
+                        double* xt, cudaStream_t s) {
+    const int n = (int)(nocc * (nmo - nocc));
+    const int m = (int)(nstates * nmo);
+    dim3 grid((unsigned)std::min<int64_t>((n + 255) / 256, 64), (unsigned)std::min(m, 65535));
+    k_gather_panel<<<grid, 256, 0, s>>>(eri, (int)nmo, (int)nocc, n, states, m, xt);
+    GWB_LAUNCH("k_gather_panel");
+    return 1;
+}
+
+int launch_sigma_x_diag(const double* eri, int64_t nmo, int64_t nocc, double* out, cudaStream_t s) {
+    k_sigma_x_diag<<<(unsigned)((nmo + 127) / 128), 128, 0, s>>>(eri, (int)nmo, (int)nocc, out);
+    GWB_LAUNCH("k_sigma_x_diag");
+    return 1;
+}
+
+int launch_delta(const double* mo, int64_t nmo, int64_t nocc, double* delta, int* bad_gap, cudaStream_t s) {
+    const int64_t n = nocc * (nmo - nocc);
+    k_delta<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(mo, (int)nmo, (int)nocc, delta, bad_gap);
+    GWB_LAUNCH("k_delta");
+    return 1;
+}
+
+int launch_scale_vectors(const double* delta, int64_t n, int64_t n_pad, const double* omega, int64_t nf,
+                         double* dvec, cudaStream_t s) {
+    dim3 grid((unsigned)((n_pad + 255) / 256), (unsigned)nf);
+    k_scale_vectors<<<grid, 256, 0, s>>>(delta, (int)n, (int)n_pad, omega, (int)nf, dvec);
+    GWB_LAUNCH("k_scale_vectors");
+    return 1;
+}
+
+int launch_build_tall(const TallGeometry& g, const double* v, const double* xt, const double* dvec, int64_t nf,
+                      double* a, cudaStream_t s) {
+    dim3 grid((unsigned)((g.n_pad + 255) / 256), (unsigned)std::min<int64_t>(g.rows, 65535));
+    k_build_tall<<<grid, 256, 0, s>>>(g.n, g.m, g.n_pad, g.ld, g.stride, v, xt, dvec, (int)nf, a);
+    GWB_LAUNCH("k_build_tall");
+    return 1;
+}
+
+int launch_cholesky_step(const TallGeometry& g, int64_t k, int64_t nf, double* a, double* linv, double* qacc,
+                         unsigned long long* err_pivot, cudaStream_t s) {
+    const size_t smem = 2 * 64 * kLds * sizeof(double);
+    const size_t smem_potrf = 2 * kNb * (kNb + 1) * sizeof(double);
+    // Per-device opt-in for > 48 KB dynamic shared memory (cheap; repeated per call).
+    GWB_CUDA(cudaFuncSetAttribute(k_trsm_panel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    GWB_CUDA(cudaFuncSetAttribute(k_syrk_update, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    GWB_CUDA(cudaFuncSetAttribute(k_potrf_diag, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_potrf));
+    int launches = 0;
+    k_potrf_diag<<<(unsigned)nf, 256, smem_potrf, s>>>(a, g.ld, g.stride, k, linv, err_pivot);
+    GWB_LAUNCH("k_potrf_diag");
+    ++launches;
+    const int64_t below = g.rows - (k + kNb);
+    if (below > 0) {
+        dim3 grid((unsigned)(below / kNb), (unsigned)nf);
+        k_trsm_panel<<<grid, 256, smem, s>>>(a, g.ld, g.stride, k, g.n_pad, g.rows, linv, qacc, g.m_pad);
+        GWB_LAUNCH("k_trsm_panel");
+        ++launches;
+    }
+    const int64_t t_sq = (g.n_pad - (k + kNb)) / kNb;
+    if (t_sq > 0) {
+        const int64_t t_rhs = g.m_pad / kNb;
+        const int64_t tiles = t_sq * (t_sq + 1) / 2 + t_rhs * t_sq;
+        dim3 grid((unsigned)tiles, (unsigned)nf);
+        k_syrk_update<<<grid, 256, smem, s>>>(a, g.ld, g.stride, k, t_sq, t_rhs);
+        GWB_LAUNCH("k_syrk_update");
+        ++launches;
+    }
+    return launches;
+}
+
+int launch_negate_copy(const double* qacc, int64_t nf, int64_t m, int64_t ldq_in, double* q_out, int64_t ldq_out,
+                       cudaStream_t s) {
+    dim3 grid((unsigned)std::min<int64_t>((m + 255) / 256, 64), (unsigned)nf);
+    k_negate_copy<<<grid, 256, 0, s>>>(qacc, (int)nf, (int)m, ldq_in, q_out, ldq_out);
+    GWB_LAUNCH("k_negate_copy");
+    return 1;
+}
+
+} // namespace gwb200

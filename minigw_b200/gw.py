@@ -1,0 +1,286 @@
+"""Host-side mirror of the reference's G0W0 interface, driving libgwb200.
+
+Names, argument meaning and error behaviour follow the reference (scnlong/miniGW):
+
+    GwInput / GwSettings / GwResult / GwTimings   include/gw/gw.hpp:17-69
+    run_g0w0                                      src/gw/gw.cpp:125-191
+    read_gw_input_hdf5                            src/hdf5_input.cpp:192-212
+    generate_transformed_legendre_grid            src/gw/frequency_grids.cpp:62-93
+    B200Backend (name "b200", device family)      include/linalg/linalg.hpp:23-63,
+                                                  registered like src/linalg/backend_factory.cpp:22-66
+    output_self_energy_before_pade / _after_pade  src/io.cpp:86-108
+    output_final_energy_table                     src/io.cpp:110-126
+
+Failures raise GwB200Error (a RuntimeError, as the reference throws std::runtime_error).
+All numerical work runs in libgwb200 on the GPU.
+"""
+from __future__ import annotations
+
+import time
+from dataclasses import dataclass, field
+from typing import Optional, Sequence
+
+import ctypes as C
+import numpy as np
+
+from ._lib import FP64, MIXED, GwB200Error, Stats, check, dptr, iptr, lib
+
+HARTREE_TO_EV = 27.211386245988  # include/types.hpp:12
+
+
+@dataclass
+class GwInput:
+    """include/gw/gw.hpp:17-23 (eri_mo C-order [nmo]*4, mo_energy, vxc_mo, nocc, fermi_energy)."""
+    eri_mo: np.ndarray
+    mo_energy: np.ndarray
+    vxc_mo: np.ndarray
+    nocc: int
+    fermi_energy: float
+
+    @property
+    def nmo(self) -> int:
+        return int(self.mo_energy.shape[0])
+
+
+@dataclass
+class GwSettings:
+    """include/gw/gw.hpp:25-43.  `states` extends the reference's single selected state /
+    all states: when given, it is the explicit 0-based state list (the driver loop of
+    src/gw/sigma_c_driver.cpp:142 accepts any list)."""
+    num_freq_points_total: int = 200
+    num_pade_params: int = 16
+    selected_state_0based: Optional[int] = 4
+    eta: float = 0.0
+    states: Optional[Sequence[int]] = None
+    precision: str = "fp64"
+    device: int = 0
+
+
+@dataclass
+class GwTimings:
+    """include/gw/gw.hpp:45-56, plus the device-event split of the screening."""
+    total_wall_seconds: float = 0.0
+    exchange_seconds: float = 0.0
+    screening_setup_seconds: float = 0.0
+    sigma_c_wall_seconds: float = 0.0
+    pade_seconds: float = 0.0
+    device: dict = field(default_factory=dict)
+
+
+@dataclass
+class GwResult:
+    """include/gw/gw.hpp:58-65 (sigma_x is returned as its diagonal)."""
+    sigma_x_diag: np.ndarray
+    sigma_c_im_points: np.ndarray
+    qp_energy: np.ndarray
+    omegas: np.ndarray
+    weights: np.ndarray
+    timings: GwTimings
+
+
+def generate_transformed_legendre_grid(num_freq_points: int) -> tuple[np.ndarray, np.ndarray]:
+    """Transformed Gauss-Legendre grid (src/gw/frequency_grids.cpp:62-93)."""
+    if num_freq_points <= 0:
+        raise GwB200Error(1, "generate_transformed_legendre_grid: num_freq_points must be positive")
+    om = np.zeros(num_freq_points)
+    w = np.zeros(num_freq_points)
+    check(lib.gwb200_grid(num_freq_points, dptr(om), dptr(w)))
+    return om, w
+
+
+def read_gw_input_hdf5(path: str) -> GwInput:
+    """Read gw_input.h5 (src/hdf5_input.cpp:192-212) with libgwb200's minimal HDF5 reader."""
+    nmo = C.c_int64()
+    nocc = C.c_int64()
+    fermi = C.c_double()
+    check(lib.gwb200_read_input_h5(path.encode(), C.byref(nmo), C.byref(nocc), C.byref(fermi), None, None, None))
+    n = nmo.value
+    mo = np.zeros(n)
+    eri = np.zeros((n, n, n, n))
+    vxc = np.zeros((n, n))
+    check(lib.gwb200_read_input_h5(path.encode(), C.byref(nmo), C.byref(nocc), C.byref(fermi),
+                                   dptr(mo), dptr(eri), dptr(vxc)))
+    return GwInput(eri_mo=eri, mo_energy=mo, vxc_mo=vxc, nocc=nocc.value, fermi_energy=fermi.value)
+
+
+def _precision_code(p: str | int) -> int:
+    if p in ("fp64", FP64):
+        return FP64
+    if p in ("mixed", MIXED):
+        return MIXED
+    raise GwB200Error(7, f"unknown precision {p!r}")
+
+
+class B200Backend:
+    """The `b200` linear-algebra backend: one device handle holding a resident system.
+
+    capabilities() mirrors gw::linalg::BackendCapabilities for a device backend
+    (include/linalg/linalg.hpp:23-41): not thread-safe, uses device memory, so the
+    reference's validate_backend_for_execution rejects OpenMP frequency mode with it
+    (src/linalg/backend_factory.cpp:68-99).
+    """
+
+    def __init__(self, device: int = 0):
+        h = C.c_void_p()
+        check(lib.gwb200_create(device, C.byref(h)))
+        self._h = h
+        self.nmo = 0
+        self.nocc = 0
+        self.fermi = 0.0
+
+    @staticmethod
+    def name() -> str:
+        return "b200"
+
+    @staticmethod
+    def capabilities() -> dict:
+        return {"family": "Device", "thread_safe": False, "uses_internal_threads": False,
+                "distributed_mpi": False, "uses_device_memory": True}
+
+    def close(self) -> None:
+        if self._h:
+            lib.gwb200_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def load_system(self, inp: GwInput) -> None:
+        eri = np.ascontiguousarray(inp.eri_mo, dtype=np.float64)
+        mo = np.ascontiguousarray(inp.mo_energy, dtype=np.float64)
+        vxc = np.ascontiguousarray(inp.vxc_mo, dtype=np.float64)
+        nmo = mo.shape[0]
+        if eri.size != nmo ** 4 or vxc.size != nmo ** 2:
+            raise GwB200Error(1, "MolecularIntegrals: ERI tensor must have shape [nmo,nmo,nmo,nmo]")
+        check(lib.gwb200_load_system(self._h, nmo, int(inp.nocc), dptr(mo), dptr(eri), dptr(vxc),
+                                     float(inp.fermi_energy)))
+        self.nmo, self.nocc, self.fermi = nmo, int(inp.nocc), float(inp.fermi_energy)
+
+    def sigma_c(self, omegas, weights, states, eta: float = 0.0, precision="fp64"):
+        om = np.ascontiguousarray(omegas, dtype=np.float64)
+        w = np.ascontiguousarray(weights, dtype=np.float64)
+        st = np.ascontiguousarray(states, dtype=np.int64)
+        out = np.zeros((self.nmo, om.shape[0]), dtype=np.complex128)
+        stats = Stats()
+        check(lib.gwb200_sigma_c(self._h, dptr(om), dptr(w), om.shape[0], iptr(st), st.shape[0], float(eta),
+                                 _precision_code(precision), dptr(out), C.byref(stats)))
+        return out, stats.as_dict()
+
+    def screened_forms(self, omegas, states, eta: float = 0.0, precision="fp64"):
+        om = np.ascontiguousarray(omegas, dtype=np.float64)
+        st = np.ascontiguousarray(states, dtype=np.int64)
+        out = np.zeros((om.shape[0], st.shape[0], self.nmo))
+        stats = Stats()
+        check(lib.gwb200_screened_forms(self._h, dptr(om), om.shape[0], iptr(st), st.shape[0], float(eta),
+                                        _precision_code(precision), dptr(out), C.byref(stats)))
+        return out, stats.as_dict()
+
+    def sigma_x_diag(self) -> np.ndarray:
+        out = np.zeros(self.nmo)
+        check(lib.gwb200_sigma_x_diag(self._h, dptr(out)))
+        return out
+
+    def qp(self, omegas, sigma, npade, states) -> np.ndarray:
+        om = np.ascontiguousarray(omegas, dtype=np.float64)
+        sg = np.ascontiguousarray(sigma, dtype=np.complex128)
+        st = np.ascontiguousarray(states, dtype=np.int64)
+        out = np.zeros(self.nmo)
+        check(lib.gwb200_qp(self._h, dptr(om), om.shape[0], dptr(sg), int(npade), iptr(st), st.shape[0], dptr(out)))
+        return out
+
+    def pade_sweep(self, omegas, sigma_row, npade, npts=19836, fermi=None, x_start=-6.5, interval=0.00065):
+        om = np.ascontiguousarray(omegas, dtype=np.float64)
+        row = np.ascontiguousarray(sigma_row, dtype=np.complex128)
+        out = np.zeros((npts, 3))
+        f = self.fermi if fermi is None else fermi
+        check(lib.gwb200_pade_sweep(self._h, dptr(om), om.shape[0], dptr(row), int(npade), int(npts), float(f),
+                                    float(x_start), float(interval), dptr(out)))
+        return out
+
+    def fp64_peak_tflops(self) -> float:
+        v = C.c_double()
+        check(lib.gwb200_fp64_peak_tflops(self._h, C.byref(v)))
+        return v.value
+
+
+def selected_states(nmo: int, settings: GwSettings) -> list[int]:
+    """src/gw/gw.cpp:28-40 (plus the explicit list extension)."""
+    if settings.states is not None:
+        return [int(s) for s in settings.states]
+    if settings.selected_state_0based is not None:
+        if settings.selected_state_0based >= nmo:
+            raise GwB200Error(1, "Selected state is out of range")
+        return [int(settings.selected_state_0based)]
+    return list(range(nmo))
+
+
+def run_g0w0(inp: GwInput, settings: GwSettings, backend: B200Backend | None = None) -> GwResult:
+    """src/gw/gw.cpp:125-191 on the b200 backend: grid, exchange, Sigma_c(iw), QP."""
+    t0 = time.perf_counter()
+    own = backend is None
+    be = backend or B200Backend(settings.device)
+    try:
+        t = time.perf_counter()
+        be.load_system(inp)
+        setup = time.perf_counter() - t
+        omegas, weights = generate_transformed_legendre_grid(settings.num_freq_points_total)
+        states = selected_states(inp.nmo, settings)
+        t = time.perf_counter()
+        sigma, stats = be.sigma_c(omegas, weights, states, settings.eta, settings.precision)
+        sig_wall = time.perf_counter() - t
+        sigx = be.sigma_x_diag()
+        t = time.perf_counter()
+        qp = be.qp(omegas, sigma, settings.num_pade_params, states)
+        pade = time.perf_counter() - t
+    finally:
+        if own:
+            be.close()
+    timings = GwTimings(total_wall_seconds=time.perf_counter() - t0, screening_setup_seconds=setup,
+                        sigma_c_wall_seconds=sig_wall, pade_seconds=pade, device=stats)
+    return GwResult(sigma_x_diag=sigx, sigma_c_im_points=sigma, qp_energy=qp, omegas=omegas, weights=weights,
+                    timings=timings)
+
+
+def _g17(x: float) -> str:
+    return format(float(x), ".17g")
+
+
+def output_self_energy_before_pade(path: str, sigma_c: np.ndarray, state_0based: int) -> None:
+    """E_c_before_Pade.out: one '(re,im)' line per frequency at precision 17 (src/io.cpp:86-92)."""
+    with open(path, "w") as f:
+        for z in sigma_c[state_0based]:
+            f.write(f"({_g17(z.real)},{_g17(z.imag)})\n")
+
+
+def output_self_energy_after_pade(path: str, sweep: np.ndarray) -> None:
+    """E_c.out: 'E[eV] Re Im' lines at precision 17 (src/io.cpp:94-108); `sweep` from pade_sweep."""
+    with open(path, "w") as f:
+        for e, re, im in sweep:
+            f.write(f"{_g17(e)} {_g17(re)} {_g17(im)}\n")
+
+
+def _cpp_default(x: float) -> str:
+    # std::ostream default formatting (precision 6, %g-like).
+    return format(float(x), ".6g")
+
+
+def output_final_energy_table(mo_energy, sigma_x_diag, vxc, qp_energy, states) -> str:
+    """The summary table of gw.out (src/io.cpp:110-126), returned as text."""
+    lines = ["{:<10}{:<15}{:<15}{:<15}{:<15}{:<15}".format("Orbital", "KS Energy", "Sigma_x", "Sigma_c", "Vxc",
+                                                           "QP Energy"),
+             "{:<10}{:<15}{:<15}{:<15}{:<15}{:<15}".format("-------", "---------", "-------", "-------", "-------",
+                                                           "---------")]
+    for idx in states:
+        sc = qp_energy[idx] + vxc[idx, idx] - mo_energy[idx] - sigma_x_diag[idx]
+        vals = [mo_energy[idx], sigma_x_diag[idx], sc, vxc[idx, idx], qp_energy[idx]]
+        lines.append("{:<10}".format(idx + 1) + "".join("{:<15}".format(_cpp_default(v * HARTREE_TO_EV)) for v in vals))
+    return "\n".join(lines) + "\n"
