@@ -56,6 +56,12 @@ typedef struct gwb200_stats {
     int64_t info;                /* NOT_SPD: 1-based failing pivot; else 0 */
     int64_t nph;                 /* n = nocc * nvir */
     int64_t ncols;               /* m = nstates * nmo */
+    /* Filled only when the environment sets GWB200_PROFILE=1: CUDA-event time summed over the
+     * launches of the trailing-update kernel (the dominant kernel), their count, and their
+     * algorithmic flops (lower-triangle and right-hand-side tiles of the true n, m). */
+    double device_ms_update;
+    int64_t update_launches;
+    double flops_update;
 } gwb200_stats;
 
 typedef struct gwb200_handle gwb200_handle;
@@ -74,6 +80,12 @@ int gwb200_create(int device, gwb200_handle** out);
 
 /* Release every device buffer of the handle.  Safe on NULL. */
 int gwb200_destroy(gwb200_handle* h);
+
+/* Issue the handle's work on the caller's CUDA stream (a cudaStream_t passed as void*; NULL
+ * restores the handle's own stream), so a caller can order and time it with its own events.
+ * No reference counterpart: the reference's device workspace owns its implicit stream
+ * (src/workspace/device_screening_workspace.cu:288-310). */
+int gwb200_set_stream(gwb200_handle* h, void* stream);
 
 /* Upload one molecular system and build its resident device state: the occupied-virtual
  * index map, the V_ph=(jb|ia) gather and the exchange diagonal.  eri (nmo^4), mo_energy

@@ -32,7 +32,8 @@ MIXED = 1
 
 # Every symbol include/gwb200.h declares.
 EXPORTS = (
-    "gwb200_last_error", "gwb200_version", "gwb200_create", "gwb200_destroy", "gwb200_load_system",
+    "gwb200_last_error", "gwb200_version", "gwb200_create", "gwb200_destroy", "gwb200_set_stream",
+    "gwb200_load_system",
     "gwb200_sigma_c", "gwb200_screened_forms", "gwb200_sigma_x_diag", "gwb200_qp", "gwb200_pade_sweep",
     "gwb200_grid", "gwb200_read_input_h5", "gwb200_fp64_peak_tflops",
 )
@@ -60,6 +61,9 @@ class Stats(C.Structure):
         ("info", C.c_int64),
         ("nph", C.c_int64),
         ("ncols", C.c_int64),
+        ("device_ms_update", C.c_double),
+        ("update_launches", C.c_int64),
+        ("flops_update", C.c_double),
     ]
 
     def as_dict(self) -> dict:
@@ -81,6 +85,7 @@ def _load() -> C.CDLL:
     lib.gwb200_version.restype = C.c_char_p
     lib.gwb200_create.argtypes = [C.c_int, C.POINTER(_vp)]
     lib.gwb200_destroy.argtypes = [_vp]
+    lib.gwb200_set_stream.argtypes = [_vp, _vp]
     lib.gwb200_load_system.argtypes = [_vp, C.c_int64, C.c_int64, _dp, _dp, _dp, C.c_double]
     lib.gwb200_sigma_c.argtypes = [_vp, _dp, _dp, C.c_int64, _ip, C.c_int64, C.c_double, C.c_int, _dp,
                                    C.POINTER(Stats)]

@@ -1,6 +1,6 @@
 """Build libgwb200.so (sm_100a) and the `gw` command-line driver in-tree.
 
-    python -m minigw_b200.build [--verbose]
+    python minigw_b200/build.py [--verbose] [--ptxas-info]
 
 Outputs (git-ignored, shipped with the tree):
     minigw_b200/libgwb200.so   C ABI of include/gwb200.h

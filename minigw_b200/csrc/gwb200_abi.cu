@@ -4,6 +4,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <limits>
 #include <new>
@@ -59,7 +60,8 @@ int guarded(F&& body) {
 
 struct gwb200_handle {
     int device = 0;
-    cudaStream_t stream = nullptr;
+    cudaStream_t stream = nullptr;      // stream all work is issued on
+    cudaStream_t own_stream = nullptr;  // the handle's own stream
     cudaEvent_t ev[6] = {};
     // resident system
     bool loaded = false;
@@ -135,6 +137,11 @@ void compute_forms(gwb200_handle* h, const double* omega, int64_t nfreq, const i
     const size_t have = h->a.bytes + h->dvec.bytes + h->linv.bytes + h->qacc.bytes;
     const size_t budget = (size_t)((double)(free_b + have) * 0.85);
     int64_t fc = (int64_t)std::min<size_t>((size_t)nfreq, std::max<size_t>(1, budget / per_freq));
+    // GWB200_MAX_FREQ_CHUNK caps the chunk (tests use it to exercise the multi-chunk path).
+    if (const char* env = std::getenv("GWB200_MAX_FREQ_CHUNK")) {
+        const long long cap = std::atoll(env);
+        if (cap > 0) fc = std::min<int64_t>(fc, cap);
+    }
     if ((size_t)fc * per_freq > free_b + have) fail(GWB200_OOM, "not enough device memory for one frequency of eps(iw)");
     h->a.ensure(sizeof(double) * (size_t)fc * g.stride);
     h->dvec.ensure(sizeof(double) * (size_t)fc * g.n_pad);
@@ -145,6 +152,8 @@ void compute_forms(gwb200_handle* h, const double* omega, int64_t nfreq, const i
     launches += launch_gather_panel(h->eri.as<double>(), h->nmo, h->nocc, h->states.as<int64_t>(), nstates,
                                     h->xt.as<double>(), s);
     GWB_CUDA(cudaEventRecord(h->ev[1], s));
+    const char* prof_env = std::getenv("GWB200_PROFILE");
+    UpdateProfiler prof(prof_env && prof_env[0] == '1', s);
     int64_t chunks = 0;
     for (int64_t f0 = 0; f0 < nfreq; f0 += fc) {
         const int64_t nf = std::min(fc, nfreq - f0);
@@ -155,7 +164,7 @@ void compute_forms(gwb200_handle* h, const double* omega, int64_t nfreq, const i
         GWB_CUDA(cudaMemsetAsync(h->qacc.p, 0, sizeof(double) * (size_t)nf * g.m_pad, s));
         for (int64_t k = 0; k < g.n_pad; k += kNb)
             launches += launch_cholesky_step(g, k, nf, h->a.as<double>(), h->linv.as<double>(), h->qacc.as<double>(),
-                                             h->err.as<unsigned long long>(), s);
+                                             h->err.as<unsigned long long>(), s, prof.enabled ? &prof : nullptr);
         launches += launch_negate_copy(h->qacc.as<double>(), nf, m, g.m_pad, h->qall.as<double>() + f0 * g.m_pad,
                                        g.m_pad, s);
         ++chunks;
@@ -169,6 +178,7 @@ void compute_forms(gwb200_handle* h, const double* omega, int64_t nfreq, const i
         st->nph = g.n;
         st->ncols = m;
     }
+    if (prof.enabled && st) prof.collect(st);
 }
 
 void finish_forms(gwb200_handle* h, gwb200_stats* st) {
@@ -210,7 +220,8 @@ int gwb200_create(int device, gwb200_handle** out) {
         auto* h = new gwb200_handle();
         h->device = device;
         try {
-            GWB_CUDA(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+            GWB_CUDA(cudaStreamCreateWithFlags(&h->own_stream, cudaStreamNonBlocking));
+            h->stream = h->own_stream;
             for (auto& e2 : h->ev) GWB_CUDA(cudaEventCreate(&e2));
         } catch (...) {
             gwb200_destroy(h);
@@ -229,9 +240,17 @@ int gwb200_destroy(gwb200_handle* h) {
         b->release();
     for (auto& e : h->ev)
         if (e) cudaEventDestroy(e);
-    if (h->stream) cudaStreamDestroy(h->stream);
+    if (h->own_stream) cudaStreamDestroy(h->own_stream);
     delete h;
     return GWB200_OK;
+}
+
+int gwb200_set_stream(gwb200_handle* h, void* stream) {
+    return guarded([&] {
+        check_handle(h);
+        GWB_CUDA(cudaStreamSynchronize(h->stream));
+        h->stream = stream ? static_cast<cudaStream_t>(stream) : h->own_stream;
+    });
 }
 
 int gwb200_load_system(gwb200_handle* h, int64_t nmo, int64_t nocc, const double* mo_energy, const double* eri,

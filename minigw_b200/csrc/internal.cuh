@@ -6,6 +6,7 @@
 #include <cstdint>
 #include <stdexcept>
 #include <string>
+#include <vector>
 
 #include "../../include/gwb200.h"
 
@@ -62,6 +63,40 @@ inline TallGeometry make_geometry(int64_t n, int64_t m) {
     return g;
 }
 
+// Optional event timing of every trailing-update launch (the dominant kernel).
+struct UpdateProfiler {
+    bool enabled;
+    cudaStream_t stream;
+    std::vector<cudaEvent_t> events;  // pairs (start, stop)
+    double flops = 0.0;
+    UpdateProfiler(bool on, cudaStream_t s) : enabled(on), stream(s) {}
+    ~UpdateProfiler() {
+        for (auto e : events) cudaEventDestroy(e);
+    }
+    void begin() {
+        cudaEvent_t e;
+        cuda_check(cudaEventCreate(&e), "cudaEventCreate", __FILE__, __LINE__);
+        cuda_check(cudaEventRecord(e, stream), "cudaEventRecord", __FILE__, __LINE__);
+        events.push_back(e);
+    }
+    void end(double launch_flops) {
+        begin();
+        flops += launch_flops;
+    }
+    void collect(gwb200_stats* st) {
+        cuda_check(cudaStreamSynchronize(stream), "cudaStreamSynchronize", __FILE__, __LINE__);
+        double ms = 0.0;
+        for (size_t i = 0; i + 1 < events.size(); i += 2) {
+            float t = 0.f;
+            cuda_check(cudaEventElapsedTime(&t, events[i], events[i + 1]), "cudaEventElapsedTime", __FILE__, __LINE__);
+            ms += t;
+        }
+        st->device_ms_update = ms;
+        st->update_launches = (int64_t)(events.size() / 2);
+        st->flops_update = flops;
+    }
+};
+
 // ---- kernel launchers (kernels_fp64.cu, kernels_small.cu) ----
 int launch_gather_vph(const double* eri, int64_t nmo, int64_t nocc, double* v, cudaStream_t s);
 int launch_gather_panel(const double* eri, int64_t nmo, int64_t nocc, const int64_t* states, int64_t nstates,
@@ -74,7 +109,7 @@ int launch_build_tall(const TallGeometry& g, const double* v, const double* xt, 
                       double* a, cudaStream_t s);
 // One right-looking step at block column k for nf frequencies; returns launches issued.
 int launch_cholesky_step(const TallGeometry& g, int64_t k, int64_t nf, double* a, double* linv, double* qacc,
-                         unsigned long long* err_pivot, cudaStream_t s);
+                         unsigned long long* err_pivot, cudaStream_t s, UpdateProfiler* prof);
 int launch_sigma_contract(const double* qall, int64_t nfreq, int64_t nstates, int64_t nmo, int64_t ldq,
                           const int64_t* states, const double* mo, double fermi, const double* omega,
                           const double* weight, double* sigma, cudaStream_t s);

@@ -375,7 +375,7 @@ int launch_build_tall(const TallGeometry& g, const double* v, const double* xt, 
 }
 
 int launch_cholesky_step(const TallGeometry& g, int64_t k, int64_t nf, double* a, double* linv, double* qacc,
-                         unsigned long long* err_pivot, cudaStream_t s) {
+                         unsigned long long* err_pivot, cudaStream_t s, UpdateProfiler* prof) {
     const size_t smem = 2 * 64 * kLds * sizeof(double);
     const size_t smem_potrf = 2 * kNb * (kNb + 1) * sizeof(double);
     // Per-device opt-in for > 48 KB dynamic shared memory (cheap; repeated per call).
@@ -398,8 +398,15 @@ int launch_cholesky_step(const TallGeometry& g, int64_t k, int64_t nf, double* a
         const int64_t t_rhs = g.m_pad / kNb;
         const int64_t tiles = t_sq * (t_sq + 1) / 2 + t_rhs * t_sq;
         dim3 grid((unsigned)tiles, (unsigned)nf);
+        if (prof) prof->begin();
         k_syrk_update<<<grid, 256, smem, s>>>(a, g.ld, g.stride, k, t_sq, t_rhs);
         GWB_LAUNCH("k_syrk_update");
+        if (prof) {
+            // algorithmic flops: 2*nb per element of the true trailing lower triangle and RHS block
+            const double rem = (double)std::max<int64_t>(0, g.n - (k + kNb));
+            const double kb = (double)std::min<int64_t>(kNb, std::max<int64_t>(0, g.n - k));
+            prof->end((double)nf * 2.0 * kb * (rem * (rem + 1.0) / 2.0 + (double)g.m * rem));
+        }
         ++launches;
     }
     return launches;

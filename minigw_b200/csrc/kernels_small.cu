@@ -165,8 +165,8 @@ __global__ void k_pade_sweep(const double* __restrict__ sigma_row, const double*
     }
 }
 
-// Sigma_c(p_s, i w_n) = (1/pi) sum_{f', k} w_{f'} g(k, n, f') q[f', s, k], with
-// g = a / (a^2 + w_{f'}^2), a = i w_n + E_F - e_k, and q = -x^T W_c x >= 0 the squared norms
+// Sigma_c(p_s, i w_n) = -(1/pi) sum_{f', k} w_{f'} g(k, n, f') q[f', s, k], with
+// g = a / (a^2 + w_{f'}^2), a = i w_n + E_F - e_k, and q = x^T W_c x <= 0 the screened forms
 // (the reference's accumulation, src/gw/sigma_c_driver.cpp:154-168, with W_c hoisted out of
 // the loop over w_n).  One block per (n, s); fixed-shape tree reduction (deterministic).
 __global__ void __launch_bounds__(256) k_sigma_contract(const double* __restrict__ qall, int nfreq, int nmo,
@@ -186,7 +186,7 @@ __global__ void __launch_bounds__(256) k_sigma_contract(const double* __restrict
         const double dr = ar * ar - ai * ai + wp * wp, di = 2.0 * ar * ai;
         const double inv = 1.0 / (dr * dr + di * di);
         const double gr = (ar * dr + ai * di) * inv, gi = (ai * dr - ar * di) * inv;
-        const double scale = weight[fp] * q;
+        const double scale = -weight[fp] * q;
         sr = fma(gr, scale, sr);
         si = fma(gi, scale, si);
     }

@@ -154,6 +154,10 @@ class B200Backend:
         except Exception:
             pass
 
+    def set_stream(self, stream_ptr: int | None) -> None:
+        """Issue all work on a caller's CUDA stream (e.g. torch.cuda.Stream().cuda_stream)."""
+        check(lib.gwb200_set_stream(self._h, C.c_void_p(stream_ptr) if stream_ptr else None))
+
     def load_system(self, inp: GwInput) -> None:
         eri = np.ascontiguousarray(inp.eri_mo, dtype=np.float64)
         mo = np.ascontiguousarray(inp.mo_energy, dtype=np.float64)
