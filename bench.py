@@ -1,0 +1,343 @@
+#!/usr/bin/env python
+"""GW solves/s of the b200 G0W0 screening + self-energy path on synthetic inputs.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload cfg3] [--precision fp64]
+    python bench.py --impl reference ...        # the reference's own CPU path (oracle/_ref)
+
+A step is one GW solve of the workload: Sigma_c(iw) over all frequencies (V_ph / panel gathers,
+eps(iw) build, blocked Cholesky + panel solve, G0-weighted contraction) followed by the Pade /
+quasiparticle update, through the C ABI.  `value` times K steps with the system resident in HBM
+(CUDA events on the library's stream, max over ranks); `e2e` times the same steps including the
+host->device upload of the ERI from pinned host memory and the device->host read of Sigma_c and
+the QP energies.  Under torchrun each rank solves its own replica (independent systems, no
+collective in the data path): `scaling` is weak and `value` sums over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import datetime
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+WORKLOAD_TEXT = {
+    "cfg1": "H2O-shaped synthetic molecule: nmo=24 nocc=5 nph=95, 200 freq, 16 Pade, state 5",
+    "cfg2": "mixed-vs-fp64 molecule: nmo=120 nocc=20 nph=2000, 64 freq, 16 Pade, HOMO-2..LUMO+2",
+    "cfg3": "frequency-batched large solve: nmo=200 nocc=30 nph=5100, 128 freq, 16 Pade, HOMO-4..LUMO+4",
+}
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
+    ap.add_argument("--workload", choices=sorted(WORKLOAD_TEXT), default="cfg3")
+    ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64")
+    ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-pairs", type=int, default=0, help="reference (f_n, f') pairs per CPU sample (0 = auto)")
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------------------------------------
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.dev = device_index
+        self.proc = None
+        self.lines: list[str] = []
+        self.thread = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "200",
+                 "-i", str(self.dev)], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except (FileNotFoundError, OSError):
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        if self.thread:
+            self.thread.join(timeout=2)
+        sm, smax, power, reasons = [], [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+                power.append(float(parts[3]))
+            except ValueError:
+                continue
+            for name, val in zip(names, parts[5:9]):
+                if val.lower() == "active":
+                    reasons.add(name)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        # median over samples under load (the upper half by power)
+        pw_cut = statistics.median(power)
+        loaded = [s for s, p in zip(sm, power) if p >= pw_cut] or sm
+        return {"sm_mhz": statistics.median(loaded), "sm_max_mhz": max(smax), "reasons": sorted(reasons),
+                "samples": len(sm), "power_w_max": max(power)}
+
+
+# ---------------------------------------------------------------------------------------------
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def cpu_reference_sample(inp, wl, omegas, weights, pairs: int, threads: int):
+    """Times the reference's own CPU path (oracle/_ref: the reference's sources compiled
+    unmodified) on `pairs` (f_n, f') pairs of the workload: each pair is one W_c build
+    (zgetrf + zgetrs, BLAS/LAPACK backend) plus all panel contractions for the requested
+    states and their accumulation (src/gw/sigma_c_driver.cpp:133-164).  A full solve does
+    nfreq^2 such pairs, so solves/s = 1 / (nfreq^2 * seconds_per_pair)."""
+    import oracle
+
+    if not oracle.Ref.available:
+        return None
+    ref = oracle.Ref(blas_threads=threads)
+    fsel = [int(i * (wl.nfreq - 1) / max(1, pairs - 1)) for i in range(pairs)] if pairs > 1 else [wl.nfreq // 2]
+    sec, _ = ref.pair_seconds(inp, omegas[fsel], weights[fsel], float(omegas[0]), list(wl.states),
+                              backend="blas-lapack", threads=1)
+    per_pair = sec / len(fsel)
+    return {"seconds_per_pair": per_pair, "pairs": len(fsel), "threads": threads,
+            "solves_per_s": 1.0 / (wl.nfreq ** 2 * per_pair)}
+
+
+def auto_pairs(wl) -> int:
+    return {"cfg1": 400, "cfg2": 6, "cfg3": 2}[wl.name]
+
+
+def run_reference(args, wl):
+    """--impl reference: the reference's own CPU implementation of the path on the host cores."""
+    world, rank, _ = dist_setup()
+    if rank != 0:
+        return 0
+    import oracle
+    from minigw_b200.synthetic import make_input
+
+    threads = os.cpu_count() or 1
+    if not oracle.Ref.available:
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libgwref.so was not built (the reference "
+                          "tree was absent when the repository was built)"}))
+        return 0
+    from minigw_b200 import generate_transformed_legendre_grid
+
+    inp = make_input(wl.nmo, wl.nocc, args.seed)
+    om, w = generate_transformed_legendre_grid(wl.nfreq)
+    pairs = args.cpu_pairs or auto_pairs(wl)
+    for _ in range(args.warmup):
+        cpu_reference_sample(inp, wl, om, w, max(1, pairs // 2), threads)
+    samples = [cpu_reference_sample(inp, wl, om, w, pairs, threads) for _ in range(args.steps)]
+    per_pair = statistics.mean(s["seconds_per_pair"] for s in samples)
+    solve_s = wl.nfreq ** 2 * per_pair
+    value = 1.0 / solve_s
+    sample_txt = (f"{pairs} (f_n, f') pairs per step of the {wl.name} solve (one W_c build by zgetrf+zgetrs on "
+                  f"nph={wl.nph} plus {len(wl.states)}x{wl.nmo} panel contractions each), blas-lapack backend, "
+                  f"{threads} OpenBLAS threads; solve time = nfreq^2 x seconds per pair (extrapolated)")
+    out = {
+        "impl": "reference", "metric": "gw_solves_per_s", "value": value, "unit": "GW solves/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": per_pair * pairs * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c128",
+        "data": f"synthetic (seeded generator, seed {args.seed})",
+        "config": {"workload": f"{wl.name}: {WORKLOAD_TEXT[wl.name]}", "nmo": wl.nmo, "nocc": wl.nocc,
+                   "nph": wl.nph, "nfreq": wl.nfreq, "npade": wl.npade, "states": list(wl.states)},
+        "seconds_per_solve_extrapolated": solve_s,
+        "cpu_baseline": {"value": value, "unit": "GW solves/s", "cores": threads, "kind": "reference",
+                         "sample": sample_txt},
+        "e2e": {"value": value, "unit": "GW solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(out))
+    return 0
+
+
+# ---------------------------------------------------------------------------------------------
+def run_b200(args, wl):
+    import numpy as np
+    import torch
+
+    world, rank, local = dist_setup()
+    if world > 1:
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    else:
+        dist = None
+        torch.cuda.set_device(local)
+
+    from minigw_b200 import B200Backend, generate_transformed_legendre_grid
+    from minigw_b200.synthetic import make_input_on_device
+
+    inp = make_input_on_device(wl.nmo, wl.nocc, seed=args.seed + rank, device=local, pin=True)
+    om, w = generate_transformed_legendre_grid(wl.nfreq)
+    states = list(wl.states)
+    be = B200Backend(local)
+    stream = torch.cuda.Stream(device=local)
+    be.set_stream(stream.cuda_stream)
+    peak_fp64 = be.fp64_peak_tflops()
+    be.load_system(inp)
+
+    def step():
+        sig, st = be.sigma_c(om, w, states, precision=args.precision)
+        be.qp(om, sig, wl.npade, states)
+        return sig, st
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    def max_over_ranks(x: float) -> float:
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    for _ in range(max(3, args.warmup)):
+        step()
+
+    # ---- value: system resident in HBM ----
+    os.environ["GWB200_PROFILE"] = "1"
+    clocks = ClockSampler(local)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
+    barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    stats = []
+    ev[0].record(stream)
+    for i in range(args.steps):
+        _, st = step()
+        ev[i + 1].record(stream)
+        stats.append(st)
+    torch.cuda.synchronize()
+    clock_info = clocks.stop()
+    barrier()
+    os.environ.pop("GWB200_PROFILE", None)
+    step_ms = [ev[i].elapsed_time(ev[i + 1]) for i in range(args.steps)]
+    total_ms = ev[0].elapsed_time(ev[-1])
+    total_ms = max_over_ranks(total_ms)
+    ms_per_step = total_ms / args.steps
+
+    # ---- e2e: ERI uploaded from pinned host memory every step ----
+    h2d = inp.eri_mo.nbytes + inp.mo_energy.nbytes + inp.vxc_mo.nbytes + 2 * om.nbytes + 8 * len(states) * 2
+    d2h = 16 * wl.nmo * wl.nfreq + 8 * wl.nmo
+    ee0, ee1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier()
+    torch.cuda.synchronize()
+    ee0.record(stream)
+    for _ in range(args.steps):
+        be.load_system(inp)
+        step()
+    ee1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    e2e_ms = max_over_ranks(ee0.elapsed_time(ee1)) / args.steps
+
+    # ---- roofline of the dominant kernel (trailing update), measured live ----
+    upd_ms = sum(s["device_ms_update"] for s in stats)
+    upd_n = sum(s["update_launches"] for s in stats)
+    upd_flops = sum(s["flops_update"] for s in stats)
+    achieved = upd_flops / (upd_ms * 1e-3) / 1e12 if upd_ms > 0 else None
+    scr_ms = statistics.mean(s["device_ms_screening"] for s in stats)
+    scr_tflops = stats[0]["flops_screening"] / (scr_ms * 1e-3) / 1e12
+    launches = sum(s["kernel_launches"] for s in stats) + args.steps  # + one QP kernel per step
+
+    value = world * 1e3 / ms_per_step
+    result = {
+        "metric": "gw_solves_per_s", "value": value, "unit": "GW solves/s", "n_gpus": world, "steps": args.steps,
+        "warmup": max(3, args.warmup), "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64",
+        "data": f"synthetic (seeded generator, seed {args.seed}+rank; GEMM of the ERI on the GPU)",
+        "config": {"workload": f"{wl.name}: {WORKLOAD_TEXT[wl.name]}", "nmo": wl.nmo, "nocc": wl.nocc,
+                   "nph": wl.nph, "ncols": wl.ncols, "nfreq": wl.nfreq, "npade": wl.npade, "states": states,
+                   "precision": args.precision, "parallelism": f"{world} independent replica(s)",
+                   "l2": "inputs larger than L2 (eps(iw) is a "
+                         f"{(wl.nph + wl.ncols) * wl.nph * 8 / 1e6:.0f} MB matrix per frequency)"},
+        "ms_per_frequency": ms_per_step / wl.nfreq,
+        "frequency_points_per_s": world * wl.nfreq * 1e3 / ms_per_step,
+        "p50_ms": statistics.median(step_ms), "p99_ms": max(step_ms) if len(step_ms) < 100 else
+        sorted(step_ms)[int(0.99 * len(step_ms))], "step_ms": [round(x, 3) for x in step_ms],
+        "screening": {"device_ms": scr_ms, "tflops": scr_tflops, "flops_per_solve": stats[0]["flops_screening"]},
+        "roofline": {"bound": "tensor", "kernel": "k_syrk_update (FP64 DMMA trailing update)",
+                     "achieved": achieved, "peak": peak_fp64, "unit": "TFLOP/s",
+                     "frac": (achieved / peak_fp64) if achieved else None,
+                     "peak_source": "FP64 DMMA (mma.sync m8n8k4 f64) probe measured in this run; "
+                                    "MEASURED_PEAKS.json has no FP64 figure",
+                     "launches": upd_n, "traffic": None},
+        "e2e": {"value": world * 1e3 / e2e_ms, "unit": "GW solves/s", "h2d_bytes_per_step": int(h2d),
+                "d2h_bytes_per_step": int(d2h), "ms_per_step": e2e_ms},
+        "gpu_launches": int(launches),
+        "clocks": clock_info,
+    }
+    be.close()
+
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            host_inp = inp
+            cb = cpu_reference_sample(host_inp, wl, om, w, args.cpu_pairs or auto_pairs(wl), os.cpu_count() or 1)
+        except Exception as exc:  # the baseline is reported, never fatal
+            cb = None
+            result["cpu_baseline_error"] = str(exc)
+        if cb:
+            result["cpu_baseline"] = {
+                "value": cb["solves_per_s"], "unit": "GW solves/s", "cores": cb["threads"], "kind": "reference",
+                "sample": f"{cb['pairs']} (f_n, f') pairs of the {wl.name} solve through the reference's own code "
+                          f"(oracle/_ref, blas-lapack backend, {cb['threads']} OpenBLAS threads), "
+                          f"{cb['seconds_per_pair']:.3f} s per pair; solve time = nfreq^2 x pair time "
+                          "(extrapolated)"}
+    if dist is not None:
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(result))
+    return 0
+
+
+def main() -> int:
+    args = parse_args()
+    from minigw_b200.synthetic import WORKLOADS
+
+    wl = WORKLOADS[args.workload]
+    if args.impl == "reference":
+        return run_reference(args, wl)
+    return run_b200(args, wl)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -101,3 +101,49 @@ def make_input(nmo: int, nocc: int, seed: int = 0, out_eri: np.ndarray | None = 
 
 def make_workload_input(w: Workload, seed: int = 0, out_eri: np.ndarray | None = None) -> GwInput:
     return make_input(w.nmo, w.nocc, seed, out_eri)
+
+
+def make_input_on_device(nmo: int, nocc: int, seed: int = 0, device: int = 0, pin: bool = True) -> GwInput:
+    """Same recipe as make_input (identical random draws), with the nmo^2 x nmo^2 ERI product and
+    its symmetrisation done by torch on the GPU (FP64), then copied to (pinned) host memory.
+    Only the rounding of the ERI sum differs from the numpy path.  Used for the large benchmark
+    workloads, where the host GEMM would take minutes."""
+    import torch
+
+    rng = np.random.default_rng(seed)
+    nvir = nmo - nocc
+    occ = np.sort(rng.uniform(-1.2, -0.3, nocc))
+    vir = np.sort(rng.uniform(0.05, 3.0, nvir))
+    mo = np.concatenate([occ, vir])
+    fermi = 0.5 * (occ[-1] + vir[0])
+    nk = 2 * nmo
+    idx = np.arange(nmo)
+    decay = 0.3 * np.exp(-np.abs(idx[:, None] - idx[None, :]) / 8.0)
+    g = rng.standard_normal((nk, nmo, nmo))
+    lfac = (np.triu(g) + np.transpose(np.triu(g, 1), (0, 2, 1))) * decay
+    npq = nmo * nmo
+    dev = torch.device("cuda", device)
+    lmat = torch.from_numpy(np.ascontiguousarray(lfac.reshape(nk, npq))).to(dev)
+    e = lmat.t() @ lmat
+    del lmat
+    blk = 4096
+    for i0 in range(0, npq, blk):
+        i1 = min(npq, i0 + blk)
+        for j0 in range(i0, npq, blk):
+            j1 = min(npq, j0 + blk)
+            s = 0.5 * (e[i0:i1, j0:j1] + e[j0:j1, i0:i1].t())
+            e[i0:i1, j0:j1] = s
+            e[j0:j1, i0:i1] = s.t()
+    host = torch.empty((npq, npq), dtype=torch.float64, pin_memory=pin)
+    host.copy_(e)
+    del e
+    torch.cuda.synchronize(dev)
+    torch.cuda.empty_cache()
+    eri = host.numpy().reshape(nmo, nmo, nmo, nmo)
+    vxc = rng.normal(0.0, 0.01, (nmo, nmo))
+    vxc = np.triu(vxc, 1)
+    vxc = vxc + vxc.T
+    vxc[idx, idx] = rng.uniform(-0.6, -0.2, nmo)
+    inp = GwInput(eri_mo=eri, mo_energy=mo, vxc_mo=vxc, nocc=nocc, fermi_energy=float(fermi))
+    inp._pinned_owner = host  # keep the pinned tensor alive with the array view
+    return inp
