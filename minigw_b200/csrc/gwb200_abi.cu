@@ -162,9 +162,8 @@ void compute_forms(gwb200_handle* h, const double* omega, int64_t nfreq, const i
         launches += launch_build_tall(g, h->v.as<double>(), h->xt.as<double>(), h->dvec.as<double>(), nf,
                                       h->a.as<double>(), s);
         GWB_CUDA(cudaMemsetAsync(h->qacc.p, 0, sizeof(double) * (size_t)nf * g.m_pad, s));
-        for (int64_t k = 0; k < g.n_pad; k += kNb)
-            launches += launch_cholesky_step(g, k, nf, h->a.as<double>(), h->linv.as<double>(), h->qacc.as<double>(),
-                                             h->err.as<unsigned long long>(), s, prof.enabled ? &prof : nullptr);
+        launches += launch_factor_chunk(g, nf, h->a.as<double>(), h->linv.as<double>(), h->qacc.as<double>(),
+                                        h->err.as<unsigned long long>(), s, prof.enabled ? &prof : nullptr);
         launches += launch_negate_copy(h->qacc.as<double>(), nf, m, g.m_pad, h->qall.as<double>() + f0 * g.m_pad,
                                        g.m_pad, s);
         ++chunks;

@@ -107,9 +107,10 @@ int launch_scale_vectors(const double* delta, int64_t n, int64_t n_pad, const do
                          double* dvec, cudaStream_t s);
 int launch_build_tall(const TallGeometry& g, const double* v, const double* xt, const double* dvec, int64_t nf,
                       double* a, cudaStream_t s);
-// One right-looking step at block column k for nf frequencies; returns launches issued.
-int launch_cholesky_step(const TallGeometry& g, int64_t k, int64_t nf, double* a, double* linv, double* qacc,
-                         unsigned long long* err_pivot, cudaStream_t s, UpdateProfiler* prof);
+// Blocked Cholesky of the tall matrices of nf frequencies (outer blocks of two 64-wide inner
+// blocks); returns launches issued.
+int launch_factor_chunk(const TallGeometry& g, int64_t nf, double* a, double* linv, double* qacc,
+                        unsigned long long* err_pivot, cudaStream_t s, UpdateProfiler* prof);
 int launch_sigma_contract(const double* qall, int64_t nfreq, int64_t nstates, int64_t nmo, int64_t ldq,
                           const int64_t* states, const double* mo, double fermi, const double* omega,
                           const double* weight, double* sigma, cudaStream_t s);

@@ -129,23 +129,29 @@ __device__ __forceinline__ void dmma_8x8x4(double (&c)[2], double a, double b) {
                  : "d"(a), "d"(b));
 }
 
-__device__ __forceinline__ void tile_mma_64(const double* __restrict__ As, const double* __restrict__ Bs,
-                                            double (&acc)[2][4][2], double sgn) {
+template <int LD, int KD>
+__device__ __forceinline__ void tile_mma(const double* __restrict__ As, const double* __restrict__ Bs,
+                                         double (&acc)[2][4][2], double sgn) {
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int g = lane >> 2, t = lane & 3;
     const int r0 = 16 * (w >> 1), c0 = 32 * (w & 1);
 #pragma unroll 4
-    for (int kk = 0; kk < kNb; kk += 4) {
+    for (int kk = 0; kk < KD; kk += 4) {
         double af[2], bf[4];
 #pragma unroll
-        for (int i = 0; i < 2; ++i) af[i] = sgn * As[(r0 + 8 * i + g) * kLds + kk + t];
+        for (int i = 0; i < 2; ++i) af[i] = sgn * As[(r0 + 8 * i + g) * LD + kk + t];
 #pragma unroll
-        for (int j = 0; j < 4; ++j) bf[j] = Bs[(c0 + 8 * j + g) * kLds + kk + t];
+        for (int j = 0; j < 4; ++j) bf[j] = Bs[(c0 + 8 * j + g) * LD + kk + t];
 #pragma unroll
         for (int i = 0; i < 2; ++i)
 #pragma unroll
             for (int j = 0; j < 4; ++j) dmma_8x8x4(acc[i][j], af[i], bf[j]);
     }
+}
+
+__device__ __forceinline__ void tile_mma_64(const double* __restrict__ As, const double* __restrict__ Bs,
+                                            double (&acc)[2][4][2], double sgn) {
+    tile_mma<kLds, kNb>(As, Bs, acc, sgn);
 }
 
 // Copy a 64x64 tile (global row stride ld) into shared memory (stride kLds), 16-byte loads.
@@ -264,56 +270,88 @@ __global__ void __launch_bounds__(256) k_trsm_panel(double* __restrict__ a, int6
     }
 }
 
-// Step 3: trailing update C -= P_i P_j^T over the lower tiles of the remaining square block
-// and all tiles of the right-hand-side rows.  Tile x < t(t+1)/2 is square tile (ti >= tj);
-// beyond that, right-hand-side tile rows follow.
-__global__ void __launch_bounds__(256) k_syrk_update(double* __restrict__ a, int64_t ld, int64_t stride, int64_t k,
-                                                     int64_t t_sq, int64_t t_rhs) {
+// Step 3: update C -= sum_chunks P_i P_j^T of the output column tiles [tc0, tc0+T) (64-wide,
+// absolute tile indices): every tile on or below the diagonal in the square block, then every
+// tile of the right-hand-side rows.  The contraction runs over nk 64-wide column chunks of the
+// factored panels starting at column kb0, one chunk in shared memory at a time (cp.async), so
+// K = 64*nk costs one read and one write of C: the outer-block trailing update uses nk = 2
+// (16 flop per byte of C traffic), the narrow look-left update of an inner block nk = 1..q-1.
+// C is loaded into registers before the chunk loop and added in the epilogue, so its latency
+// overlaps the MMAs.
+__device__ __forceinline__ void cp_async_16(double* smem_dst, const double* gsrc) {
+    const unsigned saddr = (unsigned)__cvta_generic_to_shared(smem_dst);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(saddr), "l"(gsrc));
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+    asm volatile("cp.async.commit_group;\n" ::);
+    asm volatile("cp.async.wait_group 0;\n" ::);
+}
+// 64 x 32 slice of a panel (global row stride ld) into shared memory (stride kLdk).
+constexpr int kKc = 32;   // K sub-chunk of the pipelined update
+constexpr int kLdk = 36;  // its padded shared row stride (same bank spread as kLds)
+__device__ __forceinline__ void load_slice_async(double* __restrict__ s, const double* __restrict__ gsrc, int64_t ld) {
+    for (int idx = threadIdx.x; idx < 64 * (kKc / 2); idx += blockDim.x) {
+        const int r = idx / (kKc / 2), c2 = idx % (kKc / 2);
+        cp_async_16(s + r * kLdk + 2 * c2, gsrc + (size_t)r * ld + 2 * c2);
+    }
+}
+
+__global__ void __launch_bounds__(256, 3) k_update(double* __restrict__ a, int64_t ld, int64_t stride, int64_t kb0,
+                                                   int nk, int64_t tc0, int64_t T, int64_t nsq) {
     extern __shared__ double smem[];
-    double* Pi = smem;
-    double* Pj = smem + 64 * kLds;
+    // two pipeline stages, each holding the 64x32 slices of P_i and P_j
+    auto stage = [&](int st, int which) { return smem + (2 * st + which) * 64 * kLdk; };
     const int f = blockIdx.y;
     const int64_t x = blockIdx.x;
-    const int64_t n_sq = t_sq * (t_sq + 1) / 2;
-    int64_t ti, tj;
-    if (x < n_sq) {
-        ti = (int64_t)((sqrt(8.0 * (double)x + 1.0) - 1.0) * 0.5);
-        while (ti * (ti + 1) / 2 > x) --ti;
-        while ((ti + 1) * (ti + 2) / 2 <= x) ++ti;
-        tj = x - ti * (ti + 1) / 2;
+    const int64_t L = nsq - tc0;                     // square row tiles of the first column tile
+    const int64_t n_square = T * L - T * (T - 1) / 2;
+    int64_t c, tr;
+    if (x < n_square) {
+        // column offset c: largest c with cum(c) = c*L - c(c-1)/2 <= x
+        const double b = 2.0 * (double)L + 1.0;
+        c = (int64_t)((b - sqrt(fmax(b * b - 8.0 * (double)x, 0.0))) * 0.5);
+        auto cum = [L](int64_t cc) { return cc * L - cc * (cc - 1) / 2; };
+        while (c > 0 && cum(c) > x) --c;
+        while (c + 1 < T && cum(c + 1) <= x) ++c;
+        tr = tc0 + c + (x - cum(c));
     } else {
-        const int64_t y = x - n_sq;
-        ti = t_sq + y / t_sq;
-        tj = y % t_sq;
-        if (ti >= t_sq + t_rhs) return;
+        const int64_t y = x - n_square;
+        c = y % T;
+        tr = nsq + y / T;
     }
-    const int64_t base = k + kNb;
-    const int64_t ri = base + ti * kNb, cj = base + tj * kNb;
+    const int64_t ri = tr * kNb, cj = (tc0 + c) * kNb;
     double* A = a + (size_t)f * stride;
-    load_tile_64(Pi, A + ri * ld + k, ld);
-    load_tile_64(Pj, A + cj * ld + k, ld);
+    const int nsub = nk * (kNb / kKc);
+    load_slice_async(stage(0, 0), A + ri * ld + kb0, ld);
+    load_slice_async(stage(0, 1), A + cj * ld + kb0, ld);
+    asm volatile("cp.async.commit_group;\n" ::);
+    double acc[2][4][2] = {};
+    for (int sc = 0; sc < nsub; ++sc) {
+        if (sc + 1 < nsub) {
+            const int64_t kc = kb0 + (int64_t)(sc + 1) * kKc;
+            load_slice_async(stage((sc + 1) & 1, 0), A + ri * ld + kc, ld);
+            load_slice_async(stage((sc + 1) & 1, 1), A + cj * ld + kc, ld);
+            asm volatile("cp.async.commit_group;\n" ::);
+            asm volatile("cp.async.wait_group 1;\n" ::);
+        } else {
+            asm volatile("cp.async.wait_group 0;\n" ::);
+        }
+        __syncthreads();
+        tile_mma<kLdk, kKc>(stage(sc & 1, 0), stage(sc & 1, 1), acc, -1.0);
+        __syncthreads();
+    }
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int g = lane >> 2, t = lane & 3;
     const int rr = 16 * (w >> 1), cc = 32 * (w & 1);
-    double acc[2][4][2];
 #pragma unroll
     for (int i = 0; i < 2; ++i)
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
-            const double2 v = *reinterpret_cast<const double2*>(A + (size_t)(ri + rr + 8 * i + g) * ld + cj + cc + 8 * j + 2 * t);
-            acc[i][j][0] = v.x;
-            acc[i][j][1] = v.y;
-        }
-    __syncthreads();
-    tile_mma_64(Pi, Pj, acc, -1.0);
-#pragma unroll
-    for (int i = 0; i < 2; ++i)
-#pragma unroll
-        for (int j = 0; j < 4; ++j) {
-            double2 v;
-            v.x = acc[i][j][0];
-            v.y = acc[i][j][1];
-            *reinterpret_cast<double2*>(A + (size_t)(ri + rr + 8 * i + g) * ld + cj + cc + 8 * j + 2 * t) = v;
+            double2* pc = reinterpret_cast<double2*>(A + (size_t)(ri + rr + 8 * i + g) * ld + cj + cc + 8 * j + 2 * t);
+            double2 v = *pc;
+            v.x += acc[i][j][0];
+            v.y += acc[i][j][1];
+            *pc = v;
         }
 }
 
@@ -374,40 +412,58 @@ int launch_build_tall(const TallGeometry& g, const double* v, const double* xt, 
     return 1;
 }
 
-int launch_cholesky_step(const TallGeometry& g, int64_t k, int64_t nf, double* a, double* linv, double* qacc,
-                         unsigned long long* err_pivot, cudaStream_t s, UpdateProfiler* prof) {
+// Algorithmic flops of one update: 2 * K_true * (true lower elements of the output columns
+// [c0, c1) intersected with [0, n) + m per output column).
+static double update_flops(const TallGeometry& g, int64_t kb0, int nk, int64_t c0, int64_t c1) {
+    const int64_t kt = std::max<int64_t>(0, std::min<int64_t>(kb0 + (int64_t)nk * kNb, g.n) - kb0);
+    const int64_t a0 = std::min(c0, g.n), a1 = std::min(c1, g.n);
+    const double cols = (double)(a1 - a0);
+    const double lower = cols * (double)g.n - 0.5 * (double)(a0 + a1 - 1) * cols;  // sum_{c} (n - c)
+    return 2.0 * (double)kt * (lower + (double)g.m * cols);
+}
+
+int launch_factor_chunk(const TallGeometry& g, int64_t nf, double* a, double* linv, double* qacc,
+                        unsigned long long* err_pivot, cudaStream_t s, UpdateProfiler* prof) {
     const size_t smem = 2 * 64 * kLds * sizeof(double);
     const size_t smem_potrf = 2 * kNb * (kNb + 1) * sizeof(double);
-    // Per-device opt-in for > 48 KB dynamic shared memory (cheap; repeated per call).
     GWB_CUDA(cudaFuncSetAttribute(k_trsm_panel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    GWB_CUDA(cudaFuncSetAttribute(k_syrk_update, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    const size_t smem_update = 4 * 64 * kLdk * sizeof(double);
+    GWB_CUDA(cudaFuncSetAttribute(k_update, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_update));
     GWB_CUDA(cudaFuncSetAttribute(k_potrf_diag, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_potrf));
+    const int64_t nsq = g.n_pad / kNb;   // square tile rows/cols
+    const int64_t nrt = g.rows / kNb;    // all tile rows
+    constexpr int64_t kInner = 2;        // 64-wide inner blocks per outer block
     int launches = 0;
-    k_potrf_diag<<<(unsigned)nf, 256, smem_potrf, s>>>(a, g.ld, g.stride, k, linv, err_pivot);
-    GWB_LAUNCH("k_potrf_diag");
-    ++launches;
-    const int64_t below = g.rows - (k + kNb);
-    if (below > 0) {
-        dim3 grid((unsigned)(below / kNb), (unsigned)nf);
-        k_trsm_panel<<<grid, 256, smem, s>>>(a, g.ld, g.stride, k, g.n_pad, g.rows, linv, qacc, g.m_pad);
-        GWB_LAUNCH("k_trsm_panel");
-        ++launches;
-    }
-    const int64_t t_sq = (g.n_pad - (k + kNb)) / kNb;
-    if (t_sq > 0) {
-        const int64_t t_rhs = g.m_pad / kNb;
-        const int64_t tiles = t_sq * (t_sq + 1) / 2 + t_rhs * t_sq;
+    auto update = [&](int64_t kb0, int nk, int64_t tc0, int64_t T) {
+        const int64_t L = nsq - tc0;
+        const int64_t tiles = T * L - T * (T - 1) / 2 + T * (nrt - nsq);
+        if (tiles <= 0) return;
         dim3 grid((unsigned)tiles, (unsigned)nf);
         if (prof) prof->begin();
-        k_syrk_update<<<grid, 256, smem, s>>>(a, g.ld, g.stride, k, t_sq, t_rhs);
-        GWB_LAUNCH("k_syrk_update");
-        if (prof) {
-            // algorithmic flops: 2*nb per element of the true trailing lower triangle and RHS block
-            const double rem = (double)std::max<int64_t>(0, g.n - (k + kNb));
-            const double kb = (double)std::min<int64_t>(kNb, std::max<int64_t>(0, g.n - k));
-            prof->end((double)nf * 2.0 * kb * (rem * (rem + 1.0) / 2.0 + (double)g.m * rem));
-        }
+        k_update<<<grid, 256, smem_update, s>>>(a, g.ld, g.stride, kb0, nk, tc0, T, nsq);
+        GWB_LAUNCH("k_update");
+        if (prof) prof->end((double)nf * update_flops(g, kb0, nk, tc0 * kNb, (tc0 + T) * kNb));
         ++launches;
+    };
+    for (int64_t ob = 0; ob < nsq; ob += kInner) {
+        const int64_t q = std::min(kInner, nsq - ob);
+        for (int64_t j = 0; j < q; ++j) {
+            const int64_t kt = ob + j;
+            const int64_t k = kt * kNb;
+            if (j > 0) update(ob * kNb, (int)j, kt, 1);  // look-left: earlier inner blocks onto this column
+            k_potrf_diag<<<(unsigned)nf, 256, smem_potrf, s>>>(a, g.ld, g.stride, k, linv, err_pivot);
+            GWB_LAUNCH("k_potrf_diag");
+            ++launches;
+            const int64_t below = g.rows - (k + kNb);
+            if (below > 0) {
+                dim3 grid((unsigned)(below / kNb), (unsigned)nf);
+                k_trsm_panel<<<grid, 256, smem, s>>>(a, g.ld, g.stride, k, g.n_pad, g.rows, linv, qacc, g.m_pad);
+                GWB_LAUNCH("k_trsm_panel");
+                ++launches;
+            }
+        }
+        const int64_t tc0 = ob + q;
+        if (tc0 < nsq) update(ob * kNb, (int)q, tc0, nsq - tc0);  // outer-block trailing update, K = 64*q
     }
     return launches;
 }
