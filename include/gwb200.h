@@ -145,6 +145,27 @@ int gwb200_grid(int64_t nfreq, double* omega, double* weight);
 int gwb200_read_input_h5(const char* path, int64_t* nmo, int64_t* nocc, double* fermi_energy,
                          double* mo_energy, double* eri, double* vxc);
 
+/* Screened quadratic forms with NO device allocation, for callers that cannot call cudaMalloc
+ * (a framework whose caching allocator owns the device memory, a serving loop that cannot take
+ * the device-wide synchronisation of cudaMalloc/cudaFree, a process admitted under a fixed memory
+ * budget).  Same result as gwb200_screened_forms, from caller-owned DEVICE buffers:
+ *   d_v      n x n   V_ph[jb, ia] = (jb|ia), row-major
+ *   d_xt     m x n   the right-hand sides, row j = x_j[ia] (e.g. (p_s k|ia) for j = s*nmo + k)
+ *   d_delta  n       e_a - e_i, all > 0
+ *   d_omega  nfreq   imaginary frequencies
+ *   d_q_out  nfreq x m  x_j^T W_c(i w_f) x_j (<= 0), row-major
+ * on `stream` (a cudaStream_t as void*, NULL = the legacy default stream) of the CURRENT device.
+ * Every intermediate lives in one file-scope device array of 4 MiB that each GPU loading the
+ * library holds until exit; one frequency must fit: (n64 + m64) * n64 + n64 + 4096 + m64 doubles
+ * <= 524256 (n64, m64 = n, m rounded up to 64), e.g. n = m = 320, else GWB200_BAD_SHAPE.  The
+ * first call on a device looks up that array's device address (cudaGetSymbolAddress); make that
+ * first call before any stream capture.  All calls share the array and it keeps the last call's
+ * contents: calls that overlap on the GPU race and must be serialised by the caller.
+ * No counterpart in the reference (an addition of this library). */
+int gwb200_screened_forms_noalloc(int64_t n, int64_t m, const double* d_v, const double* d_xt,
+                                  const double* d_delta, const double* d_omega, int64_t nfreq,
+                                  double* d_q_out, void* stream);
+
 /* Measured FP64 tensor (DMMA) throughput of this device in TFLOP/s, from a short
  * microbenchmark of mma.sync f64 (used as the roofline denominator of the plain form). */
 int gwb200_fp64_peak_tflops(gwb200_handle* h, double* tflops);

@@ -35,7 +35,7 @@ EXPORTS = (
     "gwb200_last_error", "gwb200_version", "gwb200_create", "gwb200_destroy", "gwb200_set_stream",
     "gwb200_load_system",
     "gwb200_sigma_c", "gwb200_screened_forms", "gwb200_sigma_x_diag", "gwb200_qp", "gwb200_pade_sweep",
-    "gwb200_grid", "gwb200_read_input_h5", "gwb200_fp64_peak_tflops",
+    "gwb200_grid", "gwb200_read_input_h5", "gwb200_screened_forms_noalloc", "gwb200_fp64_peak_tflops",
 )
 
 
@@ -97,6 +97,7 @@ def _load() -> C.CDLL:
                                       C.c_double, _dp]
     lib.gwb200_grid.argtypes = [C.c_int64, _dp, _dp]
     lib.gwb200_read_input_h5.argtypes = [C.c_char_p, _ip, _ip, _dp, _dp, _dp, _dp]
+    lib.gwb200_screened_forms_noalloc.argtypes = [C.c_int64, C.c_int64, _vp, _vp, _vp, _vp, C.c_int64, _vp, _vp]
     lib.gwb200_fp64_peak_tflops.argtypes = [_vp, _dp]
     for name in EXPORTS:
         if name not in ("gwb200_last_error", "gwb200_version"):

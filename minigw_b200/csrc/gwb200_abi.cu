@@ -423,6 +423,14 @@ int gwb200_read_input_h5(const char* path, int64_t* nmo, int64_t* nocc, double* 
     });
 }
 
+int gwb200_screened_forms_noalloc(int64_t n, int64_t m, const double* d_v, const double* d_xt,
+                                  const double* d_delta, const double* d_omega, int64_t nfreq, double* d_q_out,
+                                  void* stream) {
+    return guarded([&] {
+        screened_forms_noalloc(n, m, d_v, d_xt, d_delta, d_omega, nfreq, d_q_out, static_cast<cudaStream_t>(stream));
+    });
+}
+
 int gwb200_fp64_peak_tflops(gwb200_handle* h, double* tflops) {
     return guarded([&] {
         check_handle(h);

@@ -122,6 +122,10 @@ int launch_pade_sweep(const double* sigma_row, const double* omega, int64_t nfre
 int launch_negate_copy(const double* qacc, int64_t nf, int64_t m, int64_t ldq_in, double* q_out, int64_t ldq_out,
                        cudaStream_t s);
 double measure_fp64_peak_tflops(cudaStream_t s);
+// noalloc.cu
+size_t noalloc_scratch_bytes();
+void screened_forms_noalloc(int64_t n, int64_t m, const double* d_v, const double* d_xt, const double* d_delta,
+                            const double* d_omega, int64_t nfreq, double* d_q_out, cudaStream_t s);
 
 // ---- host helpers (host_grid.cpp, host_h5.cpp) ----
 void transformed_legendre_grid(int64_t n, double* omega, double* weight);
