@@ -258,8 +258,12 @@ def run_b200(args, wl):
     ms_per_step = total_ms / args.steps
 
     # ---- e2e: ERI uploaded from pinned host memory every step ----
-    h2d = inp.eri_mo.nbytes + inp.mo_energy.nbytes + inp.vxc_mo.nbytes + 2 * om.nbytes + 8 * len(states) * 2
-    d2h = 16 * wl.nmo * wl.nfreq + 8 * wl.nmo
+    # bytes the library moves per e2e step: the (pq|o.) ERI block and exchange diagonal, mo energies
+    # and vxc diagonal (load_system); grid, weights and states (sigma_c); Sigma_c back to the device
+    # plus grid and states (qp); Sigma_c and the QP energies read back
+    nmo, nocc, nf, ns = wl.nmo, wl.nocc, wl.nfreq, len(states)
+    h2d = 8 * (nmo * nmo * nocc * nmo + nmo * nocc + 2 * nmo) + (16 * nf + 8 * ns) + (16 * nmo * nf + 8 * nf + 8 * ns)
+    d2h = 16 * nmo * nf + 8 * nmo
     ee0, ee1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     barrier()
     torch.cuda.synchronize()
@@ -296,6 +300,8 @@ def run_b200(args, wl):
         "frequency_points_per_s": world * wl.nfreq * 1e3 / ms_per_step,
         "p50_ms": statistics.median(step_ms), "p99_ms": max(step_ms) if len(step_ms) < 100 else
         sorted(step_ms)[int(0.99 * len(step_ms))], "step_ms": [round(x, 3) for x in step_ms],
+        "step_screening_ms": [round(s["device_ms_screening"], 3) for s in stats],
+        "step_update_ms": [round(s["device_ms_update"], 3) for s in stats],
         "screening": {"device_ms": scr_ms, "tflops": scr_tflops, "flops_per_solve": stats[0]["flops_screening"]},
         "roofline": {"bound": "tensor", "kernel": "k_update (FP64 DMMA trailing update)",
                      "achieved": achieved, "peak": peak_fp64, "unit": "TFLOP/s",
@@ -309,6 +315,13 @@ def run_b200(args, wl):
         "clocks": clock_info,
     }
     be.close()
+    try:
+        result["host_loadavg"] = open("/proc/loadavg").read().split()[:3]
+        apps = subprocess.run(["nvidia-smi", "--query-compute-apps=pid,used_memory", "--format=csv,noheader",
+                               "-i", str(local)], capture_output=True, text=True, timeout=10).stdout.strip()
+        result["gpu_processes"] = len([line for line in apps.splitlines() if line.strip()])
+    except Exception:
+        pass
 
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:

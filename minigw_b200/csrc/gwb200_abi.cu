@@ -68,7 +68,7 @@ struct gwb200_handle {
     int64_t nmo = 0, nocc = 0, n = 0;
     double fermi = 0.0;
     bool bad_gap = false;
-    DevBuf eri, mo, vxc_diag, delta, v, sigx, flag;
+    DevBuf pqo, xdiag, mo, vxc_diag, delta, v, sigx, flag;  // pqo: the (pq|o.) block of the ERI
     // per-call workspaces (grow-only, reused across calls)
     DevBuf xt, dvec, a, linv, qacc, qall, sigma, omega, weight, states, err, qp;
 };
@@ -149,7 +149,7 @@ void compute_forms(gwb200_handle* h, const double* omega, int64_t nfreq, const i
     h->qacc.ensure(sizeof(double) * (size_t)fc * g.m_pad);
 
     GWB_CUDA(cudaEventRecord(h->ev[0], s));
-    launches += launch_gather_panel(h->eri.as<double>(), h->nmo, h->nocc, h->states.as<int64_t>(), nstates,
+    launches += launch_gather_panel(h->pqo.as<double>(), h->nmo, h->nocc, h->states.as<int64_t>(), nstates,
                                     h->xt.as<double>(), s);
     GWB_CUDA(cudaEventRecord(h->ev[1], s));
     const char* prof_env = std::getenv("GWB200_PROFILE");
@@ -234,7 +234,7 @@ int gwb200_destroy(gwb200_handle* h) {
     if (!h) return GWB200_OK;
     cudaSetDevice(h->device);
     if (h->stream) cudaStreamSynchronize(h->stream);
-    for (DevBuf* b : {&h->eri, &h->mo, &h->vxc_diag, &h->delta, &h->v, &h->sigx, &h->flag, &h->xt, &h->dvec, &h->a,
+    for (DevBuf* b : {&h->pqo, &h->xdiag, &h->mo, &h->vxc_diag, &h->delta, &h->v, &h->sigx, &h->flag, &h->xt, &h->dvec, &h->a,
                       &h->linv, &h->qacc, &h->qall, &h->sigma, &h->omega, &h->weight, &h->states, &h->err, &h->qp})
         b->release();
     for (auto& e : h->ev)
@@ -262,9 +262,12 @@ int gwb200_load_system(gwb200_handle* h, int64_t nmo, int64_t nocc, const double
         if (nmo > 1024) fail(GWB200_BAD_SHAPE, "nmo > 1024 is not supported");
         cudaStream_t s = h->stream;
         h->loaded = false;
-        const size_t n4 = (size_t)nmo * nmo * nmo * nmo;
+        const size_t nmo2 = (size_t)nmo * nmo;
         const int64_t n = nocc * (nmo - nocc);
-        h->eri.ensure(sizeof(double) * n4);
+        // Only the (pq|o.) block is uploaded: every V_ph / panel element has an occupied third
+        // index.  One 2D copy: nmo^2 rows of nocc*nmo contiguous doubles, source pitch nmo^2.
+        h->pqo.ensure(sizeof(double) * nmo2 * nocc * nmo);
+        h->xdiag.ensure(sizeof(double) * nmo * nocc);
         h->mo.ensure(sizeof(double) * nmo);
         h->vxc_diag.ensure(sizeof(double) * nmo);
         h->sigx.ensure(sizeof(double) * nmo);
@@ -273,13 +276,19 @@ int gwb200_load_system(gwb200_handle* h, int64_t nmo, int64_t nocc, const double
         h->flag.ensure(sizeof(int));
         std::vector<double> vd((size_t)nmo);
         for (int64_t p = 0; p < nmo; ++p) vd[(size_t)p] = vxc[p * nmo + p];
-        GWB_CUDA(cudaMemcpyAsync(h->eri.p, eri, sizeof(double) * n4, cudaMemcpyHostToDevice, s));
+        GWB_CUDA(cudaMemcpy2DAsync(h->pqo.p, sizeof(double) * nocc * nmo, eri, sizeof(double) * nmo2,
+                                   sizeof(double) * nocc * nmo, nmo2, cudaMemcpyHostToDevice, s));
+        // exchange diagonal eri[p,i,p,i]: for each p, nocc elements with stride nmo^2 + 1
+        for (int64_t p = 0; p < nmo; ++p)
+            GWB_CUDA(cudaMemcpy2DAsync(h->xdiag.as<double>() + p * nocc, sizeof(double),
+                                       eri + ((size_t)p * nmo * nmo + p) * nmo, sizeof(double) * (nmo2 + 1),
+                                       sizeof(double), nocc, cudaMemcpyHostToDevice, s));
         GWB_CUDA(cudaMemcpyAsync(h->mo.p, mo_energy, sizeof(double) * nmo, cudaMemcpyHostToDevice, s));
         GWB_CUDA(cudaMemcpyAsync(h->vxc_diag.p, vd.data(), sizeof(double) * nmo, cudaMemcpyHostToDevice, s));
         GWB_CUDA(cudaMemsetAsync(h->flag.p, 0, sizeof(int), s));
         launch_delta(h->mo.as<double>(), nmo, nocc, h->delta.as<double>(), h->flag.as<int>(), s);
-        launch_gather_vph(h->eri.as<double>(), nmo, nocc, h->v.as<double>(), s);
-        launch_sigma_x_diag(h->eri.as<double>(), nmo, nocc, h->sigx.as<double>(), s);
+        launch_gather_vph(h->pqo.as<double>(), nmo, nocc, h->v.as<double>(), s);
+        launch_sigma_x_diag(h->xdiag.as<double>(), nmo, nocc, h->sigx.as<double>(), s);
         int bad = 0;
         GWB_CUDA(cudaMemcpyAsync(&bad, h->flag.p, sizeof(int), cudaMemcpyDeviceToHost, s));
         GWB_CUDA(cudaStreamSynchronize(s));

@@ -98,10 +98,12 @@ struct UpdateProfiler {
 };
 
 // ---- kernel launchers (kernels_fp64.cu, kernels_small.cu) ----
-int launch_gather_vph(const double* eri, int64_t nmo, int64_t nocc, double* v, cudaStream_t s);
-int launch_gather_panel(const double* eri, int64_t nmo, int64_t nocc, const int64_t* states, int64_t nstates,
+// pqo: the device-resident (pq|o.) block, pqo[(p*nmo + q)*nocc + i][s] = eri[p,q,i,s], i < nocc.
+int launch_gather_vph(const double* pqo, int64_t nmo, int64_t nocc, double* v, cudaStream_t s);
+int launch_gather_panel(const double* pqo, int64_t nmo, int64_t nocc, const int64_t* states, int64_t nstates,
                         double* xt, cudaStream_t s);
-int launch_sigma_x_diag(const double* eri, int64_t nmo, int64_t nocc, double* out, cudaStream_t s);
+// xdiag[p*nocc + i] = eri[p,i,p,i]
+int launch_sigma_x_diag(const double* xdiag, int64_t nmo, int64_t nocc, double* out, cudaStream_t s);
 int launch_delta(const double* mo, int64_t nmo, int64_t nocc, double* delta, int* bad_gap, cudaStream_t s);
 int launch_scale_vectors(const double* delta, int64_t n, int64_t n_pad, const double* omega, int64_t nf,
                          double* dvec, cudaStream_t s);

@@ -20,45 +20,48 @@ namespace {
 // ---------------------------------------------------------------------------
 // Gathers (bit-exact copies).
 
+// The device keeps only the (pq|o.) block of the ERI: pqo[(p*nmo + q)*nocc + i][s] = eri[p,q,i,s]
+// for i < nocc (every element the path reads except the exchange diagonal), uploaded by one 2D
+// copy whose rows are nocc*nmo contiguous doubles.
+
 // V[jb, ia] = eri[j, b, i, a]  (src/gw/sigma.cpp:56-71), row-major n x n.
 // blockIdx.y strides over rows jb; threads over ia: for fixed (jb, i) the source run
-// eri[j,b,i,nocc:nmo] is contiguous, so loads coalesce in runs of nvir.
-__global__ void k_gather_vph(const double* __restrict__ eri, int nmo, int nocc, int n, double* __restrict__ v) {
+// pqo[(j,b,i)][nocc:nmo] is contiguous, so loads coalesce in runs of nvir.
+__global__ void k_gather_vph(const double* __restrict__ pqo, int nmo, int nocc, int n, double* __restrict__ v) {
     const int nvir = nmo - nocc;
     for (int jb = blockIdx.y; jb < n; jb += gridDim.y) {
         const int j = jb / nvir, b = nocc + jb % nvir;
-        const size_t base = ((size_t)j * nmo + b) * (size_t)nmo * nmo;
+        const size_t base = ((size_t)j * nmo + b) * (size_t)nocc * nmo;
         for (int ia = blockIdx.x * blockDim.x + threadIdx.x; ia < n; ia += gridDim.x * blockDim.x) {
             const int i = ia / nvir, a = nocc + ia % nvir;
-            v[(size_t)jb * n + ia] = eri[base + (size_t)i * nmo + a];
+            v[(size_t)jb * n + ia] = pqo[base + (size_t)i * nmo + a];
         }
     }
 }
 
 // Xt[s*nmo + k, ia] = eri[p_s, k, i, a]  (src/workspace/pq_ph_panel.cpp:25-47, transposed so
 // that every right-hand side is a contiguous row), row-major m x n.
-__global__ void k_gather_panel(const double* __restrict__ eri, int nmo, int nocc, int n,
+__global__ void k_gather_panel(const double* __restrict__ pqo, int nmo, int nocc, int n,
                                const int64_t* __restrict__ states, int m, double* __restrict__ xt) {
     const int nvir = nmo - nocc;
     for (int row = blockIdx.y; row < m; row += gridDim.y) {
         const int s = row / nmo, k = row % nmo;
         const size_t p = (size_t)states[s];
-        const size_t base = (p * nmo + k) * (size_t)nmo * nmo;
+        const size_t base = (p * nmo + k) * (size_t)nocc * nmo;
         for (int ia = blockIdx.x * blockDim.x + threadIdx.x; ia < n; ia += gridDim.x * blockDim.x) {
             const int i = ia / nvir, a = nocc + ia % nvir;
-            xt[(size_t)row * n + ia] = eri[base + (size_t)i * nmo + a];
+            xt[(size_t)row * n + ia] = pqo[base + (size_t)i * nmo + a];
         }
     }
 }
 
-// Sigma_x[p,p] = -sum_{i<nocc} eri[p,i,p,i] in the reference's order (src/gw/sigma.cpp:29-36).
-__global__ void k_sigma_x_diag(const double* __restrict__ eri, int nmo, int nocc, double* __restrict__ out) {
+// Sigma_x[p,p] = -sum_{i<nocc} eri[p,i,p,i] in the reference's order (src/gw/sigma.cpp:29-36);
+// xdiag[p*nocc + i] = eri[p,i,p,i] (uploaded element by element).
+__global__ void k_sigma_x_diag(const double* __restrict__ xdiag, int nmo, int nocc, double* __restrict__ out) {
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= nmo) return;
     double value = 0.0;
-    for (int i = 0; i < nocc; ++i) {
-        value = __dsub_rn(value, eri[(((size_t)p * nmo + i) * nmo + p) * nmo + i]);
-    }
+    for (int i = 0; i < nocc; ++i) value = __dsub_rn(value, xdiag[(size_t)p * nocc + i]);
     out[p] = value;
 }
 
@@ -365,26 +368,26 @@ __global__ void k_negate_copy(const double* __restrict__ qacc, int nf, int m, in
 
 } // namespace
 
-int launch_gather_vph(const double* eri, int64_t nmo, int64_t nocc, double* v, cudaStream_t s) {
+int launch_gather_vph(const double* pqo, int64_t nmo, int64_t nocc, double* v, cudaStream_t s) {
     const int n = (int)(nocc * (nmo - nocc));
     dim3 grid((unsigned)std::min<int64_t>((n + 255) / 256, 64), (unsigned)std::min(n, 65535));
-    k_gather_vph<<<grid, 256, 0, s>>>(eri, (int)nmo, (int)nocc, n, v);
+    k_gather_vph<<<grid, 256, 0, s>>>(pqo, (int)nmo, (int)nocc, n, v);
     GWB_LAUNCH("k_gather_vph");
     return 1;
 }
 
-int launch_gather_panel(const double* eri, int64_t nmo, int64_t nocc, const int64_t* states, int64_t nstates,
+int launch_gather_panel(const double* pqo, int64_t nmo, int64_t nocc, const int64_t* states, int64_t nstates,
                         double* xt, cudaStream_t s) {
     const int n = (int)(nocc * (nmo - nocc));
     const int m = (int)(nstates * nmo);
     dim3 grid((unsigned)std::min<int64_t>((n + 255) / 256, 64), (unsigned)std::min(m, 65535));
-    k_gather_panel<<<grid, 256, 0, s>>>(eri, (int)nmo, (int)nocc, n, states, m, xt);
+    k_gather_panel<<<grid, 256, 0, s>>>(pqo, (int)nmo, (int)nocc, n, states, m, xt);
     GWB_LAUNCH("k_gather_panel");
     return 1;
 }
 
-int launch_sigma_x_diag(const double* eri, int64_t nmo, int64_t nocc, double* out, cudaStream_t s) {
-    k_sigma_x_diag<<<(unsigned)((nmo + 127) / 128), 128, 0, s>>>(eri, (int)nmo, (int)nocc, out);
+int launch_sigma_x_diag(const double* xdiag, int64_t nmo, int64_t nocc, double* out, cudaStream_t s) {
+    k_sigma_x_diag<<<(unsigned)((nmo + 127) / 128), 128, 0, s>>>(xdiag, (int)nmo, (int)nocc, out);
     GWB_LAUNCH("k_sigma_x_diag");
     return 1;
 }
