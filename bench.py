@@ -215,9 +215,8 @@ def run_b200(args, wl):
     be.load_system(inp)
 
     def step():
-        sig, st = be.sigma_c(om, w, states, precision=args.precision)
-        be.qp(om, sig, wl.npade, states)
-        return sig, st
+        r = be.run_g0w0(wl.nfreq, wl.npade, states, precision=args.precision)
+        return r["sigma"], r["stats"]
 
     def barrier():
         if dist is not None:
@@ -259,11 +258,11 @@ def run_b200(args, wl):
 
     # ---- e2e: ERI uploaded from pinned host memory every step ----
     # bytes the library moves per e2e step: the (pq|o.) ERI block and exchange diagonal, mo energies
-    # and vxc diagonal (load_system); grid, weights and states (sigma_c); Sigma_c back to the device
-    # plus grid and states (qp); Sigma_c and the QP energies read back
+    # and vxc diagonal (load_system); grid, weights and states (run_g0w0); Sigma_c, Sigma_x diagonal,
+    # QP energies and the pivot flag read back
     nmo, nocc, nf, ns = wl.nmo, wl.nocc, wl.nfreq, len(states)
-    h2d = 8 * (nmo * nmo * nocc * nmo + nmo * nocc + 2 * nmo) + (16 * nf + 8 * ns) + (16 * nmo * nf + 8 * nf + 8 * ns)
-    d2h = 16 * nmo * nf + 8 * nmo
+    h2d = 8 * (nmo * nmo * nocc * nmo + nmo * nocc + 2 * nmo) + (16 * nf + 8 * ns)
+    d2h = 16 * nmo * nf + 8 * nmo + 8 * nmo + 8
     ee0, ee1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     barrier()
     torch.cuda.synchronize()
@@ -283,7 +282,7 @@ def run_b200(args, wl):
     achieved = upd_flops / (upd_ms * 1e-3) / 1e12 if upd_ms > 0 else None
     scr_ms = statistics.mean(s["device_ms_screening"] for s in stats)
     scr_tflops = stats[0]["flops_screening"] / (scr_ms * 1e-3) / 1e12
-    launches = sum(s["kernel_launches"] for s in stats) + args.steps  # + one QP kernel per step
+    launches = sum(s["kernel_launches"] for s in stats)
 
     value = world * 1e3 / ms_per_step
     result = {

@@ -108,6 +108,17 @@ int gwb200_sigma_c(gwb200_handle* h, const double* omega, const double* weight, 
                    const int64_t* states, int64_t nstates, double eta, int precision,
                    double* sigma_out, gwb200_stats* stats);
 
+/* One whole G0W0 solve on the device for the loaded system: the transformed Gauss-Legendre grid,
+ * Sigma_c(iw) for the requested states, the exchange diagonal and the QP energies, with Sigma_c
+ * staying on the device between the screening and the Pade/QP step (one host synchronisation).
+ * Outputs are optional (NULL skips): omega_out/weight_out nfreq, sigma_out nmo x nfreq complex,
+ * sigma_x_out nmo, qp_out nmo (NaN where not requested).
+ * Replaces: gw::run_g0w0 (src/gw/gw.cpp:125-191) past input loading: grid (:138),
+ * calculate_exchange (:149), compute_sigma_c_with_backend (:163-172), solve_qp_energies (:180-186). */
+int gwb200_run_g0w0(gwb200_handle* h, int64_t nfreq, int64_t npade, const int64_t* states, int64_t nstates,
+                    double eta, int precision, double* omega_out, double* weight_out, double* sigma_out,
+                    double* sigma_x_out, double* qp_out, gwb200_stats* stats);
+
 /* Screened quadratic forms Q[f, s, k] = x_{p_s k}^T W_c(i w_f) x_{p_s k} (real, <= 0), layout
  * [nfreq][nstates][nmo].  The per-frequency quantity the reference computes as
  * quadratic_forms_panel (src/workspace/screening_workspace.cpp:69-102); exported for checking. */

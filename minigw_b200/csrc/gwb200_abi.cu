@@ -70,7 +70,7 @@ struct gwb200_handle {
     bool bad_gap = false;
     DevBuf pqo, xdiag, mo, vxc_diag, delta, v, sigx, flag;  // pqo: the (pq|o.) block of the ERI
     // per-call workspaces (grow-only, reused across calls)
-    DevBuf xt, dvec, a, linv, qacc, qall, sigma, omega, weight, states, err, qp;
+    DevBuf xt, dvec, a, linv, qacc, qall, sigma, omega, weight, states, err, qp, qp_scratch;
 };
 
 namespace {
@@ -103,7 +103,7 @@ float elapsed(cudaEvent_t a, cudaEvent_t b) {
 // Screened quadratic forms for all requested frequencies into h->qall ([nfreq][m] doubles,
 // x^T W_c x <= 0).  Records ev[0] (start), ev[1] (after gather), ev[2] (after screening).
 void compute_forms(gwb200_handle* h, const double* omega, int64_t nfreq, const int64_t* states, int64_t nstates,
-                   double eta, int precision, gwb200_stats* st) {
+                   double eta, int precision, gwb200_stats* st, const double* weight = nullptr) {
     if (!omega) fail(GWB200_BAD_ARGUMENT, "null omega");
     if (nfreq <= 0) fail(GWB200_BAD_SHAPE, "--freq-points must be positive");
     check_states(h, states, nstates);
@@ -128,6 +128,10 @@ void compute_forms(gwb200_handle* h, const double* omega, int64_t nfreq, const i
     h->err.ensure(sizeof(unsigned long long));
     GWB_CUDA(cudaMemcpyAsync(h->omega.p, omega, sizeof(double) * nfreq, cudaMemcpyHostToDevice, s));
     GWB_CUDA(cudaMemcpyAsync(h->states.p, states, sizeof(int64_t) * nstates, cudaMemcpyHostToDevice, s));
+    if (weight) {  // uploaded up front: a pageable upload later would wait for the whole screening
+        h->weight.ensure(sizeof(double) * nfreq);
+        GWB_CUDA(cudaMemcpyAsync(h->weight.p, weight, sizeof(double) * nfreq, cudaMemcpyHostToDevice, s));
+    }
     GWB_CUDA(cudaMemsetAsync(h->err.p, 0xFF, sizeof(unsigned long long), s));
 
     // Frequency chunk size from the HBM budget: tall matrices + scale vectors + 64x64 inverses.
@@ -194,6 +198,33 @@ void finish_forms(gwb200_handle* h, gwb200_stats* st) {
     }
 }
 
+// G0-weighted frequency contraction of h->qall into h->sigma (nmo x nfreq complex, zero rows for
+// unrequested states), with the weights compute_forms uploaded.  Records ev[3].
+void contract_on_device(gwb200_handle* h, int64_t nfreq, int64_t nstates, gwb200_stats* st) {
+    cudaStream_t s = h->stream;
+    const int64_t m = nstates * h->nmo;
+    const int64_t ldq = make_geometry(h->n, m).m_pad;
+    const size_t sig_bytes = sizeof(double) * 2 * (size_t)h->nmo * nfreq;
+    h->sigma.ensure(sig_bytes);
+    GWB_CUDA(cudaMemsetAsync(h->sigma.p, 0, sig_bytes, s));
+    st->kernel_launches += launch_sigma_contract(h->qall.as<double>(), nfreq, nstates, h->nmo, ldq,
+                                                 h->states.as<int64_t>(), h->mo.as<double>(), h->fermi,
+                                                 h->omega.as<double>(), h->weight.as<double>(),
+                                                 h->sigma.as<double>(), s);
+    GWB_CUDA(cudaEventRecord(h->ev[3], s));
+}
+
+// Pade + QP fixed point on h->sigma / h->omega / h->states (already on the device) into h->qp.
+void qp_on_device(gwb200_handle* h, int64_t nfreq, int64_t npade, int64_t nstates) {
+    cudaStream_t s = h->stream;
+    h->qp.ensure(sizeof(double) * h->nmo);
+    h->qp_scratch.ensure(qp_scratch_bytes(nfreq, nstates));
+    launch_fill(h->qp.as<double>(), std::numeric_limits<double>::quiet_NaN(), h->nmo, s);
+    launch_qp(h->sigma.as<double>(), h->omega.as<double>(), nfreq, h->nmo, h->states.as<int64_t>(), nstates, npade,
+              h->mo.as<double>(), h->fermi, h->sigx.as<double>(), h->vxc_diag.as<double>(), h->qp.as<double>(),
+              h->qp_scratch.p, s);
+}
+
 } // namespace
 
 extern "C" {
@@ -235,7 +266,8 @@ int gwb200_destroy(gwb200_handle* h) {
     cudaSetDevice(h->device);
     if (h->stream) cudaStreamSynchronize(h->stream);
     for (DevBuf* b : {&h->pqo, &h->xdiag, &h->mo, &h->vxc_diag, &h->delta, &h->v, &h->sigx, &h->flag, &h->xt, &h->dvec, &h->a,
-                      &h->linv, &h->qacc, &h->qall, &h->sigma, &h->omega, &h->weight, &h->states, &h->err, &h->qp})
+                      &h->linv, &h->qacc, &h->qall, &h->sigma, &h->omega, &h->weight, &h->states, &h->err, &h->qp,
+                      &h->qp_scratch})
         b->release();
     for (auto& e : h->ev)
         if (e) cudaEventDestroy(e);
@@ -327,25 +359,45 @@ int gwb200_sigma_c(gwb200_handle* h, const double* omega, const double* weight, 
         gwb200_stats local{};
         gwb200_stats* st = stats ? stats : &local;
         *st = gwb200_stats{};
-        compute_forms(h, omega, nfreq, states, nstates, eta, precision, st);
-        cudaStream_t s = h->stream;
-        const int64_t m = nstates * h->nmo;
-        const int64_t ldq = make_geometry(h->n, m).m_pad;
-        const size_t sig_bytes = sizeof(double) * 2 * (size_t)h->nmo * nfreq;
-        h->weight.ensure(sizeof(double) * nfreq);
-        h->sigma.ensure(sig_bytes);
-        GWB_CUDA(cudaMemcpyAsync(h->weight.p, weight, sizeof(double) * nfreq, cudaMemcpyHostToDevice, s));
-        GWB_CUDA(cudaMemsetAsync(h->sigma.p, 0, sig_bytes, s));
-        st->kernel_launches += launch_sigma_contract(h->qall.as<double>(), nfreq, nstates, h->nmo, ldq,
-                                                     h->states.as<int64_t>(), h->mo.as<double>(), h->fermi,
-                                                     h->omega.as<double>(), h->weight.as<double>(),
-                                                     h->sigma.as<double>(), s);
-        GWB_CUDA(cudaEventRecord(h->ev[3], s));
+        compute_forms(h, omega, nfreq, states, nstates, eta, precision, st, weight);
+        contract_on_device(h, nfreq, nstates, st);
         finish_forms(h, st);
         st->device_ms_contract = elapsed(h->ev[2], h->ev[3]);
         st->device_ms_total = elapsed(h->ev[0], h->ev[3]);
-        GWB_CUDA(cudaMemcpyAsync(sigma_out, h->sigma.p, sig_bytes, cudaMemcpyDeviceToHost, s));
+        GWB_CUDA(cudaMemcpyAsync(sigma_out, h->sigma.p, sizeof(double) * 2 * (size_t)h->nmo * nfreq,
+                                 cudaMemcpyDeviceToHost, h->stream));
+        GWB_CUDA(cudaStreamSynchronize(h->stream));
+    });
+}
+
+int gwb200_run_g0w0(gwb200_handle* h, int64_t nfreq, int64_t npade, const int64_t* states, int64_t nstates,
+                    double eta, int precision, double* omega_out, double* weight_out, double* sigma_out,
+                    double* sigma_x_out, double* qp_out, gwb200_stats* stats) {
+    return guarded([&] {
+        check_system(h);
+        if (nfreq <= 0) fail(GWB200_BAD_SHAPE, "--freq-points must be positive");
+        if (npade <= 0) fail(GWB200_BAD_SHAPE, "--pade-params must be positive");
+        gwb200_stats local{};
+        gwb200_stats* st = stats ? stats : &local;
+        *st = gwb200_stats{};
+        std::vector<double> omega((size_t)nfreq), weight((size_t)nfreq);
+        transformed_legendre_grid(nfreq, omega.data(), weight.data());
+        compute_forms(h, omega.data(), nfreq, states, nstates, eta, precision, st, weight.data());
+        contract_on_device(h, nfreq, nstates, st);
+        qp_on_device(h, nfreq, npade, nstates);
+        st->kernel_launches += 2;
+        finish_forms(h, st);
+        st->device_ms_contract = elapsed(h->ev[2], h->ev[3]);
+        st->device_ms_total = elapsed(h->ev[0], h->ev[3]);
+        cudaStream_t s = h->stream;
+        if (sigma_out)
+            GWB_CUDA(cudaMemcpyAsync(sigma_out, h->sigma.p, sizeof(double) * 2 * (size_t)h->nmo * nfreq,
+                                     cudaMemcpyDeviceToHost, s));
+        if (sigma_x_out) GWB_CUDA(cudaMemcpyAsync(sigma_x_out, h->sigx.p, sizeof(double) * h->nmo, cudaMemcpyDeviceToHost, s));
+        if (qp_out) GWB_CUDA(cudaMemcpyAsync(qp_out, h->qp.p, sizeof(double) * h->nmo, cudaMemcpyDeviceToHost, s));
         GWB_CUDA(cudaStreamSynchronize(s));
+        if (omega_out) std::copy(omega.begin(), omega.end(), omega_out);
+        if (weight_out) std::copy(weight.begin(), weight.end(), weight_out);
     });
 }
 
@@ -371,15 +423,10 @@ int gwb200_qp(gwb200_handle* h, const double* omega, int64_t nfreq, const double
         h->omega.ensure(sizeof(double) * nfreq);
         h->sigma.ensure(sig_bytes);
         h->states.ensure(sizeof(int64_t) * nstates);
-        h->qp.ensure(sizeof(double) * h->nmo);
-        std::vector<double> nan((size_t)h->nmo, std::numeric_limits<double>::quiet_NaN());
         GWB_CUDA(cudaMemcpyAsync(h->omega.p, omega, sizeof(double) * nfreq, cudaMemcpyHostToDevice, s));
         GWB_CUDA(cudaMemcpyAsync(h->sigma.p, sigma, sig_bytes, cudaMemcpyHostToDevice, s));
         GWB_CUDA(cudaMemcpyAsync(h->states.p, states, sizeof(int64_t) * nstates, cudaMemcpyHostToDevice, s));
-        GWB_CUDA(cudaMemcpyAsync(h->qp.p, nan.data(), sizeof(double) * h->nmo, cudaMemcpyHostToDevice, s));
-        launch_qp(h->sigma.as<double>(), h->omega.as<double>(), nfreq, h->nmo, h->states.as<int64_t>(), nstates,
-                  npade, h->mo.as<double>(), h->fermi, h->sigx.as<double>(), h->vxc_diag.as<double>(),
-                  h->qp.as<double>(), s);
+        qp_on_device(h, nfreq, npade, nstates);
         GWB_CUDA(cudaMemcpyAsync(qp_out, h->qp.p, sizeof(double) * h->nmo, cudaMemcpyDeviceToHost, s));
         GWB_CUDA(cudaStreamSynchronize(s));
     });
@@ -393,15 +440,16 @@ int gwb200_pade_sweep(gwb200_handle* h, const double* omega, int64_t nfreq, cons
         if (nfreq <= 0 || npts <= 0) fail(GWB200_BAD_SHAPE, "nfreq and npts must be positive");
         if (npade <= 0) fail(GWB200_BAD_SHAPE, "Pade: npar must be positive");
         cudaStream_t s = h->stream;
-        DevBuf dom, drow, dout;
+        DevBuf dom, drow, dout, dscr;
         try {
             dom.ensure(sizeof(double) * nfreq);
             drow.ensure(sizeof(double) * 2 * nfreq);
             dout.ensure(sizeof(double) * 3 * (size_t)npts);
+            dscr.ensure(qp_scratch_bytes(nfreq, pade_sweep_blocks(npts)));
             GWB_CUDA(cudaMemcpyAsync(dom.p, omega, sizeof(double) * nfreq, cudaMemcpyHostToDevice, s));
             GWB_CUDA(cudaMemcpyAsync(drow.p, sigma_row, sizeof(double) * 2 * nfreq, cudaMemcpyHostToDevice, s));
             launch_pade_sweep(drow.as<double>(), dom.as<double>(), nfreq, npade, npts, fermi, x_start, interval,
-                              dout.as<double>(), s);
+                              dout.as<double>(), dscr.p, s);
             GWB_CUDA(cudaMemcpyAsync(out, dout.p, sizeof(double) * 3 * (size_t)npts, cudaMemcpyDeviceToHost, s));
             GWB_CUDA(cudaStreamSynchronize(s));
         } catch (...) {
@@ -409,11 +457,13 @@ int gwb200_pade_sweep(gwb200_handle* h, const double* omega, int64_t nfreq, cons
             dom.release();
             drow.release();
             dout.release();
+            dscr.release();
             throw;
         }
         dom.release();
         drow.release();
         dout.release();
+        dscr.release();
     });
 }
 

@@ -116,11 +116,16 @@ int launch_factor_chunk(const TallGeometry& g, int64_t nf, double* a, double* li
 int launch_sigma_contract(const double* qall, int64_t nfreq, int64_t nstates, int64_t nmo, int64_t ldq,
                           const int64_t* states, const double* mo, double fermi, const double* omega,
                           const double* weight, double* sigma, cudaStream_t s);
+int launch_fill(double* p, double v, int64_t n, cudaStream_t s);
+// scratch: qp_scratch_bytes(nfreq, nstates) bytes of device memory
+size_t qp_scratch_bytes(int64_t nfreq, int64_t nstates);
 int launch_qp(const double* sigma, const double* omega, int64_t nfreq, int64_t nmo, const int64_t* states,
               int64_t nstates, int64_t npade, const double* mo, double fermi, const double* sigx,
-              const double* vxc_diag, double* qp, cudaStream_t s);
+              const double* vxc_diag, double* qp, void* scratch, cudaStream_t s);
+// scratch: qp_scratch_bytes(nfreq, pade_sweep_blocks(npts)) bytes of device memory
+int pade_sweep_blocks(int64_t npts);
 int launch_pade_sweep(const double* sigma_row, const double* omega, int64_t nfreq, int64_t npade, int64_t npts,
-                      double fermi, double x_start, double interval, double* out, cudaStream_t s);
+                      double fermi, double x_start, double interval, double* out, void* scratch, cudaStream_t s);
 int launch_negate_copy(const double* qacc, int64_t nf, int64_t m, int64_t ldq_in, double* q_out, int64_t ldq_out,
                        cudaStream_t s);
 double measure_fp64_peak_tflops(cudaStream_t s);

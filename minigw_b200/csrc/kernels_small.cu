@@ -209,6 +209,10 @@ __global__ void __launch_bounds__(256) k_sigma_contract(const double* __restrict
     }
 }
 
+__global__ void k_fill(double* __restrict__ p, double v, int64_t n) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) p[i] = v;
+}
+
 // Short FP64 DMMA throughput probe (8 warps/block, 4 independent accumulators per warp).
 __global__ void k_dmma_probe(double* out, int iters) {
     double a = threadIdx.x * 1e-3, b = 1.0 - threadIdx.x * 1e-4;
@@ -236,31 +240,34 @@ int launch_sigma_contract(const double* qall, int64_t nfreq, int64_t nstates, in
     return 1;
 }
 
-// scratch: caller provides nstates * 2 * nfreq complex of device memory via `sigma` layout; we
-// allocate it here on the stream-ordered allocator to keep the launcher self-contained.
-int launch_qp(const double* sigma, const double* omega, int64_t nfreq, int64_t nmo, const int64_t* states,
-              int64_t nstates, int64_t npade, const double* mo, double fermi, const double* sigx,
-              const double* vxc_diag, double* qp, cudaStream_t s) {
-    if (npade > kMaxPade) fail(GWB200_BAD_SHAPE, "npade exceeds the device Pade limit of 128");
-    cplx* scratch = nullptr;
-    GWB_CUDA(cudaMallocAsync(&scratch, sizeof(cplx) * 2 * (size_t)nfreq * (size_t)nstates, s));
-    k_qp<<<(unsigned)((nstates + 63) / 64), 64, 0, s>>>(sigma, omega, (int)nfreq, (int)nmo, states, (int)nstates,
-                                                         (int)npade, mo, fermi, sigx, vxc_diag, qp, scratch);
-    GWB_LAUNCH("k_qp");
-    GWB_CUDA(cudaFreeAsync(scratch, s));
+int launch_fill(double* p, double v, int64_t n, cudaStream_t s) {
+    k_fill<<<(unsigned)std::min<int64_t>((n + 255) / 256, 1024), 256, 0, s>>>(p, v, n);
+    GWB_LAUNCH("k_fill");
     return 1;
 }
 
-int launch_pade_sweep(const double* sigma_row, const double* omega, int64_t nfreq, int64_t npade, int64_t npts,
-                      double fermi, double x_start, double interval, double* out, cudaStream_t s) {
+size_t qp_scratch_bytes(int64_t nfreq, int64_t nstates) { return 2 * sizeof(cplx) * (size_t)nfreq * (size_t)nstates; }
+
+int launch_qp(const double* sigma, const double* omega, int64_t nfreq, int64_t nmo, const int64_t* states,
+              int64_t nstates, int64_t npade, const double* mo, double fermi, const double* sigx,
+              const double* vxc_diag, double* qp, void* scratch, cudaStream_t s) {
     if (npade > kMaxPade) fail(GWB200_BAD_SHAPE, "npade exceeds the device Pade limit of 128");
-    const int blocks = (int)std::min<int64_t>((npts + 255) / 256, 148);
-    cplx* scratch = nullptr;
-    GWB_CUDA(cudaMallocAsync(&scratch, sizeof(cplx) * 2 * (size_t)nfreq * (size_t)blocks, s));
-    k_pade_sweep<<<(unsigned)blocks, 256, 0, s>>>(sigma_row, omega, (int)nfreq, (int)npade, (int)npts, fermi, x_start,
-                                                  interval, out, scratch);
+    k_qp<<<(unsigned)((nstates + 63) / 64), 64, 0, s>>>(sigma, omega, (int)nfreq, (int)nmo, states, (int)nstates,
+                                                         (int)npade, mo, fermi, sigx, vxc_diag, qp,
+                                                         static_cast<cplx*>(scratch));
+    GWB_LAUNCH("k_qp");
+    return 1;
+}
+
+int pade_sweep_blocks(int64_t npts) { return (int)std::min<int64_t>((npts + 255) / 256, 148); }
+
+int launch_pade_sweep(const double* sigma_row, const double* omega, int64_t nfreq, int64_t npade, int64_t npts,
+                      double fermi, double x_start, double interval, double* out, void* scratch, cudaStream_t s) {
+    if (npade > kMaxPade) fail(GWB200_BAD_SHAPE, "npade exceeds the device Pade limit of 128");
+    k_pade_sweep<<<(unsigned)pade_sweep_blocks(npts), 256, 0, s>>>(sigma_row, omega, (int)nfreq, (int)npade,
+                                                                   (int)npts, fermi, x_start, interval, out,
+                                                                   static_cast<cplx*>(scratch));
     GWB_LAUNCH("k_pade_sweep");
-    GWB_CUDA(cudaFreeAsync(scratch, s));
     return 1;
 }
 
@@ -270,7 +277,7 @@ double measure_fp64_peak_tflops(cudaStream_t s) {
     GWB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
     const int blocks = sms * 8, threads = 256, iters = 4096;
     double* d = nullptr;
-    GWB_CUDA(cudaMallocAsync(&d, sizeof(double) * blocks * threads, s));
+    GWB_CUDA(cudaMalloc(&d, sizeof(double) * blocks * threads));
     cudaEvent_t e0, e1;
     GWB_CUDA(cudaEventCreate(&e0));
     GWB_CUDA(cudaEventCreate(&e1));
@@ -286,7 +293,7 @@ double measure_fp64_peak_tflops(cudaStream_t s) {
         best = std::min(best, ms);
     }
     GWB_LAUNCH("k_dmma_probe");
-    GWB_CUDA(cudaFreeAsync(d, s));
+    GWB_CUDA(cudaFree(d));
     GWB_CUDA(cudaEventDestroy(e0));
     GWB_CUDA(cudaEventDestroy(e1));
     const double flops = 2.0 * (blocks * threads / 32) * (double)iters * 4 * (8 * 8 * 4);

@@ -179,6 +179,18 @@ class B200Backend:
                                  _precision_code(precision), dptr(out), C.byref(stats)))
         return out, stats.as_dict()
 
+    def run_g0w0(self, nfreq: int, npade: int, states, eta: float = 0.0, precision="fp64"):
+        """Grid, Sigma_c(iw), Sigma_x diagonal and QP energies in one device call."""
+        st = np.ascontiguousarray(states, dtype=np.int64)
+        om, w = np.zeros(nfreq), np.zeros(nfreq)
+        sig = np.zeros((self.nmo, nfreq), dtype=np.complex128)
+        sx, qp = np.zeros(self.nmo), np.zeros(self.nmo)
+        stats = Stats()
+        check(lib.gwb200_run_g0w0(self._h, int(nfreq), int(npade), iptr(st), st.shape[0], float(eta),
+                                  _precision_code(precision), dptr(om), dptr(w), dptr(sig), dptr(sx), dptr(qp),
+                                  C.byref(stats)))
+        return {"omegas": om, "weights": w, "sigma": sig, "sigma_x_diag": sx, "qp": qp, "stats": stats.as_dict()}
+
     def screened_forms(self, omegas, states, eta: float = 0.0, precision="fp64"):
         om = np.ascontiguousarray(omegas, dtype=np.float64)
         st = np.ascontiguousarray(states, dtype=np.int64)
@@ -236,22 +248,18 @@ def run_g0w0(inp: GwInput, settings: GwSettings, backend: B200Backend | None = N
         t = time.perf_counter()
         be.load_system(inp)
         setup = time.perf_counter() - t
-        omegas, weights = generate_transformed_legendre_grid(settings.num_freq_points_total)
         states = selected_states(inp.nmo, settings)
         t = time.perf_counter()
-        sigma, stats = be.sigma_c(omegas, weights, states, settings.eta, settings.precision)
-        sig_wall = time.perf_counter() - t
-        sigx = be.sigma_x_diag()
-        t = time.perf_counter()
-        qp = be.qp(omegas, sigma, settings.num_pade_params, states)
-        pade = time.perf_counter() - t
+        r = be.run_g0w0(settings.num_freq_points_total, settings.num_pade_params, states, settings.eta,
+                        settings.precision)
+        wall = time.perf_counter() - t
     finally:
         if own:
             be.close()
     timings = GwTimings(total_wall_seconds=time.perf_counter() - t0, screening_setup_seconds=setup,
-                        sigma_c_wall_seconds=sig_wall, pade_seconds=pade, device=stats)
-    return GwResult(sigma_x_diag=sigx, sigma_c_im_points=sigma, qp_energy=qp, omegas=omegas, weights=weights,
-                    timings=timings)
+                        sigma_c_wall_seconds=wall, device=r["stats"])
+    return GwResult(sigma_x_diag=r["sigma_x_diag"], sigma_c_im_points=r["sigma"], qp_energy=r["qp"],
+                    omegas=r["omegas"], weights=r["weights"], timings=timings)
 
 
 def _g17(x: float) -> str:

@@ -247,3 +247,21 @@ def test_cfg2_sampled_frequencies_against_reference():
         assert np.abs(rq.imag).max() < 1e-9 * np.abs(rq.real).max()
         err = np.abs(q[fsel] - rq.real).max() / np.abs(rq.real).max()
         assert err < 1e-11, err
+
+
+def test_run_g0w0_equals_separate_calls(backend, cfg1_input):
+    from minigw_b200 import generate_transformed_legendre_grid
+
+    backend.load_system(cfg1_input)
+    states = [2, 4, 7]
+    r = backend.run_g0w0(48, 12, states)
+    om, w = generate_transformed_legendre_grid(48)
+    np.testing.assert_array_equal(r["omegas"], om)
+    np.testing.assert_array_equal(r["weights"], w)
+    sig, _ = backend.sigma_c(om, w, states)
+    np.testing.assert_array_equal(r["sigma"], sig)
+    np.testing.assert_array_equal(r["sigma_x_diag"], backend.sigma_x_diag())
+    qp = backend.qp(om, sig, 12, states)
+    np.testing.assert_array_equal(r["qp"][states], qp[states])
+    assert np.all(np.isnan(np.delete(r["qp"], states)))
+    assert r["stats"]["kernel_launches"] > 0
