@@ -46,6 +46,9 @@ def parse_args():
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-pairs", type=int, default=0, help="reference (f_n, f') pairs per CPU sample (0 = auto)")
+    ap.add_argument("--split-frequencies", action="store_true",
+                    help="N>1: split one solve's integration frequencies over the ranks (strong scaling; one "
+                         "NCCL all-reduce of the partial Sigma_c per solve) instead of one replica per rank")
     return ap.parse_args()
 
 
@@ -192,9 +195,16 @@ def run_b200(args, wl):
     import torch
 
     world, rank, local = dist_setup()
-    if world > 1:
+    if world > 1 or args.split_frequencies:
+        import socket
+
         import torch.distributed as dist
 
+        if "MASTER_PORT" not in os.environ:  # a single process run of the split path
+            with socket.socket() as sk:
+                sk.bind(("127.0.0.1", 0))
+                os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(sk.getsockname()[1]), RANK="0",
+                                  WORLD_SIZE="1")
         torch.cuda.set_device(local)
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
                                 device_id=torch.device("cuda", local))
@@ -203,9 +213,11 @@ def run_b200(args, wl):
         torch.cuda.set_device(local)
 
     from minigw_b200 import B200Backend, generate_transformed_legendre_grid
+    from minigw_b200.sharding import shard_bounds, sharded_sigma_c, torch_allreduce_sum
     from minigw_b200.synthetic import make_input_on_device
 
-    inp = make_input_on_device(wl.nmo, wl.nocc, seed=args.seed + rank, device=local, pin=True)
+    split = args.split_frequencies
+    inp = make_input_on_device(wl.nmo, wl.nocc, seed=args.seed + (0 if split else rank), device=local, pin=True)
     om, w = generate_transformed_legendre_grid(wl.nfreq)
     states = list(wl.states)
     be = B200Backend(local)
@@ -214,9 +226,21 @@ def run_b200(args, wl):
     peak_fp64 = be.fp64_peak_tflops()
     be.load_system(inp)
 
+    reduce_sum = torch_allreduce_sum(f"cuda:{local}") if split else None
+
     def step():
-        r = be.run_g0w0(wl.nfreq, wl.npade, states, precision=args.precision)
-        return r["sigma"], r["stats"]
+        if not split:
+            r = be.run_g0w0(wl.nfreq, wl.npade, states, precision=args.precision)
+            return r["sigma"], r["stats"]
+        box = {}
+
+        def partial(b, e):
+            part, box["stats"] = be.sigma_c_shard(om, w, b, e, states, precision=args.precision)
+            return part
+
+        sig = sharded_sigma_c(partial, wl.nfreq, world, rank, reduce_sum)
+        be.qp(om, sig, wl.npade, states)
+        return sig, box["stats"]
 
     def barrier():
         if dist is not None:
@@ -236,6 +260,7 @@ def run_b200(args, wl):
     os.environ["GWB200_PROFILE"] = "1"
     clocks = ClockSampler(local)
     ev = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
+    torch.cuda.set_stream(stream)  # collectives and events on the library's stream
     clocks.start()
     time.sleep(1.5)  # nvidia-smi's start-up stalls the device; let it settle before timing
     step()
@@ -284,19 +309,24 @@ def run_b200(args, wl):
     scr_tflops = stats[0]["flops_screening"] / (scr_ms * 1e-3) / 1e12
     launches = sum(s["kernel_launches"] for s in stats)
 
-    value = world * 1e3 / ms_per_step
+    solves_per_step = 1 if split else world
+    value = solves_per_step * 1e3 / ms_per_step
     result = {
         "metric": "gw_solves_per_s", "value": value, "unit": "GW solves/s", "n_gpus": world, "steps": args.steps,
-        "warmup": max(3, args.warmup), "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+        "warmup": max(3, args.warmup), "ms_per_step": ms_per_step, "higher_is_better": True,
+        "scaling": "strong" if split else "weak",
         "vs_baseline": None, "dtype": "f64",
         "data": f"synthetic (seeded generator, seed {args.seed}+rank; GEMM of the ERI on the GPU)",
         "config": {"workload": f"{wl.name}: {WORKLOAD_TEXT[wl.name]}", "nmo": wl.nmo, "nocc": wl.nocc,
                    "nph": wl.nph, "ncols": wl.ncols, "nfreq": wl.nfreq, "npade": wl.npade, "states": states,
-                   "precision": args.precision, "parallelism": f"{world} independent replica(s)",
+                   "precision": args.precision,
+                   "parallelism": (f"integration frequencies split over {world} ranks "
+                                   f"(rank 0: {shard_bounds(wl.nfreq, world, 0)}), NCCL all-reduce of Sigma_c")
+                   if split else f"{world} independent replica(s)",
                    "l2": "inputs larger than L2 (eps(iw) is a "
                          f"{(wl.nph + wl.ncols) * wl.nph * 8 / 1e6:.0f} MB matrix per frequency)"},
         "ms_per_frequency": ms_per_step / wl.nfreq,
-        "frequency_points_per_s": world * wl.nfreq * 1e3 / ms_per_step,
+        "frequency_points_per_s": solves_per_step * wl.nfreq * 1e3 / ms_per_step,
         "p50_ms": statistics.median(step_ms), "p99_ms": max(step_ms) if len(step_ms) < 100 else
         sorted(step_ms)[int(0.99 * len(step_ms))], "step_ms": [round(x, 3) for x in step_ms],
         "step_screening_ms": [round(s["device_ms_screening"], 3) for s in stats],
@@ -308,7 +338,7 @@ def run_b200(args, wl):
                      "peak_source": "FP64 DMMA (mma.sync m8n8k4 f64) probe measured in this run; "
                                     "MEASURED_PEAKS.json has no FP64 figure",
                      "launches": upd_n, "traffic": None},
-        "e2e": {"value": world * 1e3 / e2e_ms, "unit": "GW solves/s", "h2d_bytes_per_step": int(h2d),
+        "e2e": {"value": solves_per_step * 1e3 / e2e_ms, "unit": "GW solves/s", "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h), "ms_per_step": e2e_ms},
         "gpu_launches": int(launches),
         "clocks": clock_info,

@@ -108,6 +108,17 @@ int gwb200_sigma_c(gwb200_handle* h, const double* omega, const double* weight, 
                    const int64_t* states, int64_t nstates, double eta, int precision,
                    double* sigma_out, gwb200_stats* stats);
 
+/* The contribution of the integration frequencies f' in [f_begin, f_end) of the grid to Sigma_c at
+ * every output frequency of the grid: sigma_partial_out is nmo x nfreq complex.  The partial sums of
+ * a partition of [0, nfreq) add up to gwb200_sigma_c's result (up to summation order); ranks that
+ * each solve one shard of one system reduce them with one all-reduce of nmo x nfreq complex.
+ * Replaces: the MPI frequency distribution of compute_sigma_c_serial_or_mpi + mpi_allreduce_sum_in_place
+ * (src/gw/sigma_c_driver.cpp:368-401, 507-512; src/mpi_context.cpp:45-64), split here over the
+ * integration frequency f' (each W_c solved once) instead of the output frequency f_n. */
+int gwb200_sigma_c_shard(gwb200_handle* h, const double* omega, const double* weight, int64_t nfreq,
+                         int64_t f_begin, int64_t f_end, const int64_t* states, int64_t nstates, double eta,
+                         int precision, double* sigma_partial_out, gwb200_stats* stats);
+
 /* One whole G0W0 solve on the device for the loaded system: the transformed Gauss-Legendre grid,
  * Sigma_c(iw) for the requested states, the exchange diagonal and the QP energies, with Sigma_c
  * staying on the device between the screening and the Pade/QP step (one host synchronisation).

@@ -70,7 +70,7 @@ struct gwb200_handle {
     bool bad_gap = false;
     DevBuf pqo, xdiag, mo, vxc_diag, delta, v, sigx, flag;  // pqo: the (pq|o.) block of the ERI
     // per-call workspaces (grow-only, reused across calls)
-    DevBuf xt, dvec, a, linv, qacc, qall, sigma, omega, weight, states, err, qp, qp_scratch;
+    DevBuf xt, dvec, a, linv, qacc, qall, sigma, omega, weight, states, err, qp, qp_scratch, omega_out;
 };
 
 namespace {
@@ -198,18 +198,24 @@ void finish_forms(gwb200_handle* h, gwb200_stats* st) {
     }
 }
 
-// G0-weighted frequency contraction of h->qall into h->sigma (nmo x nfreq complex, zero rows for
-// unrequested states), with the weights compute_forms uploaded.  Records ev[3].
-void contract_on_device(gwb200_handle* h, int64_t nfreq, int64_t nstates, gwb200_stats* st) {
+// G0-weighted frequency contraction of h->qall (the nf_int frequencies compute_forms solved, with
+// the weights it uploaded) into h->sigma (nmo x nf_out complex, zero rows for unrequested states).
+// omega_out_dev = NULL: the output grid is the integration grid.  Records ev[3].
+void contract_on_device(gwb200_handle* h, int64_t nf_int, int64_t nstates, gwb200_stats* st,
+                        const double* omega_out_dev = nullptr, int64_t nf_out = -1) {
     cudaStream_t s = h->stream;
     const int64_t m = nstates * h->nmo;
     const int64_t ldq = make_geometry(h->n, m).m_pad;
-    const size_t sig_bytes = sizeof(double) * 2 * (size_t)h->nmo * nfreq;
+    if (!omega_out_dev) {
+        omega_out_dev = h->omega.as<double>();
+        nf_out = nf_int;
+    }
+    const size_t sig_bytes = sizeof(double) * 2 * (size_t)h->nmo * nf_out;
     h->sigma.ensure(sig_bytes);
     GWB_CUDA(cudaMemsetAsync(h->sigma.p, 0, sig_bytes, s));
-    st->kernel_launches += launch_sigma_contract(h->qall.as<double>(), nfreq, nstates, h->nmo, ldq,
+    st->kernel_launches += launch_sigma_contract(h->qall.as<double>(), nf_int, nstates, h->nmo, ldq,
                                                  h->states.as<int64_t>(), h->mo.as<double>(), h->fermi,
-                                                 h->omega.as<double>(), h->weight.as<double>(),
+                                                 h->omega.as<double>(), h->weight.as<double>(), omega_out_dev, nf_out,
                                                  h->sigma.as<double>(), s);
     GWB_CUDA(cudaEventRecord(h->ev[3], s));
 }
@@ -267,7 +273,7 @@ int gwb200_destroy(gwb200_handle* h) {
     if (h->stream) cudaStreamSynchronize(h->stream);
     for (DevBuf* b : {&h->pqo, &h->xdiag, &h->mo, &h->vxc_diag, &h->delta, &h->v, &h->sigx, &h->flag, &h->xt, &h->dvec, &h->a,
                       &h->linv, &h->qacc, &h->qall, &h->sigma, &h->omega, &h->weight, &h->states, &h->err, &h->qp,
-                      &h->qp_scratch})
+                      &h->qp_scratch, &h->omega_out})
         b->release();
     for (auto& e : h->ev)
         if (e) cudaEventDestroy(e);
@@ -367,6 +373,35 @@ int gwb200_sigma_c(gwb200_handle* h, const double* omega, const double* weight, 
         GWB_CUDA(cudaMemcpyAsync(sigma_out, h->sigma.p, sizeof(double) * 2 * (size_t)h->nmo * nfreq,
                                  cudaMemcpyDeviceToHost, h->stream));
         GWB_CUDA(cudaStreamSynchronize(h->stream));
+    });
+}
+
+int gwb200_sigma_c_shard(gwb200_handle* h, const double* omega, const double* weight, int64_t nfreq, int64_t f_begin,
+                         int64_t f_end, const int64_t* states, int64_t nstates, double eta, int precision,
+                         double* sigma_partial_out, gwb200_stats* stats) {
+    return guarded([&] {
+        check_system(h);
+        if (!omega || !weight || !sigma_partial_out) fail(GWB200_BAD_ARGUMENT, "null input or output array");
+        if (nfreq <= 0 || f_begin < 0 || f_end > nfreq || f_begin > f_end)
+            fail(GWB200_BAD_SHAPE, "frequency shard must satisfy 0 <= f_begin <= f_end <= nfreq");
+        gwb200_stats local{};
+        gwb200_stats* st = stats ? stats : &local;
+        *st = gwb200_stats{};
+        const size_t sig_bytes = sizeof(double) * 2 * (size_t)h->nmo * nfreq;
+        if (f_begin == f_end) {  // empty shard: contributes nothing
+            std::fill(sigma_partial_out, sigma_partial_out + 2 * (size_t)h->nmo * nfreq, 0.0);
+            return;
+        }
+        cudaStream_t s = h->stream;
+        h->omega_out.ensure(sizeof(double) * nfreq);
+        GWB_CUDA(cudaMemcpyAsync(h->omega_out.p, omega, sizeof(double) * nfreq, cudaMemcpyHostToDevice, s));
+        compute_forms(h, omega + f_begin, f_end - f_begin, states, nstates, eta, precision, st, weight + f_begin);
+        contract_on_device(h, f_end - f_begin, nstates, st, h->omega_out.as<double>(), nfreq);
+        finish_forms(h, st);
+        st->device_ms_contract = elapsed(h->ev[2], h->ev[3]);
+        st->device_ms_total = elapsed(h->ev[0], h->ev[3]);
+        GWB_CUDA(cudaMemcpyAsync(sigma_partial_out, h->sigma.p, sig_bytes, cudaMemcpyDeviceToHost, s));
+        GWB_CUDA(cudaStreamSynchronize(s));
     });
 }
 

@@ -113,9 +113,12 @@ int launch_build_tall(const TallGeometry& g, const double* v, const double* xt, 
 // blocks); returns launches issued.
 int launch_factor_chunk(const TallGeometry& g, int64_t nf, double* a, double* linv, double* qacc,
                         unsigned long long* err_pivot, cudaStream_t s, UpdateProfiler* prof);
-int launch_sigma_contract(const double* qall, int64_t nfreq, int64_t nstates, int64_t nmo, int64_t ldq,
-                          const int64_t* states, const double* mo, double fermi, const double* omega,
-                          const double* weight, double* sigma, cudaStream_t s);
+// Contraction of the screened forms of nf_int integration frequencies onto nf_out output
+// frequencies (the full grid; a shard of integration frequencies gives a partial sum).
+int launch_sigma_contract(const double* qall, int64_t nf_int, int64_t nstates, int64_t nmo, int64_t ldq,
+                          const int64_t* states, const double* mo, double fermi, const double* omega_int,
+                          const double* weight_int, const double* omega_out, int64_t nf_out, double* sigma,
+                          cudaStream_t s);
 int launch_fill(double* p, double v, int64_t n, cudaStream_t s);
 // scratch: qp_scratch_bytes(nfreq, nstates) bytes of device memory
 size_t qp_scratch_bytes(int64_t nfreq, int64_t nstates);

@@ -168,25 +168,29 @@ __global__ void k_pade_sweep(const double* __restrict__ sigma_row, const double*
 // Sigma_c(p_s, i w_n) = -(1/pi) sum_{f', k} w_{f'} g(k, n, f') q[f', s, k], with
 // g = a / (a^2 + w_{f'}^2), a = i w_n + E_F - e_k, and q = x^T W_c x <= 0 the screened forms
 // (the reference's accumulation, src/gw/sigma_c_driver.cpp:154-168, with W_c hoisted out of
-// the loop over w_n).  One block per (n, s); fixed-shape tree reduction (deterministic).
-__global__ void __launch_bounds__(256) k_sigma_contract(const double* __restrict__ qall, int nfreq, int nmo,
+// the loop over w_n).  The integration frequencies f' (omega_int, weight_int, rows of qall) may be
+// a shard of the output grid (omega_out): the shards' results then add up to the full sum.
+// One block per (n, s); fixed-shape tree reduction (deterministic).
+__global__ void __launch_bounds__(256) k_sigma_contract(const double* __restrict__ qall, int nf_int, int nmo,
                                                         int64_t ldq, const int64_t* __restrict__ states,
                                                         const double* __restrict__ mo, double fermi,
-                                                        const double* __restrict__ omega,
-                                                        const double* __restrict__ weight, double* __restrict__ sigma) {
+                                                        const double* __restrict__ omega_int,
+                                                        const double* __restrict__ weight_int,
+                                                        const double* __restrict__ omega_out, int nf_out,
+                                                        double* __restrict__ sigma) {
     const int fn = blockIdx.x, s = blockIdx.y;
-    const double wn = omega[fn];
+    const double wn = omega_out[fn];
     double sr = 0.0, si = 0.0;
-    const int total = nfreq * nmo;
+    const int total = nf_int * nmo;
     for (int idx = threadIdx.x; idx < total; idx += blockDim.x) {
         const int fp = idx / nmo, k = idx % nmo;
         const double q = qall[(size_t)fp * ldq + (size_t)s * nmo + k];
         const double ar = fermi - mo[k], ai = wn;
-        const double wp = omega[fp];
+        const double wp = omega_int[fp];
         const double dr = ar * ar - ai * ai + wp * wp, di = 2.0 * ar * ai;
         const double inv = 1.0 / (dr * dr + di * di);
         const double gr = (ar * dr + ai * di) * inv, gi = (ai * dr - ar * di) * inv;
-        const double scale = -weight[fp] * q;
+        const double scale = -weight_int[fp] * q;
         sr = fma(gr, scale, sr);
         si = fma(gi, scale, si);
     }
@@ -204,8 +208,8 @@ __global__ void __launch_bounds__(256) k_sigma_contract(const double* __restrict
     if (threadIdx.x == 0) {
         const size_t p = (size_t)states[s];
         const double inv_pi = 1.0 / 3.141592653589793238462643383279502884;
-        sigma[2 * (p * nfreq + fn)] = red[0][0] * inv_pi;
-        sigma[2 * (p * nfreq + fn) + 1] = red[1][0] * inv_pi;
+        sigma[2 * (p * nf_out + fn)] = red[0][0] * inv_pi;
+        sigma[2 * (p * nf_out + fn) + 1] = red[1][0] * inv_pi;
     }
 }
 
@@ -231,11 +235,13 @@ __global__ void k_dmma_probe(double* out, int iters) {
 
 } // namespace
 
-int launch_sigma_contract(const double* qall, int64_t nfreq, int64_t nstates, int64_t nmo, int64_t ldq,
-                          const int64_t* states, const double* mo, double fermi, const double* omega,
-                          const double* weight, double* sigma, cudaStream_t s) {
-    dim3 grid((unsigned)nfreq, (unsigned)nstates);
-    k_sigma_contract<<<grid, 256, 0, s>>>(qall, (int)nfreq, (int)nmo, ldq, states, mo, fermi, omega, weight, sigma);
+int launch_sigma_contract(const double* qall, int64_t nf_int, int64_t nstates, int64_t nmo, int64_t ldq,
+                          const int64_t* states, const double* mo, double fermi, const double* omega_int,
+                          const double* weight_int, const double* omega_out, int64_t nf_out, double* sigma,
+                          cudaStream_t s) {
+    dim3 grid((unsigned)nf_out, (unsigned)nstates);
+    k_sigma_contract<<<grid, 256, 0, s>>>(qall, (int)nf_int, (int)nmo, ldq, states, mo, fermi, omega_int, weight_int,
+                                          omega_out, (int)nf_out, sigma);
     GWB_LAUNCH("k_sigma_contract");
     return 1;
 }

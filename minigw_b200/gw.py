@@ -179,6 +179,18 @@ class B200Backend:
                                  _precision_code(precision), dptr(out), C.byref(stats)))
         return out, stats.as_dict()
 
+    def sigma_c_shard(self, omegas, weights, f_begin: int, f_end: int, states, eta: float = 0.0, precision="fp64"):
+        """Partial Sigma_c from the integration frequencies [f_begin, f_end) onto the whole grid."""
+        om = np.ascontiguousarray(omegas, dtype=np.float64)
+        w = np.ascontiguousarray(weights, dtype=np.float64)
+        st = np.ascontiguousarray(states, dtype=np.int64)
+        out = np.zeros((self.nmo, om.shape[0]), dtype=np.complex128)
+        stats = Stats()
+        check(lib.gwb200_sigma_c_shard(self._h, dptr(om), dptr(w), om.shape[0], int(f_begin), int(f_end), iptr(st),
+                                       st.shape[0], float(eta), _precision_code(precision), dptr(out),
+                                       C.byref(stats)))
+        return out, stats.as_dict()
+
     def run_g0w0(self, nfreq: int, npade: int, states, eta: float = 0.0, precision="fp64"):
         """Grid, Sigma_c(iw), Sigma_x diagonal and QP energies in one device call."""
         st = np.ascontiguousarray(states, dtype=np.int64)
