@@ -196,3 +196,16 @@ def test_synthetic_generator_contract():
     assert WORKLOADS["cfg3"].nph == 5100 and WORKLOADS["cfg3"].ncols == 2000
     assert WORKLOADS["cfg2"].nph == 2000 and WORKLOADS["cfg2"].ncols == 720
     assert WORKLOADS["cfg1"].nph == 95 and WORKLOADS["cfg1"].ncols == 24
+
+
+def test_reference_executable_with_b200_fails_loudly_without_gpu(tmp_path):
+    import torch
+
+    exe = ROOT / "oracle" / "_ref" / "gw_ref_b200"
+    if not exe.exists():
+        pytest.skip("the reference executable with the b200 backend was not built")
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    r = subprocess.run([str(exe), "--linalg-backend", "b200", "--input-dir", str(GOLDEN / "h2o"), "--output-dir",
+                        str(tmp_path)], capture_output=True, text=True, timeout=120)
+    assert r.returncode != 0 and "CUDA" in r.stderr

@@ -265,3 +265,25 @@ def test_run_g0w0_equals_separate_calls(backend, cfg1_input):
     np.testing.assert_array_equal(r["qp"][states], qp[states])
     assert np.all(np.isnan(np.delete(r["qp"], states)))
     assert r["stats"]["kernel_launches"] > 0
+
+
+REF_B200 = ROOT / "oracle" / "_ref" / "gw_ref_b200"
+
+
+@pytest.mark.skipif(not REF_B200.exists(), reason="the reference executable with the b200 backend was not built")
+def test_reference_executable_with_b200_backend(tmp_path):
+    """The reference's own `gw` (its main, CLI, backend factory, run_g0w0 and writers) with the
+    b200 backend registered as INTEGRATION.md describes: `--linalg-backend b200` on the H2O input
+    reproduces the reference's committed regression outputs."""
+    out = tmp_path / "out"
+    r = subprocess.run([str(REF_B200), "--linalg-backend", "b200", "--input-dir", str(GOLDEN / "h2o"), "--output-dir",
+                        str(out)], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    assert "Using the b200 device backend" in (out / "gw.out").read_text()
+    sig = read_complex_lines(out / "E_c_before_Pade.out")
+    gold = read_complex_lines(GOLDEN / "h2o" / "E_c_before_Pade.out")
+    assert components_close(sig, gold, 1e-8)
+    row = read_summary_row(out / "gw.out", 5)
+    grow = read_summary_row(GOLDEN / "h2o" / "gw.out", 5)
+    for key in grow:
+        assert abs(row[key] - grow[key]) <= 1e-5 * abs(grow[key]) + 1e-4, key
