@@ -29,8 +29,8 @@ extern "C" {
 typedef enum gwb200_status {
     GWB200_OK = 0,
     GWB200_BAD_SHAPE = 1,        /* nmo/nocc/nfreq/state out of range (reference: std::runtime_error) */
-    GWB200_ETA_NONZERO = 2,      /* eta != 0: eps(iw) is not SPD; this backend requires eta == 0 */
-    GWB200_NOT_SPD = 3,          /* Cholesky pivot <= 0; gwb200_stats.info = 1-based pivot row */
+    GWB200_ETA_NONZERO = 2,      /* eta != 0 where only the real (eta == 0) form exists (real forms, no-alloc entry) */
+    GWB200_NOT_SPD = 3,          /* Cholesky pivot <= 0 (eta == 0) or ~0 (eta != 0); stats.info = 1-based row */
     GWB200_OOM = 4,              /* device allocation failed */
     GWB200_DEVICE_TIMEOUT = 5,   /* a bounded device wait gave up */
     GWB200_CUDA_ERROR = 6,       /* CUDA runtime error, or no usable sm_100 device */
@@ -99,7 +99,8 @@ int gwb200_load_system(gwb200_handle* h, int64_t nmo, int64_t nocc, const double
 
 /* Correlation self-energy Sigma_c(i w_n) on the imaginary grid for the requested states.
  * sigma_out is nmo x nfreq complex, row-major (gw::MatrixComplex); rows of states not
- * requested are set to zero.  eta must be 0 (GWB200_ETA_NONZERO otherwise).
+ * requested are set to zero.  eta == 0: real SPD Cholesky of eps = I + D^1/2 V D^1/2;
+ * eta != 0: complex symmetric L L^T of I - S V S with S = diag(Pi0)^1/2 (no pivoting).
  * Replaces: gw::compute_sigma_c_with_backend (src/gw/sigma_c_driver.cpp:451-592) with the
  * device branch (:471-514): compute_w_c (src/workspace/device_screening_workspace.cu:337-374),
  * fill_panel (src/workspace/device_pq_ph_panel.cu:284), quadratic_forms_panel (:376-417) and the
@@ -130,11 +131,17 @@ int gwb200_run_g0w0(gwb200_handle* h, int64_t nfreq, int64_t npade, const int64_
                     double eta, int precision, double* omega_out, double* weight_out, double* sigma_out,
                     double* sigma_x_out, double* qp_out, gwb200_stats* stats);
 
-/* Screened quadratic forms Q[f, s, k] = x_{p_s k}^T W_c(i w_f) x_{p_s k} (real, <= 0), layout
- * [nfreq][nstates][nmo].  The per-frequency quantity the reference computes as
+/* Screened quadratic forms Q[f, s, k] = x_{p_s k}^T W_c(i w_f) x_{p_s k} (real, <= 0) at eta == 0
+ * (GWB200_ETA_NONZERO otherwise), layout [nfreq][nstates][nmo].  The per-frequency quantity the reference computes as
  * quadratic_forms_panel (src/workspace/screening_workspace.cpp:69-102); exported for checking. */
 int gwb200_screened_forms(gwb200_handle* h, const double* omega, int64_t nfreq, const int64_t* states,
                           int64_t nstates, double eta, int precision, double* q_out, gwb200_stats* stats);
+
+/* Screened quadratic forms for any eta as complex numbers (layout [nfreq][nstates][nmo], interleaved
+ * re/im): x^T W_c x of the reference's quadratic_forms_panel (src/workspace/screening_workspace.cpp:69-102).
+ * At eta == 0 the imaginary parts are zero. */
+int gwb200_screened_forms_complex(gwb200_handle* h, const double* omega, int64_t nfreq, const int64_t* states,
+                                  int64_t nstates, double eta, double* q_out, gwb200_stats* stats);
 
 /* Diagonal of the exchange self-energy, Sigma_x[p,p] = -sum_{i<nocc} (p i | p i), out[nmo].
  * Replaces: gw::calculate_exchange (src/gw/sigma.cpp:22-39) (only its diagonal is consumed,

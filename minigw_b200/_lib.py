@@ -34,7 +34,7 @@ MIXED = 1
 EXPORTS = (
     "gwb200_last_error", "gwb200_version", "gwb200_create", "gwb200_destroy", "gwb200_set_stream",
     "gwb200_load_system", "gwb200_run_g0w0", "gwb200_sigma_c_shard",
-    "gwb200_sigma_c", "gwb200_screened_forms", "gwb200_sigma_x_diag", "gwb200_qp", "gwb200_pade_sweep",
+    "gwb200_sigma_c", "gwb200_screened_forms", "gwb200_screened_forms_complex", "gwb200_sigma_x_diag", "gwb200_qp", "gwb200_pade_sweep",
     "gwb200_grid", "gwb200_read_input_h5", "gwb200_screened_forms_noalloc", "gwb200_fp64_peak_tflops",
 )
 
@@ -95,6 +95,8 @@ def _load() -> C.CDLL:
                                     _dp, _dp, C.POINTER(Stats)]
     lib.gwb200_screened_forms.argtypes = [_vp, _dp, C.c_int64, _ip, C.c_int64, C.c_double, C.c_int, _dp,
                                           C.POINTER(Stats)]
+    lib.gwb200_screened_forms_complex.argtypes = [_vp, _dp, C.c_int64, _ip, C.c_int64, C.c_double, _dp,
+                                                  C.POINTER(Stats)]
     lib.gwb200_sigma_x_diag.argtypes = [_vp, _dp]
     lib.gwb200_qp.argtypes = [_vp, _dp, C.c_int64, _dp, C.c_int64, _ip, C.c_int64, _dp]
     lib.gwb200_pade_sweep.argtypes = [_vp, _dp, C.c_int64, _dp, C.c_int64, C.c_int64, C.c_double, C.c_double,

@@ -68,6 +68,7 @@ struct gwb200_handle {
     int64_t nmo = 0, nocc = 0, n = 0;
     double fermi = 0.0;
     bool bad_gap = false;
+    bool complex_forms = false;  // the last compute_forms ran the eta != 0 (complex) path
     DevBuf pqo, xdiag, mo, vxc_diag, delta, v, sigx, flag;  // pqo: the (pq|o.) block of the ERI
     // per-call workspaces (grow-only, reused across calls)
     DevBuf xt, dvec, a, linv, qacc, qall, sigma, omega, weight, states, err, qp, qp_scratch, omega_out;
@@ -107,12 +108,14 @@ void compute_forms(gwb200_handle* h, const double* omega, int64_t nfreq, const i
     if (!omega) fail(GWB200_BAD_ARGUMENT, "null omega");
     if (nfreq <= 0) fail(GWB200_BAD_SHAPE, "--freq-points must be positive");
     check_states(h, states, nstates);
-    if (eta != 0.0)
-        fail(GWB200_ETA_NONZERO, "the b200 backend factors the SPD form of eps(iw) and requires eta == 0");
+    if (!std::isfinite(eta)) fail(GWB200_BAD_ARGUMENT, "non-finite eta");
     if (precision != GWB200_FP64 && precision != GWB200_MIXED) fail(GWB200_BAD_ARGUMENT, "unknown precision");
     if (precision == GWB200_MIXED) fail(GWB200_BAD_ARGUMENT, "the mixed-precision form is not built in this library");
-    if (h->bad_gap)
+    const bool cplx = eta != 0.0;  // eta != 0: complex symmetric factorisation
+    if (!cplx && h->bad_gap)
         fail(GWB200_NONPOSITIVE_GAP, "some e_a - e_i <= 0: chi0(iw) is not negative definite, eps(iw) is not SPD");
+    h->complex_forms = cplx;
+    const int planes = cplx ? 2 : 1;
     for (int64_t f = 0; f < nfreq; ++f)
         if (!(std::isfinite(omega[f]))) fail(GWB200_BAD_ARGUMENT, "non-finite frequency");
 
@@ -124,7 +127,7 @@ void compute_forms(gwb200_handle* h, const double* omega, int64_t nfreq, const i
     h->omega.ensure(sizeof(double) * nfreq);
     h->states.ensure(sizeof(int64_t) * nstates);
     h->xt.ensure(sizeof(double) * (size_t)m * h->n);
-    h->qall.ensure(sizeof(double) * (size_t)nfreq * g.m_pad);
+    h->qall.ensure(sizeof(double) * planes * (size_t)nfreq * g.m_pad);
     h->err.ensure(sizeof(unsigned long long));
     GWB_CUDA(cudaMemcpyAsync(h->omega.p, omega, sizeof(double) * nfreq, cudaMemcpyHostToDevice, s));
     GWB_CUDA(cudaMemcpyAsync(h->states.p, states, sizeof(int64_t) * nstates, cudaMemcpyHostToDevice, s));
@@ -135,7 +138,7 @@ void compute_forms(gwb200_handle* h, const double* omega, int64_t nfreq, const i
     GWB_CUDA(cudaMemsetAsync(h->err.p, 0xFF, sizeof(unsigned long long), s));
 
     // Frequency chunk size from the HBM budget: tall matrices + scale vectors + 64x64 inverses.
-    const size_t per_freq = sizeof(double) * ((size_t)g.stride + g.n_pad + kNb * kNb + g.m_pad);
+    const size_t per_freq = sizeof(double) * planes * ((size_t)g.stride + g.n_pad + kNb * kNb + g.m_pad);
     size_t free_b = 0, total_b = 0;
     GWB_CUDA(cudaMemGetInfo(&free_b, &total_b));
     const size_t have = h->a.bytes + h->dvec.bytes + h->linv.bytes + h->qacc.bytes;
@@ -147,10 +150,10 @@ void compute_forms(gwb200_handle* h, const double* omega, int64_t nfreq, const i
         if (cap > 0) fc = std::min<int64_t>(fc, cap);
     }
     if ((size_t)fc * per_freq > free_b + have) fail(GWB200_OOM, "not enough device memory for one frequency of eps(iw)");
-    h->a.ensure(sizeof(double) * (size_t)fc * g.stride);
-    h->dvec.ensure(sizeof(double) * (size_t)fc * g.n_pad);
-    h->linv.ensure(sizeof(double) * (size_t)fc * kNb * kNb);
-    h->qacc.ensure(sizeof(double) * (size_t)fc * g.m_pad);
+    h->a.ensure(sizeof(double) * planes * (size_t)fc * g.stride);
+    h->dvec.ensure(sizeof(double) * planes * (size_t)fc * g.n_pad);
+    h->linv.ensure(sizeof(double) * planes * (size_t)fc * kNb * kNb);
+    h->qacc.ensure(sizeof(double) * planes * (size_t)fc * g.m_pad);
 
     GWB_CUDA(cudaEventRecord(h->ev[0], s));
     launches += launch_gather_panel(h->pqo.as<double>(), h->nmo, h->nocc, h->states.as<int64_t>(), nstates,
@@ -161,6 +164,17 @@ void compute_forms(gwb200_handle* h, const double* omega, int64_t nfreq, const i
     int64_t chunks = 0;
     for (int64_t f0 = 0; f0 < nfreq; f0 += fc) {
         const int64_t nf = std::min(fc, nfreq - f0);
+        if (cplx) {
+            double* a_re = h->a.as<double>();
+            launches += launch_factor_chunk_c(g, nf, h->delta.as<double>(), h->omega.as<double>() + f0, eta,
+                                              h->v.as<double>(), h->xt.as<double>(), a_re, a_re + (size_t)nf * g.stride,
+                                              h->dvec.as<double>(), h->linv.as<double>(), h->qacc.as<double>(),
+                                              h->err.as<unsigned long long>(), s);
+            launches += launch_forms_out_c(h->qacc.as<double>(), nf, m, g.m_pad,
+                                           h->qall.as<double>() + f0 * 2 * g.m_pad, g.m_pad, s);
+            ++chunks;
+            continue;
+        }
         launches += launch_scale_vectors(h->delta.as<double>(), g.n, g.n_pad, h->omega.as<double>() + f0, nf,
                                          h->dvec.as<double>(), s);
         launches += launch_build_tall(g, h->v.as<double>(), h->xt.as<double>(), h->dvec.as<double>(), nf,
@@ -213,10 +227,16 @@ void contract_on_device(gwb200_handle* h, int64_t nf_int, int64_t nstates, gwb20
     const size_t sig_bytes = sizeof(double) * 2 * (size_t)h->nmo * nf_out;
     h->sigma.ensure(sig_bytes);
     GWB_CUDA(cudaMemsetAsync(h->sigma.p, 0, sig_bytes, s));
-    st->kernel_launches += launch_sigma_contract(h->qall.as<double>(), nf_int, nstates, h->nmo, ldq,
-                                                 h->states.as<int64_t>(), h->mo.as<double>(), h->fermi,
-                                                 h->omega.as<double>(), h->weight.as<double>(), omega_out_dev, nf_out,
-                                                 h->sigma.as<double>(), s);
+    if (h->complex_forms)
+        st->kernel_launches += launch_sigma_contract_c(h->qall.as<double>(), nf_int, nstates, h->nmo, ldq,
+                                                       h->states.as<int64_t>(), h->mo.as<double>(), h->fermi,
+                                                       h->omega.as<double>(), h->weight.as<double>(), omega_out_dev,
+                                                       nf_out, h->sigma.as<double>(), s);
+    else
+        st->kernel_launches += launch_sigma_contract(h->qall.as<double>(), nf_int, nstates, h->nmo, ldq,
+                                                     h->states.as<int64_t>(), h->mo.as<double>(), h->fermi,
+                                                     h->omega.as<double>(), h->weight.as<double>(), omega_out_dev,
+                                                     nf_out, h->sigma.as<double>(), s);
     GWB_CUDA(cudaEventRecord(h->ev[3], s));
 }
 
@@ -344,6 +364,8 @@ int gwb200_screened_forms(gwb200_handle* h, const double* omega, int64_t nfreq, 
     return guarded([&] {
         check_system(h);
         if (!q_out) fail(GWB200_BAD_ARGUMENT, "null output array");
+        if (eta != 0.0)
+            fail(GWB200_ETA_NONZERO, "real screened forms exist only at eta == 0; use gwb200_screened_forms_complex");
         gwb200_stats local{};
         gwb200_stats* st = stats ? stats : &local;
         *st = gwb200_stats{};
@@ -354,6 +376,35 @@ int gwb200_screened_forms(gwb200_handle* h, const double* omega, int64_t nfreq, 
         GWB_CUDA(cudaMemcpy2DAsync(q_out, sizeof(double) * m, h->qall.p, sizeof(double) * ldq, sizeof(double) * m,
                                    (size_t)nfreq, cudaMemcpyDeviceToHost, h->stream));
         GWB_CUDA(cudaStreamSynchronize(h->stream));
+    });
+}
+
+int gwb200_screened_forms_complex(gwb200_handle* h, const double* omega, int64_t nfreq, const int64_t* states,
+                                  int64_t nstates, double eta, double* q_out, gwb200_stats* stats) {
+    return guarded([&] {
+        check_system(h);
+        if (!q_out) fail(GWB200_BAD_ARGUMENT, "null output array");
+        gwb200_stats local{};
+        gwb200_stats* st = stats ? stats : &local;
+        *st = gwb200_stats{};
+        compute_forms(h, omega, nfreq, states, nstates, eta, GWB200_FP64, st);
+        finish_forms(h, st);
+        const int64_t m = nstates * h->nmo;
+        const int64_t ldq = make_geometry(h->n, m).m_pad;
+        if (h->complex_forms) {
+            GWB_CUDA(cudaMemcpy2DAsync(q_out, 2 * sizeof(double) * m, h->qall.p, 2 * sizeof(double) * ldq,
+                                       2 * sizeof(double) * m, (size_t)nfreq, cudaMemcpyDeviceToHost, h->stream));
+            GWB_CUDA(cudaStreamSynchronize(h->stream));
+        } else {  // eta == 0: real forms, imaginary parts zero
+            std::vector<double> re((size_t)nfreq * m);
+            GWB_CUDA(cudaMemcpy2DAsync(re.data(), sizeof(double) * m, h->qall.p, sizeof(double) * ldq,
+                                       sizeof(double) * m, (size_t)nfreq, cudaMemcpyDeviceToHost, h->stream));
+            GWB_CUDA(cudaStreamSynchronize(h->stream));
+            for (size_t i = 0; i < re.size(); ++i) {
+                q_out[2 * i] = re[i];
+                q_out[2 * i + 1] = 0.0;
+            }
+        }
     });
 }
 

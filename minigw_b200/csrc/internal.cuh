@@ -132,6 +132,17 @@ int launch_pade_sweep(const double* sigma_row, const double* omega, int64_t nfre
 int launch_negate_copy(const double* qacc, int64_t nf, int64_t m, int64_t ldq_in, double* q_out, int64_t ldq_out,
                        cudaStream_t s);
 double measure_fp64_peak_tflops(cudaStream_t s);
+// kernels_c64.cu: eta != 0 (complex symmetric M = I - S V S, S = diag(Pi0)^1/2).  Planes a_re/a_im
+// of geometry g; svec 2*n_pad, linv 2*64*64, qacc 2*m_pad doubles per frequency.
+int launch_factor_chunk_c(const TallGeometry& g, int64_t nf, const double* delta, const double* omega, double eta,
+                          const double* v, const double* xt, double* a_re, double* a_im, double* svec, double* linv,
+                          double* qacc, unsigned long long* err_pivot, cudaStream_t s);
+int launch_forms_out_c(const double* qacc, int64_t nf, int64_t m, int64_t ldq, double* q_out, int64_t ldq_out,
+                       cudaStream_t s);
+int launch_sigma_contract_c(const double* qall, int64_t nf_int, int64_t nstates, int64_t nmo, int64_t ldq,
+                            const int64_t* states, const double* mo, double fermi, const double* omega_int,
+                            const double* weight_int, const double* omega_out, int64_t nf_out, double* sigma,
+                            cudaStream_t s);
 // noalloc.cu
 size_t noalloc_scratch_bytes();
 void screened_forms_noalloc(int64_t n, int64_t m, const double* d_v, const double* d_xt, const double* d_delta,

@@ -212,6 +212,15 @@ class B200Backend:
                                         _precision_code(precision), dptr(out), C.byref(stats)))
         return out, stats.as_dict()
 
+    def screened_forms_complex(self, omegas, states, eta: float = 0.0):
+        om = np.ascontiguousarray(omegas, dtype=np.float64)
+        st = np.ascontiguousarray(states, dtype=np.int64)
+        out = np.zeros((om.shape[0], st.shape[0], self.nmo), dtype=np.complex128)
+        stats = Stats()
+        check(lib.gwb200_screened_forms_complex(self._h, dptr(om), om.shape[0], iptr(st), st.shape[0], float(eta),
+                                                dptr(out), C.byref(stats)))
+        return out, stats.as_dict()
+
     def sigma_x_diag(self) -> np.ndarray:
         out = np.zeros(self.nmo)
         check(lib.gwb200_sigma_x_diag(self._h, dptr(out)))

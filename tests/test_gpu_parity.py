@@ -168,7 +168,7 @@ def test_error_statuses(backend, cfg1_input):
             backend.sigma_c(om, w, bad_states)
         assert e.value.status == "GWB200_BAD_SHAPE"
     with pytest.raises(GwB200Error) as e:
-        backend.sigma_c(om, w, [4], eta=1e-3)
+        backend.screened_forms(om, [4], eta=1e-3)  # real forms exist only at eta == 0
     assert e.value.status == "GWB200_ETA_NONZERO"
     # a virtual level below an occupied one: chi0 is not negative definite
     inp = make_input(10, 3, seed=2)
@@ -287,3 +287,45 @@ def test_reference_executable_with_b200_backend(tmp_path):
     grow = read_summary_row(GOLDEN / "h2o" / "gw.out", 5)
     for key in grow:
         assert abs(row[key] - grow[key]) <= 1e-5 * abs(grow[key]) + 1e-4, key
+
+
+@pytest.mark.parametrize("eta", [1e-3, 0.05])
+@pytest.mark.parametrize("nmo,nocc,states,nfreq", [
+    (9, 3, [1, 2, 4], 10),       # one block
+    (30, 7, [5, 6, 7, 8], 16),   # n = 161: three blocks, ragged
+])
+def test_eta_nonzero_against_oracle(backend, oracle_lib, eta, nmo, nocc, states, nfreq):
+    """eta != 0: complex symmetric factorisation against the oracle's complex Gauss-Jordan path
+    (pinned to the live reference on CPU, tests/test_oracle.py)."""
+    from minigw_b200.synthetic import make_input
+
+    inp = make_input(nmo, nocc, seed=nmo + 1)
+    om, w = oracle_lib.grid(nfreq)
+    backend.load_system(inp)
+    sig, _ = backend.sigma_c(om, w, states, eta=eta)
+    osig, oq = oracle_lib.sigma_c(inp, om, w, states, eta=eta)
+    assert np.abs(sig - osig).max() <= SIGMA_ATOL
+    q, _ = backend.screened_forms_complex(om, states, eta=eta)
+    assert np.abs(oq.imag).max() > 0  # genuinely complex
+    assert np.abs(q - oq).max() <= 1e-11 * max(1.0, np.abs(oq).max())
+
+
+def test_eta_nonzero_h2o_end_to_end(backend, oracle_lib, h2o_input):
+    from minigw_b200 import GwSettings, run_g0w0
+
+    res = run_g0w0(h2o_input, GwSettings(eta=0.01), backend=backend)
+    om, w = oracle_lib.grid(200)
+    osig, _ = oracle_lib.sigma_c(h2o_input, om, w, [4], eta=0.01)
+    assert np.abs(res.sigma_c_im_points - osig).max() <= SIGMA_ATOL
+    assert np.isfinite(res.qp_energy[4])
+
+
+def test_complex_path_continuous_at_eta_zero(backend, cfg1_input):
+    """The complex path at eta -> 0 meets the real SPD path (S = i D^1/2)."""
+    from minigw_b200 import generate_transformed_legendre_grid
+
+    om, w = generate_transformed_legendre_grid(24)
+    backend.load_system(cfg1_input)
+    real, _ = backend.sigma_c(om, w, [4])
+    tiny, _ = backend.sigma_c(om, w, [4], eta=1e-13)
+    assert np.abs(tiny - real).max() <= 1e-9 * np.abs(real).max()

@@ -150,3 +150,18 @@ def test_live_reference_grid_bit_exact():
         a, b = o.grid(n), ref.grid(n)
         np.testing.assert_array_equal(a[0], b[0])
         np.testing.assert_array_equal(a[1], b[1])
+
+
+@pytest.mark.skipif(not __import__("oracle").Ref.available, reason="oracle/_ref not built (no reference tree)")
+def test_live_reference_bit_exact_with_eta():
+    import oracle
+
+    o = oracle.Oracle()
+    ref = oracle.Ref()
+    inp = _random_system(9, 3, seed=8)
+    states = [1, 3, 5]
+    r_ref = ref.g0w0(inp, 10, 6, states, backend="reference", eta=0.02)
+    om, w = o.grid(10)
+    sig, q = o.sigma_c(inp, om, w, states, eta=0.02)
+    np.testing.assert_array_equal(sig, r_ref["sigma"])
+    assert np.abs(q.imag).max() > 0
