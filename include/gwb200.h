@@ -42,7 +42,9 @@ typedef enum gwb200_status {
 
 typedef enum gwb200_precision {
     GWB200_FP64 = 0,             /* plain form: FP64 throughout (the drop-in) */
-    GWB200_MIXED = 1             /* mixed form (FP32 factor + FP64 correction) */
+    GWB200_MIXED = 1             /* mixed form (eta == 0): FP32 tall matrices, FP64 diagonal blocks, 3xTF32
+                                  * tensor-core panel solves and updates, FP64 norms / contraction / Pade /
+                                  * QP; FP32-level error, no FP64 refinement */
 } gwb200_precision;
 
 typedef struct gwb200_stats {

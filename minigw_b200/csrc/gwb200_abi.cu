@@ -38,6 +38,28 @@ struct DevBuf {
     }
 };
 
+// Grow-only pinned host buffer: small per-call uploads/downloads go through it, so they are true
+// asynchronous DMA (a pageable copy is staged by the driver and, for uploads, waits for the stream).
+struct PinnedBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+    void ensure(size_t want) {
+        if (want <= bytes) return;
+        release();
+        GWB_CUDA(cudaMallocHost(&p, want));
+        bytes = want;
+    }
+    void release() {
+        if (p) cudaFreeHost(p);
+        p = nullptr;
+        bytes = 0;
+    }
+    template <class T>
+    T* as() const {
+        return static_cast<T*>(p);
+    }
+};
+
 template <class F>
 int guarded(F&& body) {
     try {
@@ -72,6 +94,10 @@ struct gwb200_handle {
     DevBuf pqo, xdiag, mo, vxc_diag, delta, v, sigx, flag;  // pqo: the (pq|o.) block of the ERI
     // per-call workspaces (grow-only, reused across calls)
     DevBuf xt, dvec, a, linv, qacc, qall, sigma, omega, weight, states, err, qp, qp_scratch, omega_out;
+    PinnedBuf stage_in, stage_out;
+    // cached frequency-chunk size for a repeated geometry (avoids cudaMemGetInfo per call)
+    int64_t chunk_key[4] = {-1, -1, -1, -1};
+    int64_t chunk_fc = 0;
 };
 
 namespace {
@@ -110,7 +136,8 @@ void compute_forms(gwb200_handle* h, const double* omega, int64_t nfreq, const i
     check_states(h, states, nstates);
     if (!std::isfinite(eta)) fail(GWB200_BAD_ARGUMENT, "non-finite eta");
     if (precision != GWB200_FP64 && precision != GWB200_MIXED) fail(GWB200_BAD_ARGUMENT, "unknown precision");
-    if (precision == GWB200_MIXED) fail(GWB200_BAD_ARGUMENT, "the mixed-precision form is not built in this library");
+    const bool mixed = precision == GWB200_MIXED;
+    if (mixed && eta != 0.0) fail(GWB200_BAD_ARGUMENT, "the mixed-precision form requires eta == 0");
     const bool cplx = eta != 0.0;  // eta != 0: complex symmetric factorisation
     if (!cplx && h->bad_gap)
         fail(GWB200_NONPOSITIVE_GAP, "some e_a - e_i <= 0: chi0(iw) is not negative definite, eps(iw) is not SPD");
@@ -129,30 +156,46 @@ void compute_forms(gwb200_handle* h, const double* omega, int64_t nfreq, const i
     h->xt.ensure(sizeof(double) * (size_t)m * h->n);
     h->qall.ensure(sizeof(double) * planes * (size_t)nfreq * g.m_pad);
     h->err.ensure(sizeof(unsigned long long));
-    GWB_CUDA(cudaMemcpyAsync(h->omega.p, omega, sizeof(double) * nfreq, cudaMemcpyHostToDevice, s));
-    GWB_CUDA(cudaMemcpyAsync(h->states.p, states, sizeof(int64_t) * nstates, cudaMemcpyHostToDevice, s));
-    if (weight) {  // uploaded up front: a pageable upload later would wait for the whole screening
-        h->weight.ensure(sizeof(double) * nfreq);
-        GWB_CUDA(cudaMemcpyAsync(h->weight.p, weight, sizeof(double) * nfreq, cudaMemcpyHostToDevice, s));
+    {  // grid, states and (optionally) weights through the pinned staging buffer, all up front
+        const size_t nb_om = sizeof(double) * nfreq, nb_st = sizeof(int64_t) * nstates;
+        h->stage_in.ensure(2 * nb_om + nb_st);
+        char* st_p = h->stage_in.as<char>();
+        std::memcpy(st_p, omega, nb_om);
+        std::memcpy(st_p + nb_om, states, nb_st);
+        GWB_CUDA(cudaMemcpyAsync(h->omega.p, st_p, nb_om, cudaMemcpyHostToDevice, s));
+        GWB_CUDA(cudaMemcpyAsync(h->states.p, st_p + nb_om, nb_st, cudaMemcpyHostToDevice, s));
+        if (weight) {
+            h->weight.ensure(nb_om);
+            std::memcpy(st_p + nb_om + nb_st, weight, nb_om);
+            GWB_CUDA(cudaMemcpyAsync(h->weight.p, st_p + nb_om + nb_st, nb_om, cudaMemcpyHostToDevice, s));
+        }
     }
     GWB_CUDA(cudaMemsetAsync(h->err.p, 0xFF, sizeof(unsigned long long), s));
 
     // Frequency chunk size from the HBM budget: tall matrices + scale vectors + 64x64 inverses.
-    const size_t per_freq = sizeof(double) * planes * ((size_t)g.stride + g.n_pad + kNb * kNb + g.m_pad);
-    size_t free_b = 0, total_b = 0;
-    GWB_CUDA(cudaMemGetInfo(&free_b, &total_b));
-    const size_t have = h->a.bytes + h->dvec.bytes + h->linv.bytes + h->qacc.bytes;
-    const size_t budget = (size_t)((double)(free_b + have) * 0.85);
-    int64_t fc = (int64_t)std::min<size_t>((size_t)nfreq, std::max<size_t>(1, budget / per_freq));
+    const size_t per_freq = mixed ? sizeof(float) * ((size_t)g.stride + kNb * kNb) + sizeof(double) * (g.n_pad + g.m_pad)
+                                  : sizeof(double) * planes * ((size_t)g.stride + g.n_pad + kNb * kNb + g.m_pad);
     // GWB200_MAX_FREQ_CHUNK caps the chunk (tests use it to exercise the multi-chunk path).
-    if (const char* env = std::getenv("GWB200_MAX_FREQ_CHUNK")) {
-        const long long cap = std::atoll(env);
+    int64_t cap = 0;
+    if (const char* env = std::getenv("GWB200_MAX_FREQ_CHUNK")) cap = std::max<long long>(0, std::atoll(env));
+    const int64_t key[4] = {(int64_t)per_freq, nfreq, cap, (int64_t)g.stride};
+    int64_t fc;
+    if (std::equal(key, key + 4, h->chunk_key)) {
+        fc = h->chunk_fc;  // same geometry as the last call: its buffers are already sized
+    } else {
+        size_t free_b = 0, total_b = 0;
+        GWB_CUDA(cudaMemGetInfo(&free_b, &total_b));
+        const size_t have = h->a.bytes + h->dvec.bytes + h->linv.bytes + h->qacc.bytes;
+        const size_t budget = (size_t)((double)(free_b + have) * 0.85);
+        fc = (int64_t)std::min<size_t>((size_t)nfreq, std::max<size_t>(1, budget / per_freq));
         if (cap > 0) fc = std::min<int64_t>(fc, cap);
+        if ((size_t)fc * per_freq > free_b + have) fail(GWB200_OOM, "not enough device memory for one frequency of eps(iw)");
+        std::copy(key, key + 4, h->chunk_key);
+        h->chunk_fc = fc;
     }
-    if ((size_t)fc * per_freq > free_b + have) fail(GWB200_OOM, "not enough device memory for one frequency of eps(iw)");
-    h->a.ensure(sizeof(double) * planes * (size_t)fc * g.stride);
+    h->a.ensure((mixed ? sizeof(float) : sizeof(double) * planes) * (size_t)fc * g.stride);
     h->dvec.ensure(sizeof(double) * planes * (size_t)fc * g.n_pad);
-    h->linv.ensure(sizeof(double) * planes * (size_t)fc * kNb * kNb);
+    h->linv.ensure((mixed ? sizeof(float) : sizeof(double) * planes) * (size_t)fc * kNb * kNb);
     h->qacc.ensure(sizeof(double) * planes * (size_t)fc * g.m_pad);
 
     GWB_CUDA(cudaEventRecord(h->ev[0], s));
@@ -177,11 +220,18 @@ void compute_forms(gwb200_handle* h, const double* omega, int64_t nfreq, const i
         }
         launches += launch_scale_vectors(h->delta.as<double>(), g.n, g.n_pad, h->omega.as<double>() + f0, nf,
                                          h->dvec.as<double>(), s);
-        launches += launch_build_tall(g, h->v.as<double>(), h->xt.as<double>(), h->dvec.as<double>(), nf,
-                                      h->a.as<double>(), s);
         GWB_CUDA(cudaMemsetAsync(h->qacc.p, 0, sizeof(double) * (size_t)nf * g.m_pad, s));
-        launches += launch_factor_chunk(g, nf, h->a.as<double>(), h->linv.as<double>(), h->qacc.as<double>(),
-                                        h->err.as<unsigned long long>(), s, prof.enabled ? &prof : nullptr);
+        if (mixed) {
+            launches += launch_build_tall32(g, h->v.as<double>(), h->xt.as<double>(), h->dvec.as<double>(), nf,
+                                            h->a.as<float>(), s);
+            launches += launch_factor_chunk32(g, nf, h->a.as<float>(), h->linv.as<float>(), h->qacc.as<double>(),
+                                              h->err.as<unsigned long long>(), s, prof.enabled ? &prof : nullptr);
+        } else {
+            launches += launch_build_tall(g, h->v.as<double>(), h->xt.as<double>(), h->dvec.as<double>(), nf,
+                                          h->a.as<double>(), s);
+            launches += launch_factor_chunk(g, nf, h->a.as<double>(), h->linv.as<double>(), h->qacc.as<double>(),
+                                            h->err.as<unsigned long long>(), s, prof.enabled ? &prof : nullptr);
+        }
         launches += launch_negate_copy(h->qacc.as<double>(), nf, m, g.m_pad, h->qall.as<double>() + f0 * g.m_pad,
                                        g.m_pad, s);
         ++chunks;
@@ -199,9 +249,10 @@ void compute_forms(gwb200_handle* h, const double* omega, int64_t nfreq, const i
 }
 
 void finish_forms(gwb200_handle* h, gwb200_stats* st) {
-    unsigned long long piv = 0;
-    GWB_CUDA(cudaMemcpyAsync(&piv, h->err.p, sizeof(piv), cudaMemcpyDeviceToHost, h->stream));
+    h->stage_out.ensure(sizeof(unsigned long long));
+    GWB_CUDA(cudaMemcpyAsync(h->stage_out.p, h->err.p, sizeof(unsigned long long), cudaMemcpyDeviceToHost, h->stream));
     GWB_CUDA(cudaStreamSynchronize(h->stream));
+    const unsigned long long piv = *h->stage_out.as<unsigned long long>();
     if (piv != std::numeric_limits<unsigned long long>::max()) {
         if (st) st->info = (int64_t)piv;
         fail(GWB200_NOT_SPD, "eps(iw) is not positive definite: Cholesky pivot " + std::to_string(piv) + " <= 0");
@@ -291,6 +342,8 @@ int gwb200_destroy(gwb200_handle* h) {
     if (!h) return GWB200_OK;
     cudaSetDevice(h->device);
     if (h->stream) cudaStreamSynchronize(h->stream);
+    h->stage_in.release();
+    h->stage_out.release();
     for (DevBuf* b : {&h->pqo, &h->xdiag, &h->mo, &h->vxc_diag, &h->delta, &h->v, &h->sigx, &h->flag, &h->xt, &h->dvec, &h->a,
                       &h->linv, &h->qacc, &h->qall, &h->sigma, &h->omega, &h->weight, &h->states, &h->err, &h->qp,
                       &h->qp_scratch, &h->omega_out})
@@ -421,9 +474,11 @@ int gwb200_sigma_c(gwb200_handle* h, const double* omega, const double* weight, 
         finish_forms(h, st);
         st->device_ms_contract = elapsed(h->ev[2], h->ev[3]);
         st->device_ms_total = elapsed(h->ev[0], h->ev[3]);
-        GWB_CUDA(cudaMemcpyAsync(sigma_out, h->sigma.p, sizeof(double) * 2 * (size_t)h->nmo * nfreq,
-                                 cudaMemcpyDeviceToHost, h->stream));
+        const size_t nb_sig = sizeof(double) * 2 * (size_t)h->nmo * nfreq;
+        h->stage_out.ensure(nb_sig);
+        GWB_CUDA(cudaMemcpyAsync(h->stage_out.p, h->sigma.p, nb_sig, cudaMemcpyDeviceToHost, h->stream));
         GWB_CUDA(cudaStreamSynchronize(h->stream));
+        std::memcpy(sigma_out, h->stage_out.p, nb_sig);
     });
 }
 
@@ -476,12 +531,16 @@ int gwb200_run_g0w0(gwb200_handle* h, int64_t nfreq, int64_t npade, const int64_
         st->device_ms_contract = elapsed(h->ev[2], h->ev[3]);
         st->device_ms_total = elapsed(h->ev[0], h->ev[3]);
         cudaStream_t s = h->stream;
-        if (sigma_out)
-            GWB_CUDA(cudaMemcpyAsync(sigma_out, h->sigma.p, sizeof(double) * 2 * (size_t)h->nmo * nfreq,
-                                     cudaMemcpyDeviceToHost, s));
-        if (sigma_x_out) GWB_CUDA(cudaMemcpyAsync(sigma_x_out, h->sigx.p, sizeof(double) * h->nmo, cudaMemcpyDeviceToHost, s));
-        if (qp_out) GWB_CUDA(cudaMemcpyAsync(qp_out, h->qp.p, sizeof(double) * h->nmo, cudaMemcpyDeviceToHost, s));
+        const size_t nb_sig = sizeof(double) * 2 * (size_t)h->nmo * nfreq, nb_v = sizeof(double) * h->nmo;
+        h->stage_out.ensure(nb_sig + 2 * nb_v);
+        char* o = h->stage_out.as<char>();
+        GWB_CUDA(cudaMemcpyAsync(o, h->sigma.p, nb_sig, cudaMemcpyDeviceToHost, s));
+        GWB_CUDA(cudaMemcpyAsync(o + nb_sig, h->sigx.p, nb_v, cudaMemcpyDeviceToHost, s));
+        GWB_CUDA(cudaMemcpyAsync(o + nb_sig + nb_v, h->qp.p, nb_v, cudaMemcpyDeviceToHost, s));
         GWB_CUDA(cudaStreamSynchronize(s));
+        if (sigma_out) std::memcpy(sigma_out, o, nb_sig);
+        if (sigma_x_out) std::memcpy(sigma_x_out, o + nb_sig, nb_v);
+        if (qp_out) std::memcpy(qp_out, o + nb_sig + nb_v, nb_v);
         if (omega_out) std::copy(omega.begin(), omega.end(), omega_out);
         if (weight_out) std::copy(weight.begin(), weight.end(), weight_out);
     });

@@ -36,6 +36,8 @@ constexpr int kNb = 64;
 // Padded shared-memory row stride (doubles) of a 64-wide tile: 68*8 B rows put the
 // 8 rows touched by one m8n8k4 fragment load on distinct banks.
 constexpr int kLds = 68;
+// Default variant of the trailing-update kernel (index into the table in kernels_fp64.cu).
+constexpr int kDefaultUpdateVariant = 0;
 
 // Geometry of one frequency chunk of the tall screening matrices
 //   A_f = [ eps_f (n_pad x n_pad, lower) ; B_f^T (m_pad x n_pad) ],  row-major, ld = n_pad.
@@ -132,6 +134,11 @@ int launch_pade_sweep(const double* sigma_row, const double* omega, int64_t nfre
 int launch_negate_copy(const double* qacc, int64_t nf, int64_t m, int64_t ldq_in, double* q_out, int64_t ldq_out,
                        cudaStream_t s);
 double measure_fp64_peak_tflops(cudaStream_t s);
+// kernels_f32.cu: the mixed-precision form (FP32 tall matrices, 3xTF32 tensor-core updates).
+int launch_build_tall32(const TallGeometry& g, const double* v, const double* xt, const double* dvec, int64_t nf,
+                        float* a, cudaStream_t s);
+int launch_factor_chunk32(const TallGeometry& g, int64_t nf, float* a, float* linv, double* qacc,
+                          unsigned long long* err_pivot, cudaStream_t s, UpdateProfiler* prof);
 // kernels_c64.cu: eta != 0 (complex symmetric M = I - S V S, S = diag(Pi0)^1/2).  Planes a_re/a_im
 // of geometry g; svec 2*n_pad, linv 2*64*64, qacc 2*m_pad doubles per frequency.
 int launch_factor_chunk_c(const TallGeometry& g, int64_t nf, const double* delta, const double* omega, double eta,

@@ -13,6 +13,7 @@
 #include "internal.cuh"
 
 #include <cmath>
+#include <cstdlib>
 
 namespace gwb200 {
 namespace {
@@ -208,21 +209,25 @@ __global__ void __launch_bounds__(256) k_potrf_diag(double* __restrict__ a, int6
         const int i = idx / kNb, j = idx % kNb;
         if (j <= i) A[(size_t)i * ld + j] = T[i * L + j];
     }
-    // Inverse of the lower-triangular block by forward substitution, one column per thread.
-    if (tid < kNb) {
-        const int col = tid;
+    // Inverse of the lower-triangular block by forward substitution: column `col` is owned by the
+    // four lanes 4*col..4*col+3 of one warp (all 256 threads busy), which split each dot product
+    // and combine it with two xor-shuffles.
+    {
+        const int col = tid >> 2, part = tid & 3;
         for (int i = 0; i < kNb; ++i) {
-            double y;
-            if (i < col) {
-                y = 0.0;
-            } else if (i == col) {
-                y = 1.0 / T[i * L + i];
-            } else {
-                double s = 0.0;
-                for (int l = col; l < i; ++l) s = fma(T[i * L + l], Y[l * L + col], s);
-                y = -s / T[i * L + i];
+            double sum = 0.0;
+            if (i > col)
+                for (int l = col + part; l < i; l += 4) sum = fma(T[i * L + l], Y[l * L + col], sum);
+            sum += __shfl_xor_sync(0xffffffffu, sum, 1);
+            sum += __shfl_xor_sync(0xffffffffu, sum, 2);
+            if (part == 0) {
+                double y;
+                if (i < col) y = 0.0;
+                else if (i == col) y = 1.0 / T[i * L + i];
+                else y = -sum / T[i * L + i];
+                Y[i * L + col] = y;
             }
-            Y[i * L + col] = y;
+            __syncwarp();
         }
     }
     __syncthreads();
@@ -289,21 +294,54 @@ __device__ __forceinline__ void cp_async_wait_all() {
     asm volatile("cp.async.commit_group;\n" ::);
     asm volatile("cp.async.wait_group 0;\n" ::);
 }
-// 64 x 32 slice of a panel (global row stride ld) into shared memory (stride kLdk).
-constexpr int kKc = 32;   // K sub-chunk of the pipelined update
-constexpr int kLdk = 36;  // its padded shared row stride (same bank spread as kLds)
-__device__ __forceinline__ void load_slice_async(double* __restrict__ s, const double* __restrict__ gsrc, int64_t ld) {
-    for (int idx = threadIdx.x; idx < 64 * (kKc / 2); idx += blockDim.x) {
-        const int r = idx / (kKc / 2), c2 = idx % (kKc / 2);
-        cp_async_16(s + r * kLdk + 2 * c2, gsrc + (size_t)r * ld + 2 * c2);
+// Update kernel family: 64x64 output tile per CTA, warp tile (8*WM) x (8*WN) of m8n8k4 DMMA
+// fragments, K streamed in KC-wide slices through a STAGES-deep cp.async pipeline.
+template <int KC>
+__device__ __forceinline__ void load_slice_async(double* __restrict__ s, const double* __restrict__ gsrc, int64_t ld,
+                                                 int nthreads) {
+    constexpr int LD = KC + 4;  // (KC+4)*8 bytes per row: the 8 rows of one fragment load hit distinct banks
+    for (int idx = threadIdx.x; idx < 64 * (KC / 2); idx += nthreads) {
+        const int r = idx / (KC / 2), c2 = idx % (KC / 2);
+        cp_async_16(s + r * LD + 2 * c2, gsrc + (size_t)r * ld + 2 * c2);
     }
 }
 
-__global__ void __launch_bounds__(256, 3) k_update(double* __restrict__ a, int64_t ld, int64_t stride, int64_t kb0,
-                                                   int nk, int64_t tc0, int64_t T, int64_t nsq) {
+template <int WM, int WN, int LD, int KD>
+__device__ __forceinline__ void warp_mma(const double* __restrict__ As, const double* __restrict__ Bs,
+                                         double (&acc)[WM][WN][2], int r0, int c0) {
+    const int lane = threadIdx.x & 31;
+    const int g = lane >> 2, t = lane & 3;
+#pragma unroll 2
+    for (int kk = 0; kk < KD; kk += 4) {
+        double af[WM], bf[WN];
+#pragma unroll
+        for (int i = 0; i < WM; ++i) af[i] = -As[(r0 + 8 * i + g) * LD + kk + t];
+#pragma unroll
+        for (int j = 0; j < WN; ++j) bf[j] = Bs[(c0 + 8 * j + g) * LD + kk + t];
+#pragma unroll
+        for (int i = 0; i < WM; ++i)
+#pragma unroll
+            for (int j = 0; j < WN; ++j) dmma_8x8x4(acc[i][j], af[i], bf[j]);
+    }
+}
+
+template <int WM, int WN, int KC, int STAGES>
+struct UpdateCfg {
+    static constexpr int kWarpsM = 64 / (8 * WM), kWarpsN = 64 / (8 * WN);
+    static constexpr int kThreads = 32 * kWarpsM * kWarpsN;
+    static constexpr int kLd = KC + 4;
+    static constexpr size_t kSmem = (size_t)STAGES * 2 * 64 * kLd * sizeof(double);
+    static constexpr int kMinBlocks = (227 * 1024) / (int)kSmem < 4 ? (227 * 1024) / (int)kSmem : 4;
+};
+
+template <int WM, int WN, int KC, int STAGES>
+__global__ void __launch_bounds__(UpdateCfg<WM, WN, KC, STAGES>::kThreads, UpdateCfg<WM, WN, KC, STAGES>::kMinBlocks)
+    k_update(double* __restrict__ a, int64_t ld, int64_t stride, int64_t kb0, int nk, int64_t tc0, int64_t T,
+             int64_t nsq) {
+    using Cfg = UpdateCfg<WM, WN, KC, STAGES>;
+    constexpr int LD = Cfg::kLd;
     extern __shared__ double smem[];
-    // two pipeline stages, each holding the 64x32 slices of P_i and P_j
-    auto stage = [&](int st, int which) { return smem + (2 * st + which) * 64 * kLdk; };
+    auto stage = [&](int st, int which) { return smem + (2 * st + which) * 64 * LD; };
     const int f = blockIdx.y;
     const int64_t x = blockIdx.x;
     const int64_t L = nsq - tc0;                     // square row tiles of the first column tile
@@ -324,38 +362,75 @@ __global__ void __launch_bounds__(256, 3) k_update(double* __restrict__ a, int64
     }
     const int64_t ri = tr * kNb, cj = (tc0 + c) * kNb;
     double* A = a + (size_t)f * stride;
-    const int nsub = nk * (kNb / kKc);
-    load_slice_async(stage(0, 0), A + ri * ld + kb0, ld);
-    load_slice_async(stage(0, 1), A + cj * ld + kb0, ld);
-    asm volatile("cp.async.commit_group;\n" ::);
-    double acc[2][4][2] = {};
-    for (int sc = 0; sc < nsub; ++sc) {
-        if (sc + 1 < nsub) {
-            const int64_t kc = kb0 + (int64_t)(sc + 1) * kKc;
-            load_slice_async(stage((sc + 1) & 1, 0), A + ri * ld + kc, ld);
-            load_slice_async(stage((sc + 1) & 1, 1), A + cj * ld + kc, ld);
-            asm volatile("cp.async.commit_group;\n" ::);
-            asm volatile("cp.async.wait_group 1;\n" ::);
-        } else {
-            asm volatile("cp.async.wait_group 0;\n" ::);
+    const int nsub = nk * (kNb / KC);
+    // prologue: STAGES-1 slices in flight
+#pragma unroll
+    for (int p = 0; p < STAGES - 1; ++p) {
+        if (p < nsub) {
+            const int64_t kc = kb0 + (int64_t)p * KC;
+            load_slice_async<KC>(stage(p, 0), A + ri * ld + kc, ld, Cfg::kThreads);
+            load_slice_async<KC>(stage(p, 1), A + cj * ld + kc, ld, Cfg::kThreads);
         }
+        asm volatile("cp.async.commit_group;\n" ::);
+    }
+    const int w = threadIdx.x >> 5;
+    const int r0 = 8 * WM * (w / Cfg::kWarpsN), c0 = 8 * WN * (w % Cfg::kWarpsN);
+    double acc[WM][WN][2] = {};
+    for (int sc = 0; sc < nsub; ++sc) {
+        const int pf = sc + STAGES - 1;  // slice to prefetch into the stage freed last iteration
+        if (pf < nsub) {
+            const int64_t kc = kb0 + (int64_t)pf * KC;
+            load_slice_async<KC>(stage(pf % STAGES, 0), A + ri * ld + kc, ld, Cfg::kThreads);
+            load_slice_async<KC>(stage(pf % STAGES, 1), A + cj * ld + kc, ld, Cfg::kThreads);
+        }
+        asm volatile("cp.async.commit_group;\n" ::);
+        asm volatile("cp.async.wait_group %0;\n" ::"n"(STAGES - 1));
         __syncthreads();
-        tile_mma<kLdk, kKc>(stage(sc & 1, 0), stage(sc & 1, 1), acc, -1.0);
+        warp_mma<WM, WN, LD, KC>(stage(sc % STAGES, 0), stage(sc % STAGES, 1), acc, r0, c0);
         __syncthreads();
     }
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int lane = threadIdx.x & 31;
     const int g = lane >> 2, t = lane & 3;
-    const int rr = 16 * (w >> 1), cc = 32 * (w & 1);
 #pragma unroll
-    for (int i = 0; i < 2; ++i)
+    for (int i = 0; i < WM; ++i)
 #pragma unroll
-        for (int j = 0; j < 4; ++j) {
-            double2* pc = reinterpret_cast<double2*>(A + (size_t)(ri + rr + 8 * i + g) * ld + cj + cc + 8 * j + 2 * t);
+        for (int j = 0; j < WN; ++j) {
+            double2* pc = reinterpret_cast<double2*>(A + (size_t)(ri + r0 + 8 * i + g) * ld + cj + c0 + 8 * j + 2 * t);
             double2 v = *pc;
             v.x += acc[i][j][0];
             v.y += acc[i][j][1];
             *pc = v;
         }
+}
+
+// Variant table of the update kernel (selected by GWB200_UPDATE_VARIANT, default kDefaultUpdateVariant).
+struct UpdateVariant {
+    void (*fn)(double*, int64_t, int64_t, int64_t, int, int64_t, int64_t, int64_t);
+    int threads;
+    size_t smem;
+    const char* name;
+};
+template <int WM, int WN, int KC, int ST>
+UpdateVariant make_variant(const char* name) {
+    using Cfg = UpdateCfg<WM, WN, KC, ST>;
+    return {k_update<WM, WN, KC, ST>, Cfg::kThreads, Cfg::kSmem, name};
+}
+const UpdateVariant& update_variant() {
+    static const UpdateVariant table[] = {
+        make_variant<2, 4, 32, 2>("w16x32_k32_s2"),
+        make_variant<4, 4, 32, 2>("w32x32_k32_s2"),
+        make_variant<4, 4, 16, 3>("w32x32_k16_s3"),
+        make_variant<2, 4, 32, 3>("w16x32_k32_s3"),
+        make_variant<4, 8, 32, 2>("w32x64_k32_s2"),
+        make_variant<4, 4, 32, 3>("w32x32_k32_s3"),
+    };
+    static const int nvar = (int)(sizeof(table) / sizeof(table[0]));
+    int v = kDefaultUpdateVariant;
+    if (const char* env = std::getenv("GWB200_UPDATE_VARIANT")) {
+        const int e = std::atoi(env);
+        if (e >= 0 && e < nvar) v = e;
+    }
+    return table[v];
 }
 
 // q_out[f, j] = -qacc[f, j]  (x^T W_c x = -||L^{-1} D^1/2 x||^2).
@@ -430,8 +505,8 @@ int launch_factor_chunk(const TallGeometry& g, int64_t nf, double* a, double* li
     const size_t smem = 2 * 64 * kLds * sizeof(double);
     const size_t smem_potrf = 2 * kNb * (kNb + 1) * sizeof(double);
     GWB_CUDA(cudaFuncSetAttribute(k_trsm_panel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    const size_t smem_update = 4 * 64 * kLdk * sizeof(double);
-    GWB_CUDA(cudaFuncSetAttribute(k_update, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_update));
+    const UpdateVariant& uv = update_variant();
+    GWB_CUDA(cudaFuncSetAttribute(uv.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)uv.smem));
     GWB_CUDA(cudaFuncSetAttribute(k_potrf_diag, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_potrf));
     const int64_t nsq = g.n_pad / kNb;   // square tile rows/cols
     const int64_t nrt = g.rows / kNb;    // all tile rows
@@ -443,7 +518,7 @@ int launch_factor_chunk(const TallGeometry& g, int64_t nf, double* a, double* li
         if (tiles <= 0) return;
         dim3 grid((unsigned)tiles, (unsigned)nf);
         if (prof) prof->begin();
-        k_update<<<grid, 256, smem_update, s>>>(a, g.ld, g.stride, kb0, nk, tc0, T, nsq);
+        uv.fn<<<grid, uv.threads, uv.smem, s>>>(a, g.ld, g.stride, kb0, nk, tc0, T, nsq);
         GWB_LAUNCH("k_update");
         if (prof) prof->end((double)nf * update_flops(g, kb0, nk, tc0 * kNb, (tc0 + T) * kNb));
         ++launches;

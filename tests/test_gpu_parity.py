@@ -329,3 +329,38 @@ def test_complex_path_continuous_at_eta_zero(backend, cfg1_input):
     real, _ = backend.sigma_c(om, w, [4])
     tiny, _ = backend.sigma_c(om, w, [4], eta=1e-13)
     assert np.abs(tiny - real).max() <= 1e-9 * np.abs(real).max()
+
+
+@pytest.mark.parametrize("nmo,nocc,states,nfreq", [
+    (14, 4, list(range(14)), 17),
+    (40, 12, [11, 12], 24),      # n = 336: six blocks, outer blocks and look-left updates
+])
+def test_mixed_form_error_against_fp64(backend, nmo, nocc, states, nfreq):
+    """The mixed form (FP32 tall matrices, 3xTF32 updates, no FP64 refinement) carries FP32-level
+    error: screened forms and Sigma_c within 2e-5 relative of the FP64 form."""
+    from minigw_b200 import generate_transformed_legendre_grid
+    from minigw_b200.synthetic import make_input
+
+    inp = make_input(nmo, nocc, seed=nmo + 2)
+    om, w = generate_transformed_legendre_grid(nfreq)
+    backend.load_system(inp)
+    q64, _ = backend.screened_forms(om, states)
+    q32, _ = backend.screened_forms(om, states, precision="mixed")
+    assert np.abs(q32 - q64).max() <= 2e-5 * np.abs(q64).max()
+    s64, _ = backend.sigma_c(om, w, states)
+    s32, _ = backend.sigma_c(om, w, states, precision="mixed")
+    assert np.abs(s32 - s64).max() <= 2e-5 * np.abs(s64).max()
+
+
+def test_mixed_form_h2o_qp(backend, h2o_input, oracle_lib):
+    from minigw_b200 import GwB200Error
+
+    backend.load_system(h2o_input)
+    r64 = backend.run_g0w0(200, 16, [4])
+    r32 = backend.run_g0w0(200, 16, [4], precision="mixed")
+    rel = np.abs(r32["sigma"] - r64["sigma"]).max() / np.abs(r64["sigma"]).max()
+    assert rel < 2e-5
+    assert abs(r32["qp"][4] - r64["qp"][4]) * HA_EV < 0.01  # well-conditioned Pade on H2O: meV-level
+    with pytest.raises(GwB200Error) as e:
+        backend.run_g0w0(200, 16, [4], eta=0.01, precision="mixed")
+    assert e.value.status == "GWB200_BAD_ARGUMENT"
