@@ -308,6 +308,13 @@ def run_b200(args, wl):
     scr_ms = statistics.mean(s["device_ms_screening"] for s in stats)
     scr_tflops = stats[0]["flops_screening"] / (scr_ms * 1e-3) / 1e12
     launches = sum(s["kernel_launches"] for s in stats)
+    traffic = None
+    try:  # DRAM bytes per launch of the dominant kernel from the committed ncu capture of this workload
+        tr = json.loads((ROOT / "profiles" / "k_update_traffic.json").read_text())["workloads"].get(wl.name, {})
+        if "bytes_per_launch" in tr and args.precision == "fp64":
+            traffic = tr["bytes_per_launch"]
+    except (OSError, ValueError, KeyError):
+        pass
 
     solves_per_step = 1 if split else world
     value = solves_per_step * 1e3 / ms_per_step
@@ -337,7 +344,9 @@ def run_b200(args, wl):
                      "frac": (achieved / peak_fp64) if achieved else None,
                      "peak_source": "FP64 DMMA (mma.sync m8n8k4 f64) probe measured in this run; "
                                     "MEASURED_PEAKS.json has no FP64 figure",
-                     "launches": upd_n, "traffic": None},
+                     "launches": upd_n, "traffic": traffic,
+                     "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum per k_update launch "
+                                       "(profiles/k_update_cfg3_dram_traffic.md)" if traffic else None},
         "e2e": {"value": solves_per_step * 1e3 / e2e_ms, "unit": "GW solves/s", "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h), "ms_per_step": e2e_ms},
         "gpu_launches": int(launches),

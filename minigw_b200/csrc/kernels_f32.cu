@@ -128,13 +128,13 @@ __global__ void __launch_bounds__(256) k_potrf_diag32(float* __restrict__ a, int
             T[j * L + j] = sqrt(piv);
         }
         __syncthreads();
-        const double djj = T[j * L + j];
-        for (int i = j + 1 + tid; i < kNb; i += blockDim.x) T[i * L + j] /= djj;
+        const double rjj = 1.0 / T[j * L + j];
+        for (int i = j + 1 + tid; i < kNb; i += blockDim.x) T[i * L + j] *= rjj;
         __syncthreads();
-        const int rem = kNb - 1 - j;
-        for (int idx = tid; idx < rem * rem; idx += blockDim.x) {
-            const int i = j + 1 + idx / rem, l = j + 1 + idx % rem;
-            if (l <= i) T[i * L + l] -= T[i * L + j] * T[l * L + j];
+        // rank-1 update of the trailing lower triangle on a 16 x 16 thread grid (no index division)
+        for (int i = j + 1 + (tid >> 4); i < kNb; i += 16) {
+            const double lij = T[i * L + j];
+            for (int l = j + 1 + (tid & 15); l <= i; l += 16) T[i * L + l] -= lij * T[l * L + j];
         }
         __syncthreads();
     }
