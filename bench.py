@@ -46,6 +46,11 @@ def parse_args():
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-pairs", type=int, default=0, help="reference (f_n, f') pairs per CPU sample (0 = auto)")
+    ap.add_argument("--serving", action="store_true",
+                    help="serving stream (config 5): Poisson arrivals of mixed-size requests through the "
+                         "continuous-batching server at swept rates; reports p50/p99 latency and solves/s")
+    ap.add_argument("--requests", type=int, default=24, help="requests per serving rate")
+    ap.add_argument("--slots", type=int, default=4, help="concurrent server slots (serving mode)")
     ap.add_argument("--split-frequencies", action="store_true",
                     help="N>1: split one solve's integration frequencies over the ranks (strong scaling; one "
                          "NCCL all-reduce of the partial Sigma_c per solve) instead of one replica per rank")
@@ -396,8 +401,81 @@ def run_b200(args, wl):
     return 0
 
 
+def run_serving(args):
+    """Config 5: requests with nmo log-uniform in 16..160 (the upper bound is capped from 256 so the
+    request pool fits host memory and the run stays within minutes), nocc = round(nmo/6), 1-8
+    states around the gap, 32-128 frequencies, FP64 or mixed chosen at random; Poisson arrivals
+    at rates swept as fractions of the measured back-to-back capacity."""
+    import numpy as np
+    import torch
+
+    from minigw_b200 import B200Server
+    from minigw_b200.synthetic import make_input_on_device
+
+    rng = np.random.default_rng(args.seed)
+    pool = []
+    for i in range(args.requests):
+        nmo = int(round(np.exp(rng.uniform(np.log(16), np.log(160)))))
+        nocc = max(1, int(round(nmo / 6)))
+        ns = int(rng.integers(1, 9))
+        lo = max(0, nocc - (ns + 1) // 2)
+        states = list(range(lo, min(nmo, lo + ns)))
+        nfreq = int(rng.integers(32, 129))
+        prec = "mixed" if rng.random() < 0.5 else "fp64"
+        pool.append((make_input_on_device(nmo, nocc, seed=args.seed + 1000 + i, device=0, pin=True), nfreq, states, prec))
+    torch.cuda.empty_cache()
+    budget = int(0.6 * torch.cuda.mem_get_info(0)[0])
+    out = {"metric": "serving_p99_ms", "unit": "ms", "higher_is_better": False, "n_gpus": 1,
+           "config": {"workload": "cfg5: Poisson stream, nmo log-uniform 16..160, nocc=round(nmo/6), 1-8 states, "
+                      "32-128 freq, fp64 or mixed", "requests_per_rate": args.requests, "slots": args.slots,
+                      "hbm_budget_bytes": budget}, "rates": []}
+    with B200Server(0, slots=args.slots, hbm_budget_bytes=budget) as srv:
+        for inp, nf, st, pr in pool[:4]:  # warm-up
+            srv.wait(srv.submit(inp, nf, 12, st, precision=pr))
+        t0 = time.perf_counter()
+        tickets = [srv.submit(inp, nf, 12, st, precision=pr) for inp, nf, st, pr in pool]
+        for t in tickets:
+            srv.wait(t)
+        capacity = len(pool) / (time.perf_counter() - t0)
+        out["capacity_solves_per_s"] = capacity
+        for frac in (0.25, 0.5, 0.8, 1.0):
+            rate = frac * capacity
+            gaps = rng.exponential(1.0 / rate, len(pool))
+            t_start = time.perf_counter()
+            tickets = []
+            for (inp, nf, st, pr), gap in zip(pool, gaps):
+                time.sleep(gap)
+                tickets.append(srv.submit(inp, nf, 12, st, precision=pr))
+            res = [srv.wait(t) for t in tickets]
+            span = time.perf_counter() - t_start
+            lat = sorted(r["queue_ms"] + r["service_ms"] for r in res)
+            out["rates"].append({"offered_per_s": rate, "solves_per_s": len(res) / span,
+                                 "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+                                 "mean_queue_ms": float(np.mean([r["queue_ms"] for r in res])),
+                                 "requests": [[inp.nmo, nf, pr[0], round(r["queue_ms"], 1), round(r["service_ms"], 1),
+                                               round(r["device_ms"], 1)]
+                                              for (inp, nf, st, pr), r in zip(pool, res)]})
+        # accuracy of the mixed requests against FP64 solves of the same systems (untimed)
+        errs = []
+        for inp, nf, st, pr in pool:
+            if pr != "mixed":
+                continue
+            a = srv.wait(srv.submit(inp, nf, 12, st, precision="mixed"))
+            b = srv.wait(srv.submit(inp, nf, 12, st, precision="fp64"))
+            errs.append(float(np.abs(a["sigma"] - b["sigma"]).max() / max(np.abs(b["sigma"]).max(), 1e-300)))
+        out["mixed_sigma_c_max_rel_err_vs_fp64"] = max(errs) if errs else None
+    top = out["rates"][-1]
+    out["value"] = top["p99_ms"]
+    out["p50_ms"] = top["p50_ms"]
+    out["solves_per_s"] = top["solves_per_s"]
+    print(json.dumps(out))
+    return 0
+
+
 def main() -> int:
     args = parse_args()
+    if args.serving:
+        return run_serving(args)
     from minigw_b200.synthetic import WORKLOADS
 
     wl = WORKLOADS[args.workload]

@@ -89,6 +89,11 @@ int gwb200_destroy(gwb200_handle* h);
  * (src/workspace/device_screening_workspace.cu:288-310). */
 int gwb200_set_stream(gwb200_handle* h, void* stream);
 
+/* Cap the device memory this handle may hold (resident system + workspaces); the frequency chunk is
+ * sized to fit.  0 = no cap beyond the device's free memory.  No reference counterpart (the
+ * reference sizes nothing: it allocates per call). */
+int gwb200_set_memory_limit(gwb200_handle* h, int64_t bytes);
+
 /* Upload one molecular system and build its resident device state: the occupied-virtual
  * index map, the V_ph=(jb|ia) gather and the exchange diagonal.  eri (nmo^4), mo_energy
  * (nmo) and vxc (nmo^2) are borrowed for the call.
@@ -196,6 +201,47 @@ int gwb200_read_input_h5(const char* path, int64_t* nmo, int64_t* nocc, double* 
 int gwb200_screened_forms_noalloc(int64_t n, int64_t m, const double* d_v, const double* d_xt,
                                   const double* d_delta, const double* d_omega, int64_t nfreq,
                                   double* d_q_out, void* stream);
+
+/* ---- Serving: a continuous-batching request loop (no reference counterpart) ----
+ * One request = one G0W0 solve.  All pointers are host memory owned by the caller and must stay
+ * valid until gwb200_server_wait returns for the request's ticket.  Outputs (may be NULL) are
+ * filled when the request completes: omega/weight nfreq, sigma nmo x nfreq complex, sigma_x and
+ * qp nmo. */
+typedef struct gwb200_request {
+    int64_t nmo, nocc;
+    const double* mo_energy;  /* nmo */
+    const double* eri;        /* nmo^4, C order */
+    const double* vxc;        /* nmo^2 */
+    double fermi_energy;
+    int64_t nfreq, npade;
+    const int64_t* states;
+    int64_t nstates;
+    double eta;
+    int precision;
+    double* omega_out;
+    double* weight_out;
+    double* sigma_out;
+    double* sigma_x_out;
+    double* qp_out;
+} gwb200_request;
+
+typedef struct gwb200_server gwb200_server;
+
+/* Start `slots` workers on `device`, each with its own handle and stream and a device-memory cap
+ * of hbm_budget_bytes / slots.  Requests are admitted FIFO as workers free up; requests in
+ * different slots overlap on the GPU.  Results do not depend on which requests ran alongside. */
+int gwb200_server_create(int device, int slots, int64_t hbm_budget_bytes, gwb200_server** out);
+
+/* Queue one request (non-blocking).  GWB200_OOM if it cannot fit one slot's budget. */
+int gwb200_server_submit(gwb200_server* s, const gwb200_request* req, int64_t* ticket);
+
+/* Block until the request completes; its status is returned (and in *status), with the time it
+ * waited for a slot, its service time (host, from admission to results) and its device time. */
+int gwb200_server_wait(gwb200_server* s, int64_t ticket, int* status, double* queue_ms, double* service_ms,
+                       double* device_ms);
+
+/* Finish every queued request, stop the workers, release their handles. */
+int gwb200_server_destroy(gwb200_server* s);
 
 /* Measured FP64 tensor (DMMA) throughput of this device in TFLOP/s, from a short
  * microbenchmark of mma.sync f64 (used as the roofline denominator of the plain form). */

@@ -8,6 +8,7 @@ workload generator used by the tests and the benchmark.
 from ._lib import FP64, MIXED, STATUS, GwB200Error, version
 from .gw import (
     B200Backend,
+    B200Server,
     GwInput,
     GwResult,
     GwSettings,
@@ -22,7 +23,7 @@ from .gw import (
 )
 
 __all__ = [
-    "FP64", "MIXED", "STATUS", "GwB200Error", "version", "B200Backend", "GwInput", "GwResult", "GwSettings",
+    "FP64", "MIXED", "STATUS", "GwB200Error", "version", "B200Backend", "B200Server", "GwInput", "GwResult", "GwSettings",
     "GwTimings", "generate_transformed_legendre_grid", "output_final_energy_table", "output_self_energy_after_pade",
     "output_self_energy_before_pade", "read_gw_input_hdf5", "run_g0w0", "selected_states",
 ]

@@ -33,6 +33,8 @@ MIXED = 1
 # Every symbol include/gwb200.h declares.
 EXPORTS = (
     "gwb200_last_error", "gwb200_version", "gwb200_create", "gwb200_destroy", "gwb200_set_stream",
+    "gwb200_set_memory_limit", "gwb200_server_create", "gwb200_server_submit", "gwb200_server_wait",
+    "gwb200_server_destroy",
     "gwb200_load_system", "gwb200_run_g0w0", "gwb200_sigma_c_shard",
     "gwb200_sigma_c", "gwb200_screened_forms", "gwb200_screened_forms_complex", "gwb200_sigma_x_diag", "gwb200_qp", "gwb200_pade_sweep",
     "gwb200_grid", "gwb200_read_input_h5", "gwb200_screened_forms_noalloc", "gwb200_fp64_peak_tflops",
@@ -75,6 +77,16 @@ _ip = C.POINTER(C.c_int64)
 _vp = C.c_void_p
 
 
+class Request(C.Structure):
+    """gwb200_request (include/gwb200.h)."""
+    _fields_ = [
+        ("nmo", C.c_int64), ("nocc", C.c_int64), ("mo_energy", _dp), ("eri", _dp), ("vxc", _dp),
+        ("fermi_energy", C.c_double), ("nfreq", C.c_int64), ("npade", C.c_int64), ("states", _ip),
+        ("nstates", C.c_int64), ("eta", C.c_double), ("precision", C.c_int), ("omega_out", _dp),
+        ("weight_out", _dp), ("sigma_out", _dp), ("sigma_x_out", _dp), ("qp_out", _dp),
+    ]
+
+
 def _load() -> C.CDLL:
     if not LIB_PATH.exists():
         raise ImportError(
@@ -86,6 +98,11 @@ def _load() -> C.CDLL:
     lib.gwb200_create.argtypes = [C.c_int, C.POINTER(_vp)]
     lib.gwb200_destroy.argtypes = [_vp]
     lib.gwb200_set_stream.argtypes = [_vp, _vp]
+    lib.gwb200_set_memory_limit.argtypes = [_vp, C.c_int64]
+    lib.gwb200_server_create.argtypes = [C.c_int, C.c_int, C.c_int64, C.POINTER(_vp)]
+    lib.gwb200_server_submit.argtypes = [_vp, C.POINTER(Request), C.POINTER(C.c_int64)]
+    lib.gwb200_server_wait.argtypes = [_vp, C.c_int64, C.POINTER(C.c_int), _dp, _dp, _dp]
+    lib.gwb200_server_destroy.argtypes = [_vp]
     lib.gwb200_load_system.argtypes = [_vp, C.c_int64, C.c_int64, _dp, _dp, _dp, C.c_double]
     lib.gwb200_sigma_c.argtypes = [_vp, _dp, _dp, C.c_int64, _ip, C.c_int64, C.c_double, C.c_int, _dp,
                                    C.POINTER(Stats)]

@@ -25,7 +25,7 @@ GW_BIN = PKG / "bin" / "gw"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 CU_SOURCES = ["kernels_fp64.cu", "kernels_f32.cu", "kernels_c64.cu", "kernels_small.cu", "gwb200_abi.cu",
               "noalloc.cu"]
-CXX_SOURCES = ["host_grid.cpp", "host_h5.cpp"]
+CXX_SOURCES = ["host_grid.cpp", "host_h5.cpp", "server.cpp"]
 CLI_SOURCES = ["gw_main.cpp"]
 
 
@@ -72,11 +72,11 @@ def build(verbose: bool = False, ptxas_info: bool = False) -> Path:
     for src in CXX_SOURCES:
         obj = BUILD / (src + ".o")
         if _stale(obj, [CSRC / src] + headers):
-            _run(["g++", "-std=c++17", "-O2", "-fPIC", "-ffp-contract=off", "-Wall", "-Wextra",
+            _run(["g++", "-std=c++17", "-O2", "-fPIC", "-pthread", "-ffp-contract=off", "-Wall", "-Wextra",
                   "-I/usr/local/cuda/include", "-c", str(CSRC / src), "-o", str(obj)], verbose)
         objs.append(obj)
     if _stale(LIB, objs):
-        _run([nvcc, *ARCH, "-shared", "-o", str(LIB), *map(str, objs)], verbose)
+        _run([nvcc, *ARCH, "-shared", "-Xcompiler", "-pthread", "-o", str(LIB), *map(str, objs)], verbose)
     GW_BIN.parent.mkdir(exist_ok=True)
     cli = [CSRC / s for s in CLI_SOURCES]
     if all(p.exists() for p in cli) and _stale(GW_BIN, cli + [LIB, ROOT / "include" / "gwb200.h"]):

@@ -17,20 +17,36 @@ namespace {
 
 thread_local std::string g_last_error;
 
-// Grow-only device buffer.
+// Device buffer.  Default: grow-only (cudaMalloc).  A handle with a memory limit sizes buffers
+// exactly per request with the stream-ordered allocator on its own stream, so a sequence of
+// different requests never holds more than one request's footprint and no cudaFree synchronises
+// the device under concurrently running handles.
 struct DevBuf {
     void* p = nullptr;
     size_t bytes = 0;
+    cudaStream_t async_stream = nullptr;  // non-null: allocated stream-ordered on this stream
     void ensure(size_t want) {
         if (want <= bytes) return;
         release();
         GWB_CUDA(cudaMalloc(&p, want));
         bytes = want;
     }
+    void ensure_exact(size_t want, cudaStream_t s, cudaMemPool_t pool) {
+        if (p && want == bytes) return;
+        release();
+        if (pool) GWB_CUDA(cudaMallocFromPoolAsync(&p, want, pool, s));
+        else GWB_CUDA(cudaMallocAsync(&p, want, s));
+        bytes = want;
+        async_stream = s;
+    }
     void release() {
-        if (p) cudaFree(p);
+        if (p) {
+            if (async_stream) cudaFreeAsync(p, async_stream);
+            else cudaFree(p);
+        }
         p = nullptr;
         bytes = 0;
+        async_stream = nullptr;
     }
     template <class T>
     T* as() const {
@@ -80,6 +96,11 @@ int guarded(F&& body) {
 
 } // namespace
 
+int gwb200_fail_status(int code, const char* message) {
+    g_last_error = message ? message : "";
+    return code;
+}
+
 struct gwb200_handle {
     int device = 0;
     cudaStream_t stream = nullptr;      // stream all work is issued on
@@ -96,11 +117,21 @@ struct gwb200_handle {
     DevBuf xt, dvec, a, linv, qacc, qall, sigma, omega, weight, states, err, qp, qp_scratch, omega_out;
     PinnedBuf stage_in, stage_out;
     // cached frequency-chunk size for a repeated geometry (avoids cudaMemGetInfo per call)
-    int64_t chunk_key[4] = {-1, -1, -1, -1};
+    int64_t chunk_key[5] = {-1, -1, -1, -1, -1};
+    int64_t mem_limit = 0;          // 0: no cap
+    cudaMemPool_t pool = nullptr;   // pool for exact-size buffers (set by a server), else the default
     int64_t chunk_fc = 0;
 };
 
+void gwb200_attach_pool(gwb200_handle* h, cudaMemPool_t pool) { h->pool = pool; }
+
 namespace {
+
+// Allocate `b` for `want` bytes: grow-only, or exact and stream-ordered when the handle is limited.
+void size_buffer(gwb200_handle* h, DevBuf& b, size_t want) {
+    if (h->mem_limit > 0) b.ensure_exact(want, h->stream, h->pool);
+    else b.ensure(want);
+}
 
 void check_handle(gwb200_handle* h) {
     if (!h) fail(GWB200_BAD_ARGUMENT, "null gwb200_handle");
@@ -153,8 +184,8 @@ void compute_forms(gwb200_handle* h, const double* omega, int64_t nfreq, const i
 
     h->omega.ensure(sizeof(double) * nfreq);
     h->states.ensure(sizeof(int64_t) * nstates);
-    h->xt.ensure(sizeof(double) * (size_t)m * h->n);
-    h->qall.ensure(sizeof(double) * planes * (size_t)nfreq * g.m_pad);
+    size_buffer(h, h->xt, sizeof(double) * (size_t)m * h->n);
+    size_buffer(h, h->qall, sizeof(double) * planes * (size_t)nfreq * g.m_pad);
     h->err.ensure(sizeof(unsigned long long));
     {  // grid, states and (optionally) weights through the pinned staging buffer, all up front
         const size_t nb_om = sizeof(double) * nfreq, nb_st = sizeof(int64_t) * nstates;
@@ -178,25 +209,34 @@ void compute_forms(gwb200_handle* h, const double* omega, int64_t nfreq, const i
     // GWB200_MAX_FREQ_CHUNK caps the chunk (tests use it to exercise the multi-chunk path).
     int64_t cap = 0;
     if (const char* env = std::getenv("GWB200_MAX_FREQ_CHUNK")) cap = std::max<long long>(0, std::atoll(env));
-    const int64_t key[4] = {(int64_t)per_freq, nfreq, cap, (int64_t)g.stride};
+    const int64_t key[5] = {(int64_t)per_freq, nfreq, cap, (int64_t)g.stride, h->mem_limit};
     int64_t fc;
-    if (std::equal(key, key + 4, h->chunk_key)) {
+    if (std::equal(key, key + 5, h->chunk_key)) {
         fc = h->chunk_fc;  // same geometry as the last call: its buffers are already sized
     } else {
         size_t free_b = 0, total_b = 0;
         GWB_CUDA(cudaMemGetInfo(&free_b, &total_b));
         const size_t have = h->a.bytes + h->dvec.bytes + h->linv.bytes + h->qacc.bytes;
-        const size_t budget = (size_t)((double)(free_b + have) * 0.85);
+        size_t avail = free_b + have;  // what the chunk buffers may occupy
+        size_t budget = (size_t)((double)avail * 0.85);
+        if (h->mem_limit > 0) {  // the handle's cap minus what the system and panels already hold
+            const size_t resident = h->pqo.bytes + h->xdiag.bytes + h->v.bytes + h->xt.bytes + h->qall.bytes +
+                                    h->sigma.bytes + h->qp_scratch.bytes + ((size_t)1 << 20);
+            const size_t lim = (size_t)h->mem_limit;
+            const size_t room = lim > resident ? lim - resident : 0;
+            budget = std::min(budget, room);
+            avail = std::min(avail, room);
+        }
         fc = (int64_t)std::min<size_t>((size_t)nfreq, std::max<size_t>(1, budget / per_freq));
         if (cap > 0) fc = std::min<int64_t>(fc, cap);
-        if ((size_t)fc * per_freq > free_b + have) fail(GWB200_OOM, "not enough device memory for one frequency of eps(iw)");
-        std::copy(key, key + 4, h->chunk_key);
+        if ((size_t)fc * per_freq > avail) fail(GWB200_OOM, "not enough device memory for one frequency of eps(iw)");
+        std::copy(key, key + 5, h->chunk_key);
         h->chunk_fc = fc;
     }
-    h->a.ensure((mixed ? sizeof(float) : sizeof(double) * planes) * (size_t)fc * g.stride);
-    h->dvec.ensure(sizeof(double) * planes * (size_t)fc * g.n_pad);
-    h->linv.ensure((mixed ? sizeof(float) : sizeof(double) * planes) * (size_t)fc * kNb * kNb);
-    h->qacc.ensure(sizeof(double) * planes * (size_t)fc * g.m_pad);
+    size_buffer(h, h->a, (mixed ? sizeof(float) : sizeof(double) * planes) * (size_t)fc * g.stride);
+    size_buffer(h, h->dvec, sizeof(double) * planes * (size_t)fc * g.n_pad);
+    size_buffer(h, h->linv, (mixed ? sizeof(float) : sizeof(double) * planes) * (size_t)fc * kNb * kNb);
+    size_buffer(h, h->qacc, sizeof(double) * planes * (size_t)fc * g.m_pad);
 
     GWB_CUDA(cudaEventRecord(h->ev[0], s));
     launches += launch_gather_panel(h->pqo.as<double>(), h->nmo, h->nocc, h->states.as<int64_t>(), nstates,
@@ -355,6 +395,14 @@ int gwb200_destroy(gwb200_handle* h) {
     return GWB200_OK;
 }
 
+int gwb200_set_memory_limit(gwb200_handle* h, int64_t bytes) {
+    return guarded([&] {
+        check_handle(h);
+        if (bytes < 0) fail(GWB200_BAD_ARGUMENT, "negative memory limit");
+        h->mem_limit = bytes;
+    });
+}
+
 int gwb200_set_stream(gwb200_handle* h, void* stream) {
     return guarded([&] {
         check_handle(h);
@@ -377,13 +425,15 @@ int gwb200_load_system(gwb200_handle* h, int64_t nmo, int64_t nocc, const double
         const int64_t n = nocc * (nmo - nocc);
         // Only the (pq|o.) block is uploaded: every V_ph / panel element has an occupied third
         // index.  One 2D copy: nmo^2 rows of nocc*nmo contiguous doubles, source pitch nmo^2.
-        h->pqo.ensure(sizeof(double) * nmo2 * nocc * nmo);
-        h->xdiag.ensure(sizeof(double) * nmo * nocc);
+        if (h->mem_limit > 0)  // drop the previous request's workspaces before sizing this system
+            for (DevBuf* b : {&h->xt, &h->dvec, &h->a, &h->linv, &h->qacc, &h->qall}) b->release();
+        size_buffer(h, h->pqo, sizeof(double) * nmo2 * nocc * nmo);
+        size_buffer(h, h->xdiag, sizeof(double) * nmo * nocc);
         h->mo.ensure(sizeof(double) * nmo);
         h->vxc_diag.ensure(sizeof(double) * nmo);
         h->sigx.ensure(sizeof(double) * nmo);
         h->delta.ensure(sizeof(double) * n);
-        h->v.ensure(sizeof(double) * (size_t)n * n);
+        size_buffer(h, h->v, sizeof(double) * (size_t)n * n);
         h->flag.ensure(sizeof(int));
         std::vector<double> vd((size_t)nmo);
         for (int64_t p = 0; p < nmo; ++p) vd[(size_t)p] = vxc[p * nmo + p];

@@ -10,6 +10,11 @@
 
 #include "../../include/gwb200.h"
 
+// Sets the calling thread's gwb200_last_error() message and returns `code` (gwb200_abi.cu).
+int gwb200_fail_status(int code, const char* message);
+// Exact-size buffers of a memory-limited handle come from `pool` (gwb200_abi.cu; used by the server).
+void gwb200_attach_pool(gwb200_handle* h, cudaMemPool_t pool);
+
 namespace gwb200 {
 
 // Error carrying a gwb200_status across the host code; converted to a return code

@@ -23,7 +23,7 @@ from typing import Optional, Sequence
 import ctypes as C
 import numpy as np
 
-from ._lib import FP64, MIXED, GwB200Error, Stats, check, dptr, iptr, lib
+from ._lib import FP64, MIXED, GwB200Error, Request, Stats, check, dptr, iptr, lib
 
 HARTREE_TO_EV = 27.211386245988  # include/types.hpp:12
 
@@ -153,6 +153,10 @@ class B200Backend:
             self.close()
         except Exception:
             pass
+
+    def set_memory_limit(self, nbytes: int) -> None:
+        """Cap the device memory this handle holds (0 = no cap)."""
+        check(lib.gwb200_set_memory_limit(self._h, int(nbytes)))
 
     def set_stream(self, stream_ptr: int | None) -> None:
         """Issue all work on a caller's CUDA stream (e.g. torch.cuda.Stream().cuda_stream)."""
@@ -317,3 +321,56 @@ def output_final_energy_table(mo_energy, sigma_x_diag, vxc, qp_energy, states) -
         vals = [mo_energy[idx], sigma_x_diag[idx], sc, vxc[idx, idx], qp_energy[idx]]
         lines.append("{:<10}".format(idx + 1) + "".join("{:<15}".format(_cpp_default(v * HARTREE_TO_EV)) for v in vals))
     return "\n".join(lines) + "\n"
+
+
+class B200Server:
+    """Continuous-batching request loop (gwb200_server_*): `slots` workers, each with its own
+    handle and stream and a device-memory cap of hbm_budget/slots; requests are admitted FIFO as
+    workers free up and run concurrently on the GPU."""
+
+    def __init__(self, device: int = 0, slots: int = 4, hbm_budget_bytes: int = 64 << 30):
+        srv = C.c_void_p()
+        check(lib.gwb200_server_create(device, slots, int(hbm_budget_bytes), C.byref(srv)))
+        self._s = srv
+        self._live = {}
+
+    def submit(self, inp: GwInput, nfreq: int, npade: int, states, eta: float = 0.0, precision="fp64") -> int:
+        nmo = inp.nmo
+        keep = {
+            "mo": np.ascontiguousarray(inp.mo_energy, dtype=np.float64),
+            "eri": np.ascontiguousarray(inp.eri_mo, dtype=np.float64),
+            "vxc": np.ascontiguousarray(inp.vxc_mo, dtype=np.float64),
+            "states": np.ascontiguousarray(states, dtype=np.int64),
+            "omegas": np.zeros(nfreq), "weights": np.zeros(nfreq),
+            "sigma": np.zeros((nmo, nfreq), dtype=np.complex128), "sigma_x_diag": np.zeros(nmo), "qp": np.zeros(nmo),
+        }
+        req = Request(nmo, int(inp.nocc), dptr(keep["mo"]), dptr(keep["eri"]), dptr(keep["vxc"]),
+                      float(inp.fermi_energy), int(nfreq), int(npade), iptr(keep["states"]), len(keep["states"]),
+                      float(eta), _precision_code(precision), dptr(keep["omegas"]), dptr(keep["weights"]),
+                      dptr(keep["sigma"]), dptr(keep["sigma_x_diag"]), dptr(keep["qp"]))
+        keep["req"] = req
+        ticket = C.c_int64()
+        check(lib.gwb200_server_submit(self._s, C.byref(req), C.byref(ticket)))
+        self._live[ticket.value] = keep
+        return ticket.value
+
+    def wait(self, ticket: int) -> dict:
+        st = C.c_int()
+        q, sv, dv = C.c_double(), C.c_double(), C.c_double()
+        rc = lib.gwb200_server_wait(self._s, int(ticket), C.byref(st), C.byref(q), C.byref(sv), C.byref(dv))
+        keep = self._live.pop(int(ticket))
+        check(rc)
+        return {"omegas": keep["omegas"], "weights": keep["weights"], "sigma": keep["sigma"],
+                "sigma_x_diag": keep["sigma_x_diag"], "qp": keep["qp"], "queue_ms": q.value,
+                "service_ms": sv.value, "device_ms": dv.value}
+
+    def close(self) -> None:
+        if self._s:
+            lib.gwb200_server_destroy(self._s)
+            self._s = C.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
