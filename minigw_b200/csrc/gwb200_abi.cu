@@ -115,6 +115,8 @@ struct gwb200_handle {
     DevBuf pqo, xdiag, mo, vxc_diag, delta, v, sigx, flag;  // pqo: the (pq|o.) block of the ERI
     // per-call workspaces (grow-only, reused across calls)
     DevBuf xt, dvec, a, linv, qacc, qall, sigma, omega, weight, states, err, qp, qp_scratch, omega_out;
+    DevBuf panel32;   // split FP32 panel of the mixed form's tcgen05 trailing updates
+    DevBuf tc_sched;  // work counter of the tcgen05 update kernel
     PinnedBuf stage_in, stage_out;
     // cached frequency-chunk size for a repeated geometry (avoids cudaMemGetInfo per call)
     int64_t chunk_key[5] = {-1, -1, -1, -1, -1};
@@ -126,6 +128,13 @@ struct gwb200_handle {
 void gwb200_attach_pool(gwb200_handle* h, cudaMemPool_t pool) { h->pool = pool; }
 
 namespace {
+
+// The mixed form's outer trailing updates run on tcgen05 unless GWB200_MIXED_UPDATE=mma selects the
+// mma.sync kernel (same 3xTF32 arithmetic; kept for comparison).
+bool mixed_update_on_tcgen05() {
+    const char* env = std::getenv("GWB200_MIXED_UPDATE");
+    return !(env && std::strcmp(env, "mma") == 0);
+}
 
 // Allocate `b` for `want` bytes: grow-only, or exact and stream-ordered when the handle is limited.
 void size_buffer(gwb200_handle* h, DevBuf& b, size_t want) {
@@ -204,7 +213,9 @@ void compute_forms(gwb200_handle* h, const double* omega, int64_t nfreq, const i
     GWB_CUDA(cudaMemsetAsync(h->err.p, 0xFF, sizeof(unsigned long long), s));
 
     // Frequency chunk size from the HBM budget: tall matrices + scale vectors + 64x64 inverses.
-    const size_t per_freq = mixed ? sizeof(float) * ((size_t)g.stride + kNb * kNb) + sizeof(double) * (g.n_pad + g.m_pad)
+    const bool mixed_tc = mixed && mixed_update_on_tcgen05();
+    const size_t per_freq = mixed ? sizeof(float) * ((size_t)g.stride + kNb * kNb) + sizeof(double) * (g.n_pad + g.m_pad) +
+                                        (mixed_tc ? tc_panel_bytes_per_freq(g) : 0)
                                   : sizeof(double) * planes * ((size_t)g.stride + g.n_pad + kNb * kNb + g.m_pad);
     // GWB200_MAX_FREQ_CHUNK caps the chunk (tests use it to exercise the multi-chunk path).
     int64_t cap = 0;
@@ -216,7 +227,7 @@ void compute_forms(gwb200_handle* h, const double* omega, int64_t nfreq, const i
     } else {
         size_t free_b = 0, total_b = 0;
         GWB_CUDA(cudaMemGetInfo(&free_b, &total_b));
-        const size_t have = h->a.bytes + h->dvec.bytes + h->linv.bytes + h->qacc.bytes;
+        const size_t have = h->a.bytes + h->dvec.bytes + h->linv.bytes + h->qacc.bytes + h->panel32.bytes;
         size_t avail = free_b + have;  // what the chunk buffers may occupy
         size_t budget = (size_t)((double)avail * 0.85);
         if (h->mem_limit > 0) {  // the handle's cap minus what the system and panels already hold
@@ -237,6 +248,10 @@ void compute_forms(gwb200_handle* h, const double* omega, int64_t nfreq, const i
     size_buffer(h, h->dvec, sizeof(double) * planes * (size_t)fc * g.n_pad);
     size_buffer(h, h->linv, (mixed ? sizeof(float) : sizeof(double) * planes) * (size_t)fc * kNb * kNb);
     size_buffer(h, h->qacc, sizeof(double) * planes * (size_t)fc * g.m_pad);
+    if (mixed_tc) {
+        size_buffer(h, h->panel32, tc_panel_bytes_per_freq(g) * (size_t)fc);
+        h->tc_sched.ensure(sizeof(unsigned long long));
+    }
 
     GWB_CUDA(cudaEventRecord(h->ev[0], s));
     launches += launch_gather_panel(h->pqo.as<double>(), h->nmo, h->nocc, h->states.as<int64_t>(), nstates,
@@ -265,7 +280,9 @@ void compute_forms(gwb200_handle* h, const double* omega, int64_t nfreq, const i
             launches += launch_build_tall32(g, h->v.as<double>(), h->xt.as<double>(), h->dvec.as<double>(), nf,
                                             h->a.as<float>(), s);
             launches += launch_factor_chunk32(g, nf, h->a.as<float>(), h->linv.as<float>(), h->qacc.as<double>(),
-                                              h->err.as<unsigned long long>(), s, prof.enabled ? &prof : nullptr);
+                                              h->err.as<unsigned long long>(), s, prof.enabled ? &prof : nullptr,
+                                              mixed_tc ? h->panel32.as<float>() : nullptr,
+                                              h->tc_sched.as<unsigned long long>());
         } else {
             launches += launch_build_tall(g, h->v.as<double>(), h->xt.as<double>(), h->dvec.as<double>(), nf,
                                           h->a.as<double>(), s);
@@ -293,6 +310,8 @@ void finish_forms(gwb200_handle* h, gwb200_stats* st) {
     GWB_CUDA(cudaMemcpyAsync(h->stage_out.p, h->err.p, sizeof(unsigned long long), cudaMemcpyDeviceToHost, h->stream));
     GWB_CUDA(cudaStreamSynchronize(h->stream));
     const unsigned long long piv = *h->stage_out.as<unsigned long long>();
+    if (piv == 0)  // a bounded device wait expired (pivots are 1-based)
+        fail(GWB200_DEVICE_TIMEOUT, "a device-side wait of the tcgen05 update expired; results discarded");
     if (piv != std::numeric_limits<unsigned long long>::max()) {
         if (st) st->info = (int64_t)piv;
         fail(GWB200_NOT_SPD, "eps(iw) is not positive definite: Cholesky pivot " + std::to_string(piv) + " <= 0");
@@ -386,7 +405,7 @@ int gwb200_destroy(gwb200_handle* h) {
     h->stage_out.release();
     for (DevBuf* b : {&h->pqo, &h->xdiag, &h->mo, &h->vxc_diag, &h->delta, &h->v, &h->sigx, &h->flag, &h->xt, &h->dvec, &h->a,
                       &h->linv, &h->qacc, &h->qall, &h->sigma, &h->omega, &h->weight, &h->states, &h->err, &h->qp,
-                      &h->qp_scratch, &h->omega_out})
+                      &h->qp_scratch, &h->omega_out, &h->panel32, &h->tc_sched})
         b->release();
     for (auto& e : h->ev)
         if (e) cudaEventDestroy(e);
@@ -426,7 +445,7 @@ int gwb200_load_system(gwb200_handle* h, int64_t nmo, int64_t nocc, const double
         // Only the (pq|o.) block is uploaded: every V_ph / panel element has an occupied third
         // index.  One 2D copy: nmo^2 rows of nocc*nmo contiguous doubles, source pitch nmo^2.
         if (h->mem_limit > 0)  // drop the previous request's workspaces before sizing this system
-            for (DevBuf* b : {&h->xt, &h->dvec, &h->a, &h->linv, &h->qacc, &h->qall}) b->release();
+            for (DevBuf* b : {&h->xt, &h->dvec, &h->a, &h->linv, &h->qacc, &h->qall, &h->panel32}) b->release();
         size_buffer(h, h->pqo, sizeof(double) * nmo2 * nocc * nmo);
         size_buffer(h, h->xdiag, sizeof(double) * nmo * nocc);
         h->mo.ensure(sizeof(double) * nmo);

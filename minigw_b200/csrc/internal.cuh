@@ -142,8 +142,18 @@ double measure_fp64_peak_tflops(cudaStream_t s);
 // kernels_f32.cu: the mixed-precision form (FP32 tall matrices, 3xTF32 tensor-core updates).
 int launch_build_tall32(const TallGeometry& g, const double* v, const double* xt, const double* dvec, int64_t nf,
                         float* a, cudaStream_t s);
+// panel != NULL: the outer trailing updates run on tcgen05 (kernels_tc.cu) with `panel` as the
+// split-panel workspace (tc_panel_bytes_per_freq(g) bytes per frequency); NULL: mma.sync.
 int launch_factor_chunk32(const TallGeometry& g, int64_t nf, float* a, float* linv, double* qacc,
-                          unsigned long long* err_pivot, cudaStream_t s, UpdateProfiler* prof);
+                          unsigned long long* err_pivot, cudaStream_t s, UpdateProfiler* prof, float* panel,
+                          unsigned long long* sched);
+// kernels_tc.cu: tcgen05 3xTF32 trailing update C -= P P^T of the mixed form (K = kdim columns from
+// kb0, output columns [c_begin, n_pad), rows [c_begin, rows)).  Two launches; `sched` is one
+// device word the kernel's work counter lives in.  A device wait that expires records pivot 0 in
+// err_pivot.
+size_t tc_panel_bytes_per_freq(const TallGeometry& g);
+int launch_update32_tc(const TallGeometry& g, int64_t nf, float* a, int64_t kb0, int kdim, int64_t c_begin,
+                       float* panel, unsigned long long* sched, unsigned long long* err_pivot, cudaStream_t s);
 // kernels_c64.cu: eta != 0 (complex symmetric M = I - S V S, S = diag(Pi0)^1/2).  Planes a_re/a_im
 // of geometry g; svec 2*n_pad, linv 2*64*64, qacc 2*m_pad doubles per frequency.
 int launch_factor_chunk_c(const TallGeometry& g, int64_t nf, const double* delta, const double* omega, double eta,

@@ -1,0 +1,564 @@
+// kernels_tc.cu -- the mixed form's trailing update on the 5th-generation tensor cores (tcgen05).
+//
+// After an outer block of K = 64 or 128 columns [kb0, kb0+K) has been factored, every element of
+// the trailing lower part C = A[r][c] (c_begin <= c < n_pad, c <= r < rows) takes
+// C -= P_r . P_c with P the FP32 panel A[:, kb0:kb0+K).  The products use the 3xTF32 split
+// (x = hi + lo, hi = rna_tf32(x), lo = rna_tf32(x - hi); x.y ~ lo.hi + hi.lo + hi.hi, in that
+// order per 8-deep K step) accumulated in FP32: the same arithmetic, in the same order, as the
+// mma.sync update of kernels_f32.cu.
+//
+// Two launches per update:
+//   k_split_panel32  writes hi and lo of the panel rows [c_begin, rows) in the 128-byte-swizzled
+//                    K-major layout the tensor core reads ([K slice of 32 floats][row][128 bytes],
+//                    rows padded with zeros to a multiple of 128), so that every operand slice of a
+//                    tile is one contiguous 16 KB block (one cp.async.bulk);
+//   k_update32_tc    a persistent, warp-specialised kernel, one CTA per SM (576 threads, 226 KB of
+//                    shared memory, 256 TMEM columns):
+//                      warp 0     producer: takes work units from a global counter and hands them
+//                                 to the other roles through a 4-slot mbarrier ring; loads the
+//                                 unit's A (128 rows x K, hi and lo: 128 KB, resident for the whole
+//                                 unit) and streams B (128 rows x 32 of K, hi and lo) through a
+//                                 3-stage ring;
+//                      warp 1     allocates TMEM; lane 0 issues tcgen05.mma kind::tf32 (M = 128,
+//                                 N = 128, K = 8 per instruction, K-major SW128 operands) into a
+//                                 double-buffered FP32 accumulator and commits stage releases,
+//                                 accumulator-ready and A-release to mbarriers;
+//                      warps 2-17 epilogue: warp w reads TMEM lane quadrant w % 4, 32 columns;
+//                                 loads its C row segment before the accumulator is ready,
+//                                 tcgen05.ld, releases the accumulator, stores C - acc.
+// A work unit is (frequency, 128-row tile i, up to 16 column tiles of 128); column tile c of row
+// tile i has work iff c <= i, and units of the longest row tiles are handed out first.  Writes are
+// limited to the lower part at 64-column-block granularity (the diagonal 64 x 64 blocks in full,
+// as the other update kernels do).
+//
+// Every mbarrier wait is bounded (kWaitNs of %globaltimer); on expiry the CTA raises a shared
+// abort flag, records 0 in the pivot word (read back by the host as GWB200_DEVICE_TIMEOUT), waits
+// (bounded) for its own bulk copies and MMAs, frees its TMEM and returns.
+#include "internal.cuh"
+
+#include <mutex>
+
+namespace gwb200 {
+namespace {
+
+constexpr int kTcM = 128;                   // accumulator rows = TMEM lanes = A rows per unit
+constexpr int kTcN = 128;                   // accumulator columns per tile
+constexpr int kTcKc = 32;                   // floats of K per B pipeline stage
+constexpr int kTcStages = 3;                // B ring depth
+constexpr int kTcSeg = 16;                  // column tiles per work unit (A is loaded once per unit)
+constexpr int kSchedSlots = 4;              // unit-index ring from the producer to the other roles
+constexpr int kRowBytes = kTcKc * 4;        // one row of a K slice: 128 bytes = one swizzle atom row
+constexpr int kSliceA = kTcM * kRowBytes;   // hi (or lo) of one K slice of 128 rows: 16384 bytes
+constexpr int kSliceB = kTcN * kRowBytes;   // 16384 bytes
+constexpr int kAHalf = 4 * kSliceA;         // hi (or lo) of A for K = 128: 65536 bytes
+constexpr int kStageBytes = 2 * kSliceB;    // B stage: hi + lo slice, two copies
+constexpr int kEpiWarps = 16;               // 4 lane quadrants x 4 column quarters of 32
+constexpr int kTcThreads = 32 * (2 + kEpiWarps);
+constexpr int kTmemCols = 2 * kTcN;  // two accumulators of 128 FP32 columns
+constexpr int kHeader = 1024;        // mbarriers, unit ring, TMEM address, abort flag
+// + 1024: the operand region starts at the first 1024-byte boundary after the header (the
+// 128-byte swizzle is applied to shared-memory address bits, so every slice is 1024-aligned)
+constexpr int kTcSmem = kHeader + 1024 + 2 * kAHalf + kTcStages * kStageBytes;
+constexpr unsigned long long kWaitNs = 2000000000ull;
+
+// header layout (byte offsets)
+constexpr int kOffFull = 0;                              // kTcStages: B stage filled (tx bytes)
+constexpr int kOffEmpty = kOffFull + 8 * kTcStages;      // kTcStages: B stage consumed (tcgen05.commit)
+constexpr int kOffTFull = kOffEmpty + 8 * kTcStages;     // 2: accumulator ready (tcgen05.commit)
+constexpr int kOffTEmpty = kOffTFull + 16;               // 2: accumulator drained (kEpiWarps arrivals)
+constexpr int kOffAFull = kOffTEmpty + 16;               // 1: A of the unit loaded (tx bytes)
+constexpr int kOffAEmpty = kOffAFull + 8;                // 1: all MMAs reading A of the unit complete
+constexpr int kOffDrain = kOffAEmpty + 8;                // 1: all MMAs of this CTA complete
+constexpr int kOffUFull = kOffDrain + 8;                 // kSchedSlots: unit index written
+constexpr int kOffUEmpty = kOffUFull + 8 * kSchedSlots;  // kSchedSlots: read by MMA + epilogue warps
+constexpr int kOffUnit = kOffUEmpty + 8 * kSchedSlots;   // kSchedSlots x i64 unit indices
+constexpr int kOffTmem = kOffUnit + 8 * kSchedSlots;     // u32 TMEM base address
+constexpr int kOffAbort = kOffTmem + 4;                  // u32 abort flag
+
+static_assert(kOffAbort + 4 <= kHeader, "header overflow");
+static_assert(kTcSmem <= 227 * 1024, "shared memory");
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ unsigned long long globaltimer() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.b32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// Wait for the phase of parity `parity` to complete; false on abort or expiry (which raises abort
+// and records the timeout).
+__device__ __noinline__ bool mbar_wait(uint32_t bar, uint32_t parity, volatile uint32_t* abort_flag,
+                                       unsigned long long* err) {
+    if (mbar_try(bar, parity)) return true;
+    const unsigned long long t0 = globaltimer();
+    for (;;) {
+        if (mbar_try(bar, parity)) return true;
+        if (*abort_flag) return false;
+        if (globaltimer() - t0 > kWaitNs) {
+            *abort_flag = 1u;
+            atomicMin(err, 0ull);
+            return false;
+        }
+    }
+}
+// Bounded wait used only while draining: no abort check, no error record.
+__device__ __forceinline__ void mbar_drain(uint32_t bar, uint32_t parity) {
+    if (mbar_try(bar, parity)) return;
+    const unsigned long long t0 = globaltimer();
+    while (!mbar_try(bar, parity) && globaltimer() - t0 < kWaitNs) {
+    }
+}
+
+__device__ __forceinline__ void bulk_g2s(uint32_t dst, const void* src, uint32_t bytes, uint32_t bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+                 "l"(src), "r"(bytes), "r"(bar)
+                 : "memory");
+}
+
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+// Shared-memory matrix descriptor, K-major, 128-byte swizzle: rows of 128 bytes (32 floats of K),
+// 8-row groups of 1024 bytes (SBO), 16-byte chunk c of row r stored at chunk c ^ (r % 8); the
+// start address advances by 32 bytes per 8-deep K step inside the 128-byte row; LBO (unused for
+// swizzled K-major) 16 bytes; version 1 (bit 46), base offset 0 (1024-aligned slices), layout
+// type 2 = SWIZZLE_128B (bits 61-63).
+__device__ __forceinline__ uint64_t smem_desc_sw128(uint32_t addr) {
+    return (uint64_t)((addr >> 4) & 0x3FFFu) | ((uint64_t)(16 >> 4) << 16) | ((uint64_t)(1024 >> 4) << 32) |
+           (1ull << 46) | (2ull << 61);
+}
+// Instruction descriptor, kind::tf32: D FP32 (bits 4-5 = 1), A and B TF32 (bits 7-9, 10-12 = 2),
+// both K-major (bits 15, 16 = 0), N >> 3 at bits 17-22, M >> 4 at bits 24-28.
+constexpr uint32_t kIdescTf32 =
+    (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(kTcN >> 3) << 17) | ((uint32_t)(kTcM >> 4) << 24);
+
+__device__ __forceinline__ void mma_tf32(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
+        "l"(da), "l"(db), "r"(kIdescTf32), "r"(accumulate)
+        : "memory");
+}
+__device__ __forceinline__ void mma_commit(uint32_t bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar) : "memory");
+}
+
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32]) {
+    uint32_t r[32];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+        "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+          "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+          "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int j = 0; j < 32; ++j) v[j] = __uint_as_float(r[j]);
+}
+
+__device__ __forceinline__ float rna_tf32(float x) {
+    uint32_t r;
+    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+    return __uint_as_float(r);
+}
+
+// hi/lo of panel rows [c_begin, rows) x columns [kb0, kb0 + 32 nkc) in the 128-byte-swizzled
+// K-major layout: [K slice of 32 floats][row][128 bytes], the 16-byte chunk c of row rr stored at
+// chunk position c ^ (rr % 8); rows [rows - c_begin, rp) are zero.  Per frequency: hi at
+// panel + f*2*nkc*rp*32, lo nkc*rp*32 floats later.  One thread per 16-byte chunk.
+__global__ void k_split_panel32(const float* __restrict__ a, int64_t ld, int64_t stride, int64_t kb0, int nkc,
+                                int64_t c_begin, int64_t rows, int64_t rp, float* __restrict__ panel) {
+    const int f = blockIdx.y;
+    const float* A = a + (size_t)f * stride;
+    float4* hi = reinterpret_cast<float4*>(panel + (size_t)f * 2 * nkc * rp * 32);
+    float4* lo = hi + (size_t)nkc * rp * 8;
+    const int64_t total = (int64_t)nkc * rp * 8;
+    for (int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
+         idx += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t srow = idx >> 3;  // kb * rp + rr
+        const int c = (int)(idx & 7);
+        const int64_t kb = srow / rp, rr = srow - kb * rp;
+        const int64_t r = c_begin + rr;
+        float4 x = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (r < rows) x = *reinterpret_cast<const float4*>(A + (size_t)r * ld + kb0 + 32 * kb + 4 * c);
+        float4 h, l;
+        h.x = rna_tf32(x.x);
+        h.y = rna_tf32(x.y);
+        h.z = rna_tf32(x.z);
+        h.w = rna_tf32(x.w);
+        l.x = rna_tf32(x.x - h.x);
+        l.y = rna_tf32(x.y - h.y);
+        l.z = rna_tf32(x.z - h.z);
+        l.w = rna_tf32(x.w - h.w);
+        const int64_t dst = srow * 8 + (c ^ (int)(rr & 7));
+        hi[dst] = h;
+        lo[dst] = l;
+    }
+}
+
+// Work units: (frequency, 128-row tile i, segment of kTcSeg column tiles of 128).  Column tile c
+// of row tile i holds something to write iff c <= i; a unit covers column tiles
+// [seg*kTcSeg, min((seg+1)*kTcSeg, T, i+1)).  Within a frequency the units of the longest row
+// tiles (largest i) come first; CTAs take units in that order from a global counter.
+struct UnitSpace {
+    int64_t T, NI, NS, per_f, total;
+};
+
+__device__ __forceinline__ bool decode_unit(const UnitSpace& us, int64_t u, int& f, int64_t& i, int64_t& c0,
+                                            int64_t& c1) {
+    f = (int)(u / us.per_f);
+    const int64_t rem = u - (int64_t)f * us.per_f;
+    const int64_t q = rem / us.NS;
+    i = us.NI - 1 - q;
+    c0 = (rem - q * us.NS) * kTcSeg;
+    c1 = min(c0 + kTcSeg, min(us.T, i + 1));
+    return c0 < c1;
+}
+
+// Consumer side of the unit ring: the next unit index (>= total: no more work), or -1 on abort.
+__device__ __forceinline__ int64_t take_unit(uint32_t ufull, uint32_t uempty, const volatile int64_t* slot,
+                                             uint32_t parity, volatile uint32_t* abort_flag, unsigned long long* err) {
+    if (!mbar_wait(ufull, parity, abort_flag, err)) return -1;
+    const int64_t u = *slot;
+    mbar_arrive(uempty);
+    return u;
+}
+
+__global__ void __launch_bounds__(kTcThreads, 1)
+    k_update32_tc(float* __restrict__ a, int64_t ld, int64_t stride, int64_t c_begin, int64_t rows, int64_t n_pad,
+                  int nkc, const float* __restrict__ panel, int64_t rp, UnitSpace us,
+                  unsigned long long* __restrict__ sched, unsigned long long* err) {
+    extern __shared__ __align__(1024) uint8_t tsm[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint32_t base = smem_u32(tsm);
+    const uint32_t abuf = (base + kHeader + 1023u) & ~1023u;  // A hi at abuf, A lo at abuf + kAHalf
+    const uint32_t ring = abuf + 2 * kAHalf;                   // B stages
+    volatile uint32_t* abort_flag = reinterpret_cast<volatile uint32_t*>(tsm + kOffAbort);
+    volatile int64_t* uslot = reinterpret_cast<volatile int64_t*>(tsm + kOffUnit);
+    auto full = [&](int s) { return base + kOffFull + 8 * s; };
+    auto empty = [&](int s) { return base + kOffEmpty + 8 * s; };
+    auto tfull = [&](int b) { return base + kOffTFull + 8 * b; };
+    auto tempty = [&](int b) { return base + kOffTEmpty + 8 * b; };
+    auto ufull = [&](int j) { return base + kOffUFull + 8 * j; };
+    auto uempty = [&](int j) { return base + kOffUEmpty + 8 * j; };
+    const uint32_t afull = base + kOffAFull, aempty = base + kOffAEmpty, drain = base + kOffDrain;
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < kTcStages; ++s) {
+            mbar_init(full(s), 1);
+            mbar_init(empty(s), 1);
+        }
+        for (int b = 0; b < 2; ++b) {
+            mbar_init(tfull(b), 1);
+            mbar_init(tempty(b), kEpiWarps);
+        }
+        for (int j = 0; j < kSchedSlots; ++j) {
+            mbar_init(ufull(j), 1);
+            mbar_init(uempty(j), 1 + kEpiWarps);
+        }
+        mbar_init(afull, 1);
+        mbar_init(aempty, 1);
+        mbar_init(drain, 1);
+        *abort_flag = 0u;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    }
+    if (warp == 1) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(base + kOffTmem),
+                     "r"(kTmemCols)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *reinterpret_cast<volatile uint32_t*>(tsm + kOffTmem);
+
+    const size_t half_floats = (size_t)nkc * rp * 32;  // hi (or lo) of one frequency
+    const uint32_t a_bytes = 2u * nkc * kSliceA;
+
+    if (warp == 0) {
+        // ---- producer: takes units from the global counter, hands them on, loads A and B ----
+        int s = 0, js = 0;
+        uint32_t ph = 0, aph = 0, jph = 0;
+        uint32_t filled = 0, fill_par = 0;  // per B stage: ever filled, parity of its last fill
+        bool a_filled = false;
+        for (;;) {
+            int f = 0;
+            int64_t i = 0, c0 = 0, c1 = 0, u = 0;
+            if (lane == 0) {
+                do {
+                    u = (int64_t)atomicAdd(sched, 1ull);
+                } while (u < us.total && !decode_unit(us, u, f, i, c0, c1));
+                if (u > us.total) u = us.total;
+            }
+            u = __shfl_sync(0xffffffffu, u, 0);
+            uint32_t got = 1;
+            if (lane == 0) {
+                got = mbar_wait(uempty(js), jph ^ 1u, abort_flag, err) ? 1u : 0u;
+                if (got) {
+                    uslot[js] = u;
+                    mbar_arrive(ufull(js));
+                }
+            }
+            got = __shfl_sync(0xffffffffu, got, 0);
+            if (!got) break;
+            if (++js == kSchedSlots) {
+                js = 0;
+                jph ^= 1u;
+            }
+            if (u >= us.total) break;
+            decode_unit(us, u, f, i, c0, c1);
+            const float* hi = panel + (size_t)f * 2 * half_floats;
+            const float* lo = hi + half_floats;
+            // A of the unit, once the previous unit's MMAs are done with it
+            if (lane == 0) got = mbar_wait(aempty, aph ^ 1u, abort_flag, err) ? 1u : 0u;
+            got = __shfl_sync(0xffffffffu, got, 0);
+            if (!got) break;
+            if (lane == 0) mbar_expect_tx(afull, a_bytes);
+            __syncwarp();
+            if (lane < 2 * nkc) {  // one 16 KB copy per (hi|lo, K slice)
+                const int which = lane / nkc, kb = lane - which * nkc;
+                const float* src = (which == 0 ? hi : lo) + (size_t)((int64_t)kb * rp + i * kTcM) * 32;
+                bulk_g2s(abuf + which * kAHalf + kb * kSliceA, src, kSliceA, afull);
+            }
+            a_filled = true;
+            aph ^= 1u;
+            bool ok = true;
+            for (int64_t c = c0; ok && c < c1; ++c) {
+                for (int kb = 0; kb < nkc; ++kb) {
+                    if (lane == 0) got = mbar_wait(empty(s), ph ^ 1u, abort_flag, err) ? 1u : 0u;
+                    got = __shfl_sync(0xffffffffu, got, 0);
+                    if (!got) {
+                        ok = false;
+                        break;
+                    }
+                    if (lane == 0) mbar_expect_tx(full(s), kStageBytes);
+                    __syncwarp();
+                    if (lane < 2) {  // one 16 KB copy each of hi and lo
+                        const float* src = (lane == 0 ? hi : lo) + (size_t)((int64_t)kb * rp + c * kTcN) * 32;
+                        bulk_g2s(ring + s * kStageBytes + lane * kSliceB, src, kSliceB, full(s));
+                    }
+                    filled |= 1u << s;
+                    fill_par = (fill_par & ~(1u << s)) | (ph << s);
+                    if (++s == kTcStages) {
+                        s = 0;
+                        ph ^= 1u;
+                    }
+                }
+            }
+            if (!ok) break;
+        }
+        // every issued copy has landed before the CTA may exit (normally already consumed)
+        if (lane == 0) {
+            for (int q = 0; q < kTcStages; ++q)
+                if (filled & (1u << q)) mbar_drain(full(q), (fill_par >> q) & 1u);
+            if (a_filled) mbar_drain(afull, aph ^ 1u);
+        }
+        __syncwarp();
+    } else if (warp == 1 && lane == 0) {
+        // ---- MMA issuer: one thread waits, issues and commits ----
+        int s = 0, ab = 0, js = 0;
+        uint32_t ph = 0, acc_ph = 0, aph = 0, jph = 0;
+        bool issued = false, ok = true;
+        for (;;) {
+            const int64_t u = take_unit(ufull(js), uempty(js), uslot + js, jph, abort_flag, err);
+            if (++js == kSchedSlots) {
+                js = 0;
+                jph ^= 1u;
+            }
+            if (u < 0 || u >= us.total) break;
+            int f;
+            int64_t i, c0, c1;
+            decode_unit(us, u, f, i, c0, c1);
+            if (!mbar_wait(afull, aph, abort_flag, err)) break;
+            aph ^= 1u;
+            for (int64_t c = c0; ok && c < c1; ++c) {
+                if (!mbar_wait(tempty(ab), acc_ph ^ 1u, abort_flag, err)) {
+                    ok = false;
+                    break;
+                }
+                tc_fence_after();
+                const uint32_t d = tmem + (uint32_t)(ab * kTcN);
+                for (int kb = 0; kb < nkc; ++kb) {
+                    if (!mbar_wait(full(s), ph, abort_flag, err)) {
+                        ok = false;
+                        break;
+                    }
+                    tc_fence_after();
+                    const uint32_t st = ring + s * kStageBytes;
+#pragma unroll
+                    for (int kk = 0; kk < kTcKc / 8; ++kk) {
+                        const uint32_t ak = abuf + (uint32_t)kb * kSliceA + 32u * kk;
+                        const uint64_t ahi = smem_desc_sw128(ak);
+                        const uint64_t alo = smem_desc_sw128(ak + kAHalf);
+                        const uint64_t bhi = smem_desc_sw128(st + 32u * kk);
+                        const uint64_t blo = smem_desc_sw128(st + kSliceB + 32u * kk);
+                        mma_tf32(d, alo, bhi, (kb > 0 || kk > 0) ? 1u : 0u);
+                        mma_tf32(d, ahi, blo, 1u);
+                        mma_tf32(d, ahi, bhi, 1u);
+                    }
+                    mma_commit(empty(s));
+                    issued = true;
+                    if (++s == kTcStages) {
+                        s = 0;
+                        ph ^= 1u;
+                    }
+                }
+                if (!ok) break;
+                mma_commit(tfull(ab));
+                if (++ab == 2) {
+                    ab = 0;
+                    acc_ph ^= 1u;
+                }
+            }
+            if (!ok) break;
+            mma_commit(aempty);
+        }
+        // all MMAs of this CTA complete before TMEM is released
+        if (issued) {
+            mma_commit(drain);
+            mbar_drain(drain, 0);
+        }
+    } else if (warp >= 2) {
+        // ---- epilogue: warp -> TMEM lane quadrant (warp % 4) and 32-column quarter ----
+        const int q = warp & 3, quarter = (warp - 2) >> 2;
+        int ab = 0, js = 0;
+        uint32_t acc_ph = 0, jph = 0;
+        bool ok = true;
+        while (ok) {
+            int64_t u = 0;
+            if (lane == 0) u = take_unit(ufull(js), uempty(js), uslot + js, jph, abort_flag, err);
+            u = __shfl_sync(0xffffffffu, u, 0);
+            if (++js == kSchedSlots) {
+                js = 0;
+                jph ^= 1u;
+            }
+            if (u < 0 || u >= us.total) break;
+            int f;
+            int64_t i, c0, c1;
+            decode_unit(us, u, f, i, c0, c1);
+            const int64_t r = c_begin + i * kTcM + q * 32 + lane;
+            for (int64_t c = c0; c < c1; ++c) {
+                const int64_t cj = c_begin + c * kTcN + quarter * 32;  // this thread's 32 columns
+                // lower part at 64-column-block granularity (the diagonal 64x64 blocks in full)
+                const bool valid = r < rows && cj < n_pad && r >= (cj & ~(int64_t)63);
+                float* crow = a + (size_t)f * stride + (size_t)(valid ? r : 0) * ld + (valid ? cj : 0);
+                float4 cv[8];
+                if (valid) {
+#pragma unroll
+                    for (int j = 0; j < 8; ++j) cv[j] = reinterpret_cast<const float4*>(crow)[j];
+                }
+                uint32_t got = 1;
+                if (lane == 0) got = mbar_wait(tfull(ab), acc_ph, abort_flag, err) ? 1u : 0u;
+                got = __shfl_sync(0xffffffffu, got, 0);
+                if (!got) {
+                    ok = false;
+                    break;
+                }
+                tc_fence_after();
+                float acc[32];
+                tmem_ld32(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(ab * kTcN + quarter * 32), acc);
+                tc_fence_before();
+                __syncwarp();
+                if (lane == 0) mbar_arrive(tempty(ab));
+                if (valid) {
+#pragma unroll
+                    for (int j = 0; j < 8; ++j) {
+                        float4 v = cv[j];
+                        v.x -= acc[4 * j];
+                        v.y -= acc[4 * j + 1];
+                        v.z -= acc[4 * j + 2];
+                        v.w -= acc[4 * j + 3];
+                        reinterpret_cast<float4*>(crow)[j] = v;
+                    }
+                }
+                if (++ab == 2) {
+                    ab = 0;
+                    acc_ph ^= 1u;
+                }
+            }
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 1) {
+        __syncwarp();
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols) : "memory");
+    }
+}
+
+int sm_count() {
+    static int n = 0;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n <= 0) n = 148;
+    });
+    return n;
+}
+
+} // namespace
+
+size_t tc_panel_bytes_per_freq(const TallGeometry& g) {
+    const int64_t rp = (g.rows + kTcM - 1) / kTcM * kTcM;
+    return (size_t)2 * (128 / 4) * (size_t)rp * 16;
+}
+
+int launch_update32_tc(const TallGeometry& g, int64_t nf, float* a, int64_t kb0, int kdim, int64_t c_begin,
+                       float* panel, unsigned long long* sched, unsigned long long* err, cudaStream_t s) {
+    if (kdim <= 0 || kdim > 128 || kdim % kTcKc != 0)
+        fail(GWB200_BAD_SHAPE, "tcgen05 update: K must be 32, 64, 96 or 128");
+    const int64_t T = (g.n_pad - c_begin + kTcN - 1) / kTcN;  // the last column tile may be 64 wide
+    if (T <= 0 || nf <= 0) return 0;
+    const int64_t H = g.rows - c_begin;
+    const int64_t NI = (H + kTcM - 1) / kTcM, rp = NI * kTcM;
+    const int nkc = kdim / kTcKc;
+    {
+        const int64_t total = (int64_t)nkc * rp * 8;
+        const unsigned gx = (unsigned)std::min<int64_t>((total + 255) / 256, 4096);
+        k_split_panel32<<<dim3(gx, (unsigned)nf), 256, 0, s>>>(a, g.ld, g.stride, kb0, nkc, c_begin, g.rows, rp, panel);
+        GWB_LAUNCH("k_split_panel32");
+    }
+    GWB_CUDA(cudaFuncSetAttribute(k_update32_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmem));
+    UnitSpace us;
+    us.T = T;
+    us.NI = NI;
+    us.NS = (T + kTcSeg - 1) / kTcSeg;
+    us.per_f = NI * us.NS;
+    us.total = nf * us.per_f;
+    GWB_CUDA(cudaMemsetAsync(sched, 0, sizeof(unsigned long long), s));
+    const unsigned grid = (unsigned)std::min<int64_t>(us.total, sm_count());
+    k_update32_tc<<<grid, kTcThreads, kTcSmem, s>>>(a, g.ld, g.stride, c_begin, g.rows, g.n_pad, nkc, panel, rp, us,
+                                                     sched, err);
+    GWB_LAUNCH("k_update32_tc");
+    return 2;
+}
+
+} // namespace gwb200
