@@ -24,8 +24,8 @@
 //                                 double-buffered FP32 accumulator and commits stage releases,
 //                                 accumulator-ready and A-release to mbarriers;
 //                      warps 2-17 epilogue: warp w reads TMEM lane quadrant w % 4, 32 columns;
-//                                 loads its C row segment before the accumulator is ready,
-//                                 tcgen05.ld, releases the accumulator, stores C - acc.
+//                                 tcgen05.ld, releases the accumulator, and adds -acc to C with
+//                                 16-byte vector reductions (the read-modify-write happens in L2).
 // A work unit is (frequency, 128-row tile i, up to 16 column tiles of 128); column tile c of row
 // tile i has work iff c <= i, and units of the longest row tiles are handed out first.  Writes are
 // limited to the lower part at 64-column-block granularity (the diagonal 64 x 64 blocks in full,
@@ -467,12 +467,8 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                 const int64_t cj = c_begin + c * kTcN + quarter * 32;  // this thread's 32 columns
                 // lower part at 64-column-block granularity (the diagonal 64x64 blocks in full)
                 const bool valid = r < rows && cj < n_pad && r >= (cj & ~(int64_t)63);
-                float* crow = a + (size_t)f * stride + (size_t)(valid ? r : 0) * ld + (valid ? cj : 0);
-                float4 cv[8];
-                if (valid) {
-#pragma unroll
-                    for (int j = 0; j < 8; ++j) cv[j] = reinterpret_cast<const float4*>(crow)[j];
-                }
+                float4* crow = reinterpret_cast<float4*>(a + (size_t)f * stride + (size_t)(valid ? r : 0) * ld +
+                                                         (valid ? cj : 0));
                 uint32_t got = 1;
                 if (lane == 0) got = mbar_wait(tfull(ab), acc_ph, abort_flag, err) ? 1u : 0u;
                 got = __shfl_sync(0xffffffffu, got, 0);
@@ -486,16 +482,12 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                 tc_fence_before();
                 __syncwarp();
                 if (lane == 0) mbar_arrive(tempty(ab));
+                // C += (-acc) as vector reductions performed in L2: no load on this SM, and every
+                // element receives exactly one addition per launch (same rounding as C - acc)
                 if (valid) {
 #pragma unroll
-                    for (int j = 0; j < 8; ++j) {
-                        float4 v = cv[j];
-                        v.x -= acc[4 * j];
-                        v.y -= acc[4 * j + 1];
-                        v.z -= acc[4 * j + 2];
-                        v.w -= acc[4 * j + 3];
-                        reinterpret_cast<float4*>(crow)[j] = v;
-                    }
+                    for (int j = 0; j < 8; ++j)
+                        atomicAdd(crow + j, make_float4(-acc[4 * j], -acc[4 * j + 1], -acc[4 * j + 2], -acc[4 * j + 3]));
                 }
                 if (++ab == 2) {
                     ab = 0;
