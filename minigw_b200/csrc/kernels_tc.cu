@@ -36,6 +36,7 @@
 // (bounded) for its own bulk copies and MMAs, frees its TMEM and returns.
 #include "internal.cuh"
 
+#include <cstdlib>
 #include <mutex>
 
 namespace gwb200 {
@@ -44,21 +45,20 @@ namespace {
 constexpr int kTcM = 128;                   // accumulator rows = TMEM lanes = A rows per unit
 constexpr int kTcN = 128;                   // accumulator columns per tile
 constexpr int kTcKc = 32;                   // floats of K per B pipeline stage
-constexpr int kTcStages = 3;                // B ring depth
+constexpr int kTcStages = 6;                // B ring depth
 constexpr int kTcSeg = 16;                  // column tiles per work unit (A is loaded once per unit)
 constexpr int kSchedSlots = 4;              // unit-index ring from the producer to the other roles
 constexpr int kRowBytes = kTcKc * 4;        // one row of a K slice: 128 bytes = one swizzle atom row
-constexpr int kSliceA = kTcM * kRowBytes;   // hi (or lo) of one K slice of 128 rows: 16384 bytes
 constexpr int kSliceB = kTcN * kRowBytes;   // 16384 bytes
-constexpr int kAHalf = 4 * kSliceA;         // hi (or lo) of A for K = 128: 65536 bytes
 constexpr int kStageBytes = 2 * kSliceB;    // B stage: hi + lo slice, two copies
 constexpr int kEpiWarps = 16;               // 4 lane quadrants x 4 column quarters of 32
 constexpr int kTcThreads = 32 * (2 + kEpiWarps);
-constexpr int kTmemCols = 2 * kTcN;  // two accumulators of 128 FP32 columns
+constexpr int kTmemCols = 512;       // accumulators [0, 256), A hi [256, 384), A lo [384, 512)
+constexpr int kTmemAHi = 2 * kTcN, kTmemALo = kTmemAHi + 128;
 constexpr int kHeader = 1024;        // mbarriers, unit ring, TMEM address, abort flag
 // + 1024: the operand region starts at the first 1024-byte boundary after the header (the
 // 128-byte swizzle is applied to shared-memory address bits, so every slice is 1024-aligned)
-constexpr int kTcSmem = kHeader + 1024 + 2 * kAHalf + kTcStages * kStageBytes;
+constexpr int kTcSmem = kHeader + 1024 + kTcStages * kStageBytes;
 constexpr unsigned long long kWaitNs = 2000000000ull;
 
 // header layout (byte offsets)
@@ -66,7 +66,7 @@ constexpr int kOffFull = 0;                              // kTcStages: B stage f
 constexpr int kOffEmpty = kOffFull + 8 * kTcStages;      // kTcStages: B stage consumed (tcgen05.commit)
 constexpr int kOffTFull = kOffEmpty + 8 * kTcStages;     // 2: accumulator ready (tcgen05.commit)
 constexpr int kOffTEmpty = kOffTFull + 16;               // 2: accumulator drained (kEpiWarps arrivals)
-constexpr int kOffAFull = kOffTEmpty + 16;               // 1: A of the unit loaded (tx bytes)
+constexpr int kOffAFull = kOffTEmpty + 16;               // 1: A of the unit in TMEM (kEpiWarps arrivals)
 constexpr int kOffAEmpty = kOffAFull + 8;                // 1: all MMAs reading A of the unit complete
 constexpr int kOffDrain = kOffAEmpty + 8;                // 1: all MMAs of this CTA complete
 constexpr int kOffUFull = kOffDrain + 8;                 // kSchedSlots: unit index written
@@ -153,12 +153,23 @@ __device__ __forceinline__ uint64_t smem_desc_sw128(uint32_t addr) {
 constexpr uint32_t kIdescTf32 =
     (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(kTcN >> 3) << 17) | ((uint32_t)(kTcM >> 4) << 24);
 
-__device__ __forceinline__ void mma_tf32(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t accumulate) {
+// A from TMEM (lane = row, one 32-bit column per K element), B from shared memory.
+__device__ __forceinline__ void mma_tf32_ts(uint32_t tmem_d, uint32_t tmem_a, uint64_t db, uint32_t accumulate) {
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
         "setp.ne.b32 p, %4, 0;\n\t"
-        "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
-        "l"(da), "l"(db), "r"(kIdescTf32), "r"(accumulate)
+        "tcgen05.mma.cta_group::1.kind::tf32 [%0], [%1], %2, %3, p;\n\t}" ::"r"(tmem_d),
+        "r"(tmem_a), "l"(db), "r"(kIdescTf32), "r"(accumulate)
+        : "memory");
+}
+__device__ __forceinline__ void tmem_st32(uint32_t taddr, const float (&v)[32]) {
+    asm volatile(
+        "tcgen05.st.sync.aligned.32x32b.x32.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16,"
+        "%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31,%32};" ::"r"(taddr),
+        "f"(v[0]), "f"(v[1]), "f"(v[2]), "f"(v[3]), "f"(v[4]), "f"(v[5]), "f"(v[6]), "f"(v[7]), "f"(v[8]), "f"(v[9]),
+        "f"(v[10]), "f"(v[11]), "f"(v[12]), "f"(v[13]), "f"(v[14]), "f"(v[15]), "f"(v[16]), "f"(v[17]), "f"(v[18]),
+        "f"(v[19]), "f"(v[20]), "f"(v[21]), "f"(v[22]), "f"(v[23]), "f"(v[24]), "f"(v[25]), "f"(v[26]), "f"(v[27]),
+        "f"(v[28]), "f"(v[29]), "f"(v[30]), "f"(v[31])
         : "memory");
 }
 __device__ __forceinline__ void mma_commit(uint32_t bar) {
@@ -251,12 +262,11 @@ __device__ __forceinline__ int64_t take_unit(uint32_t ufull, uint32_t uempty, co
 __global__ void __launch_bounds__(kTcThreads, 1)
     k_update32_tc(float* __restrict__ a, int64_t ld, int64_t stride, int64_t c_begin, int64_t rows, int64_t n_pad,
                   int nkc, const float* __restrict__ panel, int64_t rp, UnitSpace us,
-                  unsigned long long* __restrict__ sched, unsigned long long* err) {
+                  unsigned long long* __restrict__ sched, unsigned long long* err, int withhold_first_stage) {
     extern __shared__ __align__(1024) uint8_t tsm[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const uint32_t base = smem_u32(tsm);
-    const uint32_t abuf = (base + kHeader + 1023u) & ~1023u;  // A hi at abuf, A lo at abuf + kAHalf
-    const uint32_t ring = abuf + 2 * kAHalf;                   // B stages
+    const uint32_t ring = (base + kHeader + 1023u) & ~1023u;  // B stages, 1024-aligned
     volatile uint32_t* abort_flag = reinterpret_cast<volatile uint32_t*>(tsm + kOffAbort);
     volatile int64_t* uslot = reinterpret_cast<volatile int64_t*>(tsm + kOffUnit);
     auto full = [&](int s) { return base + kOffFull + 8 * s; };
@@ -280,7 +290,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
             mbar_init(ufull(j), 1);
             mbar_init(uempty(j), 1 + kEpiWarps);
         }
-        mbar_init(afull, 1);
+        mbar_init(afull, kEpiWarps);
         mbar_init(aempty, 1);
         mbar_init(drain, 1);
         *abort_flag = 0u;
@@ -299,14 +309,12 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     const uint32_t tmem = *reinterpret_cast<volatile uint32_t*>(tsm + kOffTmem);
 
     const size_t half_floats = (size_t)nkc * rp * 32;  // hi (or lo) of one frequency
-    const uint32_t a_bytes = 2u * nkc * kSliceA;
 
     if (warp == 0) {
-        // ---- producer: takes units from the global counter, hands them on, loads A and B ----
+        // ---- producer: takes units from the global counter, hands them on, streams B ----
         int s = 0, js = 0;
-        uint32_t ph = 0, aph = 0, jph = 0;
+        uint32_t ph = 0, jph = 0;
         uint32_t filled = 0, fill_par = 0;  // per B stage: ever filled, parity of its last fill
-        bool a_filled = false;
         for (;;) {
             int f = 0;
             int64_t i = 0, c0 = 0, c1 = 0, u = 0;
@@ -335,19 +343,6 @@ __global__ void __launch_bounds__(kTcThreads, 1)
             decode_unit(us, u, f, i, c0, c1);
             const float* hi = panel + (size_t)f * 2 * half_floats;
             const float* lo = hi + half_floats;
-            // A of the unit, once the previous unit's MMAs are done with it
-            if (lane == 0) got = mbar_wait(aempty, aph ^ 1u, abort_flag, err) ? 1u : 0u;
-            got = __shfl_sync(0xffffffffu, got, 0);
-            if (!got) break;
-            if (lane == 0) mbar_expect_tx(afull, a_bytes);
-            __syncwarp();
-            if (lane < 2 * nkc) {  // one 16 KB copy per (hi|lo, K slice)
-                const int which = lane / nkc, kb = lane - which * nkc;
-                const float* src = (which == 0 ? hi : lo) + (size_t)((int64_t)kb * rp + i * kTcM) * 32;
-                bulk_g2s(abuf + which * kAHalf + kb * kSliceA, src, kSliceA, afull);
-            }
-            a_filled = true;
-            aph ^= 1u;
             bool ok = true;
             for (int64_t c = c0; ok && c < c1; ++c) {
                 for (int kb = 0; kb < nkc; ++kb) {
@@ -357,13 +352,19 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                         ok = false;
                         break;
                     }
-                    if (lane == 0) mbar_expect_tx(full(s), kStageBytes);
-                    __syncwarp();
-                    if (lane < 2) {  // one 16 KB copy each of hi and lo
-                        const float* src = (lane == 0 ? hi : lo) + (size_t)((int64_t)kb * rp + c * kTcN) * 32;
-                        bulk_g2s(ring + s * kStageBytes + lane * kSliceB, src, kSliceB, full(s));
+                    if (withhold_first_stage && blockIdx.x == 0 && filled == 0) {
+                        // test of the bounded waits: this stage is never filled, so the MMA
+                        // thread's wait for it can only end by expiry (GWB200_DEVICE_TIMEOUT)
+                        withhold_first_stage = 0;
+                    } else {
+                        if (lane == 0) mbar_expect_tx(full(s), kStageBytes);
+                        __syncwarp();
+                        if (lane < 2) {  // one 16 KB copy each of hi and lo
+                            const float* src = (lane == 0 ? hi : lo) + (size_t)((int64_t)kb * rp + c * kTcN) * 32;
+                            bulk_g2s(ring + s * kStageBytes + lane * kSliceB, src, kSliceB, full(s));
+                        }
+                        filled |= 1u << s;
                     }
-                    filled |= 1u << s;
                     fill_par = (fill_par & ~(1u << s)) | (ph << s);
                     if (++s == kTcStages) {
                         s = 0;
@@ -377,7 +378,6 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         if (lane == 0) {
             for (int q = 0; q < kTcStages; ++q)
                 if (filled & (1u << q)) mbar_drain(full(q), (fill_par >> q) & 1u);
-            if (a_filled) mbar_drain(afull, aph ^ 1u);
         }
         __syncwarp();
     } else if (warp == 1 && lane == 0) {
@@ -395,7 +395,8 @@ __global__ void __launch_bounds__(kTcThreads, 1)
             int f;
             int64_t i, c0, c1;
             decode_unit(us, u, f, i, c0, c1);
-            if (!mbar_wait(afull, aph, abort_flag, err)) break;
+            if (!mbar_wait(afull, aph, abort_flag, err)) break;  // A of the unit is in TMEM
+            tc_fence_after();
             aph ^= 1u;
             for (int64_t c = c0; ok && c < c1; ++c) {
                 if (!mbar_wait(tempty(ab), acc_ph ^ 1u, abort_flag, err)) {
@@ -413,14 +414,12 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                     const uint32_t st = ring + s * kStageBytes;
 #pragma unroll
                     for (int kk = 0; kk < kTcKc / 8; ++kk) {
-                        const uint32_t ak = abuf + (uint32_t)kb * kSliceA + 32u * kk;
-                        const uint64_t ahi = smem_desc_sw128(ak);
-                        const uint64_t alo = smem_desc_sw128(ak + kAHalf);
+                        const uint32_t acol = (uint32_t)(kb * kTcKc + 8 * kk);
                         const uint64_t bhi = smem_desc_sw128(st + 32u * kk);
                         const uint64_t blo = smem_desc_sw128(st + kSliceB + 32u * kk);
-                        mma_tf32(d, alo, bhi, (kb > 0 || kk > 0) ? 1u : 0u);
-                        mma_tf32(d, ahi, blo, 1u);
-                        mma_tf32(d, ahi, bhi, 1u);
+                        mma_tf32_ts(d, tmem + kTmemALo + acol, bhi, (kb > 0 || kk > 0) ? 1u : 0u);
+                        mma_tf32_ts(d, tmem + kTmemAHi + acol, blo, 1u);
+                        mma_tf32_ts(d, tmem + kTmemAHi + acol, bhi, 1u);
                     }
                     mma_commit(empty(s));
                     issued = true;
@@ -448,7 +447,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         // ---- epilogue: warp -> TMEM lane quadrant (warp % 4) and 32-column quarter ----
         const int q = warp & 3, quarter = (warp - 2) >> 2;
         int ab = 0, js = 0;
-        uint32_t acc_ph = 0, jph = 0;
+        uint32_t acc_ph = 0, jph = 0, aph = 0;
         bool ok = true;
         while (ok) {
             int64_t u = 0;
@@ -462,6 +461,37 @@ __global__ void __launch_bounds__(kTcThreads, 1)
             int f;
             int64_t i, c0, c1;
             decode_unit(us, u, f, i, c0, c1);
+            // A of the unit into TMEM once the previous unit's MMAs are done with it: this warp
+            // writes lanes 32q.. of (hi | lo) x (K 0-63 | 64-127) = columns kTmemAHi + 64 quarter
+            {
+                uint32_t got = 1;
+                if (lane == 0) got = mbar_wait(aempty, aph ^ 1u, abort_flag, err) ? 1u : 0u;
+                got = __shfl_sync(0xffffffffu, got, 0);
+                if (!got) break;
+                aph ^= 1u;
+                tc_fence_after();
+                const int64_t rr = i * kTcM + q * 32 + lane;  // panel row (< rp)
+                const float* src = panel + (size_t)f * 2 * half_floats + (quarter >> 1) * half_floats;
+                for (int h = 0; h < 2; ++h) {
+                    const int kb = 2 * (quarter & 1) + h;
+                    if (kb >= nkc) break;
+                    const float4* row = reinterpret_cast<const float4*>(src + ((size_t)kb * rp + rr) * 32);
+                    float v[32];
+#pragma unroll
+                    for (int c = 0; c < 8; ++c) {
+                        const float4 x = row[c ^ (int)(rr & 7)];
+                        v[4 * c] = x.x;
+                        v[4 * c + 1] = x.y;
+                        v[4 * c + 2] = x.z;
+                        v[4 * c + 3] = x.w;
+                    }
+                    tmem_st32(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(kTmemAHi + 64 * quarter + 32 * h), v);
+                }
+                asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+                tc_fence_before();
+                __syncwarp();
+                if (lane == 0) mbar_arrive(afull);
+            }
             const int64_t r = c_begin + i * kTcM + q * 32 + lane;
             for (int64_t c = c0; c < c1; ++c) {
                 const int64_t cj = c_begin + c * kTcN + quarter * 32;  // this thread's 32 columns
@@ -547,8 +577,12 @@ int launch_update32_tc(const TallGeometry& g, int64_t nf, float* a, int64_t kb0,
     us.total = nf * us.per_f;
     GWB_CUDA(cudaMemsetAsync(sched, 0, sizeof(unsigned long long), s));
     const unsigned grid = (unsigned)std::min<int64_t>(us.total, sm_count());
+    // GWB200_TEST_EXPIRE_WAIT=1 (tests only): one CTA withholds its first operand stage, so a
+    // device wait expires and the call reports GWB200_DEVICE_TIMEOUT with the context intact.
+    const char* expire = std::getenv("GWB200_TEST_EXPIRE_WAIT");
+    const int withhold = (expire && expire[0] == '1') ? 1 : 0;
     k_update32_tc<<<grid, kTcThreads, kTcSmem, s>>>(a, g.ld, g.stride, c_begin, g.rows, g.n_pad, nkc, panel, rp, us,
-                                                     sched, err);
+                                                     sched, err, withhold);
     GWB_LAUNCH("k_update32_tc");
     return 2;
 }

@@ -352,6 +352,55 @@ def test_mixed_form_error_against_fp64(backend, nmo, nocc, states, nfreq):
     assert np.abs(s32 - s64).max() <= 2e-5 * np.abs(s64).max()
 
 
+@pytest.mark.parametrize("nmo,nocc,nst,nfreq,chunk", [
+    (40, 10, 4, 6, None),     # n = 300: two outer trailing updates
+    (80, 20, 6, 8, "3"),      # n = 1200, three frequency chunks
+    (150, 30, 4, 16, None),   # n = 3600: 64-wide last column tiles, many work units per launch
+])
+def test_tcgen05_update_bit_identical_to_mma_sync(backend, monkeypatch, nmo, nocc, nst, nfreq, chunk):
+    """The mixed form's trailing update on tcgen05 (kernels_tc.cu) performs the same 3xTF32
+    products in the same order per element as the mma.sync update (kernels_f32.cu): the screened
+    forms agree bit for bit."""
+    from minigw_b200 import generate_transformed_legendre_grid
+    from minigw_b200.synthetic import make_input
+
+    if chunk:
+        monkeypatch.setenv("GWB200_MAX_FREQ_CHUNK", chunk)
+    inp = make_input(nmo, nocc, seed=nmo)
+    om, _ = generate_transformed_legendre_grid(nfreq)
+    states = list(range(nocc - nst // 2, nocc - nst // 2 + nst))
+    backend.load_system(inp)
+    monkeypatch.setenv("GWB200_MIXED_UPDATE", "mma")
+    q_mma, st_mma = backend.screened_forms(om, states, precision="mixed")
+    monkeypatch.delenv("GWB200_MIXED_UPDATE")
+    q_tc, st_tc = backend.screened_forms(om, states, precision="mixed")
+    assert st_tc["kernel_launches"] > st_mma["kernel_launches"]  # the tcgen05 path ran (two launches per update)
+    np.testing.assert_array_equal(q_tc, q_mma)
+    q64, _ = backend.screened_forms(om, states)
+    assert np.abs(q_tc - q64).max() <= 2e-5 * np.abs(q64).max()
+
+
+def test_tcgen05_expired_wait_reports_device_timeout(backend, monkeypatch):
+    """Every mbarrier wait of the tcgen05 update is bounded.  With one operand stage withheld
+    (test hook), the wait for it expires after about two seconds: the call returns
+    GWB200_DEVICE_TIMEOUT and the next call on the same context is correct."""
+    from minigw_b200 import GwB200Error, generate_transformed_legendre_grid
+    from minigw_b200.synthetic import make_input
+
+    inp = make_input(40, 10, seed=3)
+    om, _ = generate_transformed_legendre_grid(4)
+    states = [9, 10]
+    backend.load_system(inp)
+    monkeypatch.setenv("GWB200_TEST_EXPIRE_WAIT", "1")
+    with pytest.raises(GwB200Error) as e:
+        backend.screened_forms(om, states, precision="mixed")
+    assert e.value.status == "GWB200_DEVICE_TIMEOUT"
+    monkeypatch.delenv("GWB200_TEST_EXPIRE_WAIT")
+    q32, _ = backend.screened_forms(om, states, precision="mixed")
+    q64, _ = backend.screened_forms(om, states)
+    assert np.abs(q32 - q64).max() <= 2e-5 * np.abs(q64).max()
+
+
 def test_mixed_form_h2o_qp(backend, h2o_input, oracle_lib):
     from minigw_b200 import GwB200Error
 
