@@ -147,6 +147,14 @@ def cpu_reference_sample(inp, wl, omegas, weights, pairs: int, threads: int):
             "solves_per_s": 1.0 / (wl.nfreq ** 2 * per_pair)}
 
 
+def hbm_peak_gbs() -> float:
+    """Measured HBM copy bandwidth of this pool's B200s (MEASURED_PEAKS.json), else the fallback."""
+    try:
+        return float(json.loads((ROOT / "MEASURED_PEAKS.json").read_text())["hbm_gbs"])
+    except (OSError, ValueError, KeyError):
+        return 6650.0
+
+
 def auto_pairs(wl) -> int:
     return {"cfg1": 400, "cfg2": 6, "cfg3": 2}[wl.name]
 
@@ -357,6 +365,17 @@ def run_b200(args, wl):
         "gpu_launches": int(launches),
         "clocks": clock_info,
     }
+    if args.precision == "mixed" and achieved:
+        # the tcgen05 3xTF32 trailing update (k_split_panel32 + k_update32_tc, timed together) is
+        # bound by the FP32 C read+write, 8 bytes per updated element per K = 128 pass, i.e.
+        # flops_update / 32 bytes (flops = 2 K per element)
+        gbs = upd_flops / 32.0 / (upd_ms * 1e-3) / 1e9
+        result["roofline"] = {
+            "bound": "hbm", "kernel": "k_update32_tc (tcgen05 kind::tf32 3xTF32 trailing update, with k_split_panel32)",
+            "achieved": gbs, "peak": hbm_peak_gbs(), "unit": "GB/s", "frac": gbs / hbm_peak_gbs(),
+            "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)",
+            "tflops_fp32_equivalent": achieved, "launches": upd_n, "traffic": None,
+            "traffic_source": None}
     if args.precision == "mixed":
         # error of the mixed form against the plain FP64 form on the same system (untimed)
         r32 = be.run_g0w0(wl.nfreq, wl.npade, states, precision="mixed")

@@ -300,14 +300,17 @@ int launch_factor_chunk32(const TallGeometry& g, int64_t nf, float* a, float* li
     const int64_t nsq = g.n_pad / kNb, nrt = g.rows / kNb;
     constexpr int64_t kInner = 2;
     int launches = 0;
+    // with the tcgen05 outer updates, the profiler times those alone (the look-left updates that
+    // stay on mma.sync are a few percent of the flops)
+    UpdateProfiler* lprof = panel ? nullptr : prof;
     auto update = [&](int64_t kb0, int nk, int64_t tc0, int64_t T) {
         const int64_t L = nsq - tc0;
         const int64_t tiles = T * L - T * (T - 1) / 2 + T * (nrt - nsq);
         if (tiles <= 0) return;
-        if (prof) prof->begin();
+        if (lprof) lprof->begin();
         k_update32<<<dim3((unsigned)tiles, (unsigned)nf), 256, smem_update, s>>>(a, g.ld, g.stride, kb0, nk, tc0, T, nsq);
         GWB_LAUNCH("k_update32");
-        if (prof) prof->end((double)nf * update_flops32(g, kb0, nk, tc0 * kNb, (tc0 + T) * kNb));
+        if (lprof) lprof->end((double)nf * update_flops32(g, kb0, nk, tc0 * kNb, (tc0 + T) * kNb));
         ++launches;
     };
     for (int64_t ob = 0; ob < nsq; ob += kInner) {
