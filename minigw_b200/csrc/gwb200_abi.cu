@@ -260,6 +260,7 @@ void compute_forms(gwb200_handle* h, const double* omega, int64_t nfreq, const i
     const char* prof_env = std::getenv("GWB200_PROFILE");
     UpdateProfiler prof(prof_env && prof_env[0] == '1', s);
     int64_t chunks = 0;
+    int upd_variant = -1;  // FP64 update kernel, tuned on the first chunk (full size) of this geometry
     for (int64_t f0 = 0; f0 < nfreq; f0 += fc) {
         const int64_t nf = std::min(fc, nfreq - f0);
         if (cplx) {
@@ -284,10 +285,12 @@ void compute_forms(gwb200_handle* h, const double* omega, int64_t nfreq, const i
                                               mixed_tc ? h->panel32.as<float>() : nullptr,
                                               h->tc_sched.as<unsigned long long>());
         } else {
+            if (upd_variant < 0) upd_variant = tune_update_variant(g, nf, h->a.as<double>(), s);
             launches += launch_build_tall(g, h->v.as<double>(), h->xt.as<double>(), h->dvec.as<double>(), nf,
                                           h->a.as<double>(), s);
             launches += launch_factor_chunk(g, nf, h->a.as<double>(), h->linv.as<double>(), h->qacc.as<double>(),
-                                            h->err.as<unsigned long long>(), s, prof.enabled ? &prof : nullptr);
+                                            h->err.as<unsigned long long>(), s, prof.enabled ? &prof : nullptr,
+                                            upd_variant);
         }
         launches += launch_negate_copy(h->qacc.as<double>(), nf, m, g.m_pad, h->qall.as<double>() + f0 * g.m_pad,
                                        g.m_pad, s);

@@ -118,8 +118,16 @@ int launch_build_tall(const TallGeometry& g, const double* v, const double* xt, 
                       double* a, cudaStream_t s);
 // Blocked Cholesky of the tall matrices of nf frequencies (outer blocks of two 64-wide inner
 // blocks); returns launches issued.
+// `variant`: index into the FP64 update kernel table (tune_update_variant); -1: GWB200_UPDATE_VARIANT
+// if set, else the default.
 int launch_factor_chunk(const TallGeometry& g, int64_t nf, double* a, double* linv, double* qacc,
-                        unsigned long long* err_pivot, cudaStream_t s, UpdateProfiler* prof);
+                        unsigned long long* err_pivot, cudaStream_t s, UpdateProfiler* prof, int variant);
+// Autotuner of the FP64 trailing-update kernel: GWB200_UPDATE_VARIANT if set, else the fastest
+// variant on this geometry's largest trailing update, timed once per (device, n_pad, rows, nf) per
+// process in the workspace `a` (nf tall matrices) BEFORE the matrices are built there (the timing
+// overwrites it).  The default is kept unless another variant is more than 3% faster.
+int tune_update_variant(const TallGeometry& g, int64_t nf, double* a, cudaStream_t s);
+const char* update_variant_name(int v);
 // Contraction of the screened forms of nf_int integration frequencies onto nf_out output
 // frequencies (the full grid; a shard of integration frequencies gives a partial sum).
 int launch_sigma_contract(const double* qall, int64_t nf_int, int64_t nstates, int64_t nmo, int64_t ldq,

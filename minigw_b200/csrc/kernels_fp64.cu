@@ -12,6 +12,11 @@
 // tensor cores (mma.sync m8n8k4 f64, DMMA).
 #include "internal.cuh"
 
+#include <array>
+#include <cstdio>
+#include <map>
+#include <mutex>
+
 #include <cmath>
 #include <cstdlib>
 
@@ -415,23 +420,37 @@ UpdateVariant make_variant(const char* name) {
     using Cfg = UpdateCfg<WM, WN, KC, ST>;
     return {k_update<WM, WN, KC, ST>, Cfg::kThreads, Cfg::kSmem, name};
 }
-const UpdateVariant& update_variant() {
-    static const UpdateVariant table[] = {
-        make_variant<2, 4, 32, 2>("w16x32_k32_s2"),
-        make_variant<4, 4, 32, 2>("w32x32_k32_s2"),
-        make_variant<4, 4, 16, 3>("w32x32_k16_s3"),
-        make_variant<2, 4, 32, 3>("w16x32_k32_s3"),
-        make_variant<4, 8, 32, 2>("w32x64_k32_s2"),
-        make_variant<4, 4, 32, 3>("w32x32_k32_s3"),
-    };
-    static const int nvar = (int)(sizeof(table) / sizeof(table[0]));
-    int v = kDefaultUpdateVariant;
+const UpdateVariant kVariants[] = {
+    make_variant<2, 4, 32, 2>("w16x32_k32_s2"),
+    make_variant<4, 4, 32, 2>("w32x32_k32_s2"),
+    make_variant<4, 4, 16, 3>("w32x32_k16_s3"),
+    make_variant<2, 4, 32, 3>("w16x32_k32_s3"),
+    make_variant<4, 8, 32, 2>("w32x64_k32_s2"),
+    make_variant<4, 4, 32, 3>("w32x32_k32_s3"),
+};
+constexpr int kNumVariants = (int)(sizeof(kVariants) / sizeof(kVariants[0]));
+
+int env_update_variant() {  // GWB200_UPDATE_VARIANT forces a variant; -1 if unset or out of range
     if (const char* env = std::getenv("GWB200_UPDATE_VARIANT")) {
         const int e = std::atoi(env);
-        if (e >= 0 && e < nvar) v = e;
+        if (e >= 0 && e < kNumVariants) return e;
     }
-    return table[v];
+    return -1;
 }
+
+void launch_variant(int v, const TallGeometry& g, int64_t nf, double* a, int64_t kb0, int nk, int64_t tc0, int64_t T,
+                    cudaStream_t s) {
+    const UpdateVariant& uv = kVariants[v];
+    const int64_t nsq = g.n_pad / kNb, nrt = g.rows / kNb;
+    const int64_t L = nsq - tc0;
+    const int64_t tiles = T * L - T * (T - 1) / 2 + T * (nrt - nsq);
+    if (tiles <= 0) return;
+    uv.fn<<<dim3((unsigned)tiles, (unsigned)nf), uv.threads, uv.smem, s>>>(a, g.ld, g.stride, kb0, nk, tc0, T, nsq);
+    GWB_LAUNCH("k_update");
+}
+
+std::mutex g_tune_mu;
+std::map<std::array<int64_t, 4>, int> g_tuned;  // (device, n_pad, rows, nf) -> variant
 
 // q_out[f, j] = -qacc[f, j]  (x^T W_c x = -||L^{-1} D^1/2 x||^2).
 __global__ void k_negate_copy(const double* __restrict__ qacc, int nf, int m, int64_t ldq_in, double* __restrict__ q,
@@ -500,12 +519,65 @@ static double update_flops(const TallGeometry& g, int64_t kb0, int nk, int64_t c
     return 2.0 * (double)kt * (lower + (double)g.m * cols);
 }
 
+int tune_update_variant(const TallGeometry& g, int64_t nf, double* a, cudaStream_t s) {
+    const int forced = env_update_variant();
+    if (forced >= 0) return forced;
+    const int64_t nsq = g.n_pad / kNb;
+    if (nsq <= 2) return kDefaultUpdateVariant;  // no outer trailing update to tune on
+    int dev = 0;
+    GWB_CUDA(cudaGetDevice(&dev));
+    const std::array<int64_t, 4> key = {dev, g.n_pad, g.rows, nf};
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    auto it = g_tuned.find(key);
+    if (it != g_tuned.end()) return it->second;
+    // Time every variant on the largest trailing update of this geometry (K = 128 from column 0
+    // onto columns [128, n_pad) and all RHS rows), in the workspace before the tall matrix is built
+    // there: the values are irrelevant to the timing and are overwritten afterwards.
+    cudaEvent_t e0, e1;
+    GWB_CUDA(cudaEventCreate(&e0));
+    GWB_CUDA(cudaEventCreate(&e1));
+    float best_ms = 0.f, def_ms = 0.f;
+    float times[kNumVariants] = {};
+    int best = kDefaultUpdateVariant;
+    for (int v = 0; v < kNumVariants; ++v) {
+        GWB_CUDA(cudaFuncSetAttribute(kVariants[v].fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kVariants[v].smem));
+        launch_variant(v, g, nf, a, 0, 2, 2, nsq - 2, s);  // warm-up
+        GWB_CUDA(cudaEventRecord(e0, s));
+        for (int r = 0; r < 2; ++r) launch_variant(v, g, nf, a, 0, 2, 2, nsq - 2, s);
+        GWB_CUDA(cudaEventRecord(e1, s));
+        GWB_CUDA(cudaEventSynchronize(e1));
+        float ms = 0.f;
+        GWB_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+        times[v] = ms;
+        if (v == kDefaultUpdateVariant) def_ms = ms;
+        if (v == 0 || ms < best_ms) {
+            best_ms = ms;
+            best = v;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (def_ms <= 1.03f * best_ms) best = kDefaultUpdateVariant;  // keep the default unless clearly beaten
+    g_tuned[key] = best;
+    if (const char* verbose = std::getenv("GWB200_VERBOSE"); verbose && verbose[0] == '1') {
+        std::fprintf(stderr, "gwb200: update kernel for n_pad=%lld rows=%lld nf=%lld:", (long long)g.n_pad,
+                     (long long)g.rows, (long long)nf);
+        for (int v = 0; v < kNumVariants; ++v) std::fprintf(stderr, " %s %.3f ms", kVariants[v].name, times[v] / 2);
+        std::fprintf(stderr, " -> %s\n", kVariants[best].name);
+    }
+    return best;
+}
+
+const char* update_variant_name(int v) { return (v >= 0 && v < kNumVariants) ? kVariants[v].name : "?"; }
+
 int launch_factor_chunk(const TallGeometry& g, int64_t nf, double* a, double* linv, double* qacc,
-                        unsigned long long* err_pivot, cudaStream_t s, UpdateProfiler* prof) {
+                        unsigned long long* err_pivot, cudaStream_t s, UpdateProfiler* prof, int variant) {
     const size_t smem = 2 * 64 * kLds * sizeof(double);
     const size_t smem_potrf = 2 * kNb * (kNb + 1) * sizeof(double);
     GWB_CUDA(cudaFuncSetAttribute(k_trsm_panel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    const UpdateVariant& uv = update_variant();
+    if (variant < 0 || variant >= kNumVariants)  // untuned caller: GWB200_UPDATE_VARIANT, else the default
+        variant = env_update_variant() >= 0 ? env_update_variant() : kDefaultUpdateVariant;
+    const UpdateVariant& uv = kVariants[variant];
     GWB_CUDA(cudaFuncSetAttribute(uv.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)uv.smem));
     GWB_CUDA(cudaFuncSetAttribute(k_potrf_diag, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_potrf));
     const int64_t nsq = g.n_pad / kNb;   // square tile rows/cols

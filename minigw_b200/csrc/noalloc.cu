@@ -91,7 +91,7 @@ void screened_forms_noalloc(int64_t n, int64_t m, const double* d_v, const doubl
         launch_scale_vectors(d_delta, g.n, g.n_pad, d_omega + f0, nf, dvec, s);
         launch_build_tall(g, d_v, d_xt, dvec, nf, a, s);
         GWB_CUDA(cudaMemsetAsync(qacc, 0, sizeof(double) * (size_t)nf * g.m_pad, s));
-        launch_factor_chunk(g, nf, a, linv, qacc, err, s, nullptr);
+        launch_factor_chunk(g, nf, a, linv, qacc, err, s, nullptr, -1);
         launch_negate_copy(qacc, nf, m, g.m_pad, d_q_out + (size_t)f0 * m, m, s);
     }
     unsigned long long piv = 0;

@@ -352,6 +352,23 @@ def test_mixed_form_error_against_fp64(backend, nmo, nocc, states, nfreq):
     assert np.abs(s32 - s64).max() <= 2e-5 * np.abs(s64).max()
 
 
+def test_every_update_variant_agrees(backend, monkeypatch):
+    """The autotuner picks among six FP64 trailing-update kernels (tile shape, K slice, pipeline
+    depth); each one forced in turn gives the same screened forms up to FP64 rounding."""
+    from minigw_b200 import generate_transformed_legendre_grid
+    from minigw_b200.synthetic import make_input
+
+    inp = make_input(60, 14, seed=11)   # n = 644: trailing updates of several outer blocks
+    om, _ = generate_transformed_legendre_grid(5)
+    states = [12, 13, 14]
+    backend.load_system(inp)
+    q_auto, _ = backend.screened_forms(om, states)
+    for v in range(6):
+        monkeypatch.setenv("GWB200_UPDATE_VARIANT", str(v))
+        q, _ = backend.screened_forms(om, states)
+        assert np.abs(q - q_auto).max() <= 1e-12 * np.abs(q_auto).max(), v
+
+
 @pytest.mark.parametrize("nmo,nocc,nst,nfreq,chunk", [
     (40, 10, 4, 6, None),     # n = 300: two outer trailing updates
     (80, 20, 6, 8, "3"),      # n = 1200, three frequency chunks
