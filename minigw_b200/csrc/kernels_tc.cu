@@ -13,19 +13,21 @@
 //                    rows padded with zeros to a multiple of 128), so that every operand slice of a
 //                    tile is one contiguous 16 KB block (one cp.async.bulk);
 //   k_update32_tc    a persistent, warp-specialised kernel, one CTA per SM (576 threads, 226 KB of
-//                    shared memory, 256 TMEM columns):
+//                    shared memory, all 512 TMEM columns):
 //                      warp 0     producer: takes work units from a global counter and hands them
 //                                 to the other roles through a 4-slot mbarrier ring; loads the
-//                                 unit's A (128 rows x K, hi and lo: 128 KB, resident for the whole
-//                                 unit) and streams B (128 rows x 32 of K, hi and lo) through a
-//                                 3-stage ring;
+//                                 streams B (128 rows x 32 of K, hi and lo) through a 5-stage ring;
 //                      warp 1     allocates TMEM; lane 0 issues tcgen05.mma kind::tf32 (M = 128,
-//                                 N = 128, K = 8 per instruction, K-major SW128 operands) into a
-//                                 double-buffered FP32 accumulator and commits stage releases,
-//                                 accumulator-ready and A-release to mbarriers;
+//                                 N = 128, K = 8 per instruction) with A from TMEM (the unit's 128
+//                                 rows, hi and lo, K = 128: columns 256-511, written by the epilogue
+//                                 warps at each unit start) and B from shared memory (K-major SW128)
+//                                 into a double-buffered FP32 accumulator (columns 0-255), and
+//                                 commits stage releases, accumulator-ready and A-release;
 //                      warps 2-17 epilogue: warp w reads TMEM lane quadrant w % 4, 32 columns;
-//                                 tcgen05.ld, releases the accumulator, and adds -acc to C with
-//                                 16-byte vector reductions (the read-modify-write happens in L2).
+//                                 tcgen05.ld, releases the accumulator, stages -acc as a 128B-
+//                                 swizzled 32 x 32 box in shared memory and adds it to C with one
+//                                 TMA tensor reduce (cp.reduce.async.bulk.tensor .add, whole
+//                                 128-byte lines; the read-modify-write happens in L2).
 // A work unit is (frequency, 128-row tile i, up to 16 column tiles of 128); column tile c of row
 // tile i has work iff c <= i, and units of the longest row tiles are handed out first.  Writes are
 // limited to the lower part at 64-column-block granularity (the diagonal 64 x 64 blocks in full,
@@ -36,6 +38,9 @@
 // (bounded) for its own bulk copies and MMAs, frees its TMEM and returns.
 #include "internal.cuh"
 
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
 #include <cstdlib>
 #include <mutex>
 
@@ -45,7 +50,7 @@ namespace {
 constexpr int kTcM = 128;                   // accumulator rows = TMEM lanes = A rows per unit
 constexpr int kTcN = 128;                   // accumulator columns per tile
 constexpr int kTcKc = 32;                   // floats of K per B pipeline stage
-constexpr int kTcStages = 6;                // B ring depth
+constexpr int kTcStages = 5;                // B ring depth
 constexpr int kTcSeg = 16;                  // column tiles per work unit (A is loaded once per unit)
 constexpr int kSchedSlots = 4;              // unit-index ring from the producer to the other roles
 constexpr int kRowBytes = kTcKc * 4;        // one row of a K slice: 128 bytes = one swizzle atom row
@@ -58,7 +63,8 @@ constexpr int kTmemAHi = 2 * kTcN, kTmemALo = kTmemAHi + 128;
 constexpr int kHeader = 1024;        // mbarriers, unit ring, TMEM address, abort flag
 // + 1024: the operand region starts at the first 1024-byte boundary after the header (the
 // 128-byte swizzle is applied to shared-memory address bits, so every slice is 1024-aligned)
-constexpr int kTcSmem = kHeader + 1024 + kTcStages * kStageBytes;
+constexpr int kStgBytes = 32 * 32 * 4;       // per epilogue warp: 32 rows x 32 floats, 128B-swizzled
+constexpr int kTcSmem = kHeader + 1024 + kTcStages * kStageBytes + kEpiWarps * kStgBytes;
 constexpr unsigned long long kWaitNs = 2000000000ull;
 
 // header layout (byte offsets)
@@ -172,6 +178,15 @@ __device__ __forceinline__ void tmem_st32(uint32_t taddr, const float (&v)[32]) 
         "f"(v[28]), "f"(v[29]), "f"(v[30]), "f"(v[31])
         : "memory");
 }
+// C[f][y .. y+32)[x .. x+32) += staging tile (FP32 add performed by the TMA unit / L2, whole
+// 128-byte lines), tracked in this thread's bulk async-group.
+__device__ __forceinline__ void tma_reduce_add_3d(const CUtensorMap* map, uint32_t src, int x, int y, int z) {
+    asm volatile("cp.reduce.async.bulk.tensor.3d.global.shared::cta.add.bulk_group [%0, {%2, %3, %4}], [%1];" ::"l"(
+                     reinterpret_cast<uint64_t>(map)),
+                 "r"(src), "r"(x), "r"(y), "r"(z)
+                 : "memory");
+    asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+}
 __device__ __forceinline__ void mma_commit(uint32_t bar) {
     asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar) : "memory");
 }
@@ -262,11 +277,13 @@ __device__ __forceinline__ int64_t take_unit(uint32_t ufull, uint32_t uempty, co
 __global__ void __launch_bounds__(kTcThreads, 1)
     k_update32_tc(float* __restrict__ a, int64_t ld, int64_t stride, int64_t c_begin, int64_t rows, int64_t n_pad,
                   int nkc, const float* __restrict__ panel, int64_t rp, UnitSpace us,
-                  unsigned long long* __restrict__ sched, unsigned long long* err, int withhold_first_stage) {
+                  unsigned long long* __restrict__ sched, unsigned long long* err, int withhold_first_stage,
+                  const __grid_constant__ CUtensorMap cmap) {
     extern __shared__ __align__(1024) uint8_t tsm[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const uint32_t base = smem_u32(tsm);
     const uint32_t ring = (base + kHeader + 1023u) & ~1023u;  // B stages, 1024-aligned
+    const uint32_t stg0 = ring + kTcStages * kStageBytes;     // epilogue staging tiles, 1024-aligned
     volatile uint32_t* abort_flag = reinterpret_cast<volatile uint32_t*>(tsm + kOffAbort);
     volatile int64_t* uslot = reinterpret_cast<volatile int64_t*>(tsm + kOffUnit);
     auto full = [&](int s) { return base + kOffFull + 8 * s; };
@@ -446,6 +463,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     } else if (warp >= 2) {
         // ---- epilogue: warp -> TMEM lane quadrant (warp % 4) and 32-column quarter ----
         const int q = warp & 3, quarter = (warp - 2) >> 2;
+        const uint32_t stg = stg0 + (uint32_t)(warp - 2) * kStgBytes;
         int ab = 0, js = 0;
         uint32_t acc_ph = 0, jph = 0, aph = 0;
         bool ok = true;
@@ -492,13 +510,13 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                 __syncwarp();
                 if (lane == 0) mbar_arrive(afull);
             }
-            const int64_t r = c_begin + i * kTcM + q * 32 + lane;
+            const int64_t rs = c_begin + i * kTcM + q * 32;  // first row of this warp's 32-row box
             for (int64_t c = c0; c < c1; ++c) {
-                const int64_t cj = c_begin + c * kTcN + quarter * 32;  // this thread's 32 columns
-                // lower part at 64-column-block granularity (the diagonal 64x64 blocks in full)
-                const bool valid = r < rows && cj < n_pad && r >= (cj & ~(int64_t)63);
-                float4* crow = reinterpret_cast<float4*>(a + (size_t)f * stride + (size_t)(valid ? r : 0) * ld +
-                                                         (valid ? cj : 0));
+                const int64_t cj = c_begin + c * kTcN + quarter * 32;  // first column of the box
+                // lower part at 64-column-block granularity (the diagonal 64x64 blocks in full): a
+                // 32-row box starting at a multiple of 32 is wholly in or wholly out; rows past
+                // `rows` are clipped by the tensor map
+                const bool box = cj < n_pad && rs < rows && rs >= (cj & ~(int64_t)63);
                 uint32_t got = 1;
                 if (lane == 0) got = mbar_wait(tfull(ab), acc_ph, abort_flag, err) ? 1u : 0u;
                 got = __shfl_sync(0xffffffffu, got, 0);
@@ -512,12 +530,21 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                 tc_fence_before();
                 __syncwarp();
                 if (lane == 0) mbar_arrive(tempty(ab));
-                // C += (-acc) as vector reductions performed in L2: no load on this SM, and every
-                // element receives exactly one addition per launch (same rounding as C - acc)
-                if (valid) {
+                if (box) {
+                    // C += (-acc): the warp's 32 x 32 box staged 128B-swizzled (row `lane`, 16-byte
+                    // chunk j at chunk j ^ (lane % 8): conflict-free), then one TMA reduce-add
+                    if (lane == 0) asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
+                    __syncwarp();
 #pragma unroll
-                    for (int j = 0; j < 8; ++j)
-                        atomicAdd(crow + j, make_float4(-acc[4 * j], -acc[4 * j + 1], -acc[4 * j + 2], -acc[4 * j + 3]));
+                    for (int j = 0; j < 8; ++j) {
+                        const uint32_t dst = stg + (uint32_t)lane * 128u + (uint32_t)((j ^ (lane & 7)) * 16);
+                        asm volatile("st.shared.v4.f32 [%0], {%1, %2, %3, %4};" ::"r"(dst), "f"(-acc[4 * j]),
+                                     "f"(-acc[4 * j + 1]), "f"(-acc[4 * j + 2]), "f"(-acc[4 * j + 3])
+                                     : "memory");
+                    }
+                    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                    __syncwarp();
+                    if (lane == 0) tma_reduce_add_3d(&cmap, stg, (int)cj, (int)rs, f);
                 }
                 if (++ab == 2) {
                     ab = 0;
@@ -526,6 +553,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
             }
         }
     }
+    if (warp >= 2 && lane == 0) asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");  // reduces done
     tc_fence_before();
     __syncthreads();
     if (warp == 1) {
@@ -569,6 +597,27 @@ int launch_update32_tc(const TallGeometry& g, int64_t nf, float* a, int64_t kb0,
         GWB_LAUNCH("k_split_panel32");
     }
     GWB_CUDA(cudaFuncSetAttribute(k_update32_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmem));
+    // C of the chunk as a 3-D FP32 tensor (columns, rows, frequencies), 32 x 32 boxes, 128B swizzle
+    CUtensorMap cmap;
+    {
+        static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
+        static std::once_flag once;
+        std::call_once(once, [] {
+            void* fn = nullptr;
+            cudaDriverEntryPointQueryResult q{};
+            if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) == cudaSuccess &&
+                q == cudaDriverEntryPointSuccess)
+                encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+        });
+        if (!encode) fail(GWB200_CUDA_ERROR, "cuTensorMapEncodeTiled is not available from the driver");
+        const cuuint64_t dims[3] = {(cuuint64_t)g.n_pad, (cuuint64_t)g.rows, (cuuint64_t)nf};
+        const cuuint64_t strides[2] = {(cuuint64_t)g.ld * 4, (cuuint64_t)g.stride * 4};
+        const cuuint32_t box[3] = {32, 32, 1}, estr[3] = {1, 1, 1};
+        const CUresult r = encode(&cmap, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, a, dims, strides, box, estr,
+                                  CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                                  CU_TENSOR_MAP_L2_PROMOTION_NONE, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+        if (r != CUDA_SUCCESS) fail(GWB200_CUDA_ERROR, "cuTensorMapEncodeTiled failed for the tall matrices");
+    }
     UnitSpace us;
     us.T = T;
     us.NI = NI;
@@ -582,7 +631,7 @@ int launch_update32_tc(const TallGeometry& g, int64_t nf, float* a, int64_t kb0,
     const char* expire = std::getenv("GWB200_TEST_EXPIRE_WAIT");
     const int withhold = (expire && expire[0] == '1') ? 1 : 0;
     k_update32_tc<<<grid, kTcThreads, kTcSmem, s>>>(a, g.ld, g.stride, c_begin, g.rows, g.n_pad, nkc, panel, rp, us,
-                                                     sched, err, withhold);
+                                                     sched, err, withhold, cmap);
     GWB_LAUNCH("k_update32_tc");
     return 2;
 }
