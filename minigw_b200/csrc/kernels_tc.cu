@@ -12,22 +12,25 @@
 //                    K-major layout the tensor core reads ([K slice of 32 floats][row][128 bytes],
 //                    rows padded with zeros to a multiple of 128), so that every operand slice of a
 //                    tile is one contiguous 16 KB block (one cp.async.bulk);
-//   k_update32_tc    a persistent, warp-specialised kernel, one CTA per SM (576 threads, 226 KB of
+//   k_update32_tc    a persistent, warp-specialised kernel, one CTA per SM (18 warps, 226 KB of
 //                    shared memory, all 512 TMEM columns):
 //                      warp 0     producer: takes work units from a global counter and hands them
 //                                 to the other roles through a 4-slot mbarrier ring; loads the
-//                                 streams B (128 rows x 32 of K, hi and lo) through a 5-stage ring;
+//                                 streams B (128 rows x 32 of K, hi and lo) through a 6-stage ring,
+//                                 and prefetches the unit's A rows into L2;
 //                      warp 1     allocates TMEM; lane 0 issues tcgen05.mma kind::tf32 (M = 128,
 //                                 N = 128, K = 8 per instruction) with A from TMEM (the unit's 128
-//                                 rows, hi and lo, K = 128: columns 256-511, written by the epilogue
-//                                 warps at each unit start) and B from shared memory (K-major SW128)
+//                                 rows, hi and lo, K = 128: columns 256-511) and B from shared
+//                                 memory (K-major SW128)
 //                                 into a double-buffered FP32 accumulator (columns 0-255), and
 //                                 commits stage releases, accumulator-ready and A-release;
-//                      warps 2-17 epilogue: warp w reads TMEM lane quadrant w % 4, 32 columns;
-//                                 tcgen05.ld, releases the accumulator, stages -acc as a 128B-
-//                                 swizzled 32 x 32 box in shared memory and adds it to C with one
-//                                 TMA tensor reduce (cp.reduce.async.bulk.tensor .add, whole
-//                                 128-byte lines; the read-modify-write happens in L2).
+//                      warps 2-9  epilogue: warp w reads TMEM lane quadrant w % 4, 64 columns
+//                                 as two 32 x 32 boxes; tcgen05.ld, releases the accumulator,
+//                                 stages -acc 128B-swizzled in shared memory and adds it to C with
+//                                 a TMA tensor reduce (cp.reduce.async.bulk.tensor .add, whole
+//                                 128-byte lines; the read-modify-write happens in L2);
+//                      warps 10-17 A loaders: fill the unit's A into TMEM (tcgen05.st) as soon as
+//                                 the previous unit's MMAs release it.
 // A work unit is (frequency, 128-row tile i, up to 16 column tiles of 128); column tile c of row
 // tile i has work iff c <= i, and units of the longest row tiles are handed out first.  Writes are
 // limited to the lower part at 64-column-block granularity (the diagonal 64 x 64 blocks in full,
@@ -50,14 +53,15 @@ namespace {
 constexpr int kTcM = 128;                   // accumulator rows = TMEM lanes = A rows per unit
 constexpr int kTcN = 128;                   // accumulator columns per tile
 constexpr int kTcKc = 32;                   // floats of K per B pipeline stage
-constexpr int kTcStages = 5;                // B ring depth
+constexpr int kTcStages = 6;                // B ring depth
 constexpr int kTcSeg = 16;                  // column tiles per work unit (A is loaded once per unit)
 constexpr int kSchedSlots = 4;              // unit-index ring from the producer to the other roles
 constexpr int kRowBytes = kTcKc * 4;        // one row of a K slice: 128 bytes = one swizzle atom row
 constexpr int kSliceB = kTcN * kRowBytes;   // 16384 bytes
 constexpr int kStageBytes = 2 * kSliceB;    // B stage: hi + lo slice, two copies
-constexpr int kEpiWarps = 16;               // 4 lane quadrants x 4 column quarters of 32
-constexpr int kTcThreads = 32 * (2 + kEpiWarps);
+constexpr int kEpiWarps = 8;                // epilogue: 4 lane quadrants x 2 column halves of 64
+constexpr int kLoadWarps = 8;               // A into TMEM: 4 lane quadrants x (hi | lo)
+constexpr int kTcThreads = 32 * (2 + kEpiWarps + kLoadWarps);
 constexpr int kTmemCols = 512;       // accumulators [0, 256), A hi [256, 384), A lo [384, 512)
 constexpr int kTmemAHi = 2 * kTcN, kTmemALo = kTmemAHi + 128;
 constexpr int kHeader = 1024;        // mbarriers, unit ring, TMEM address, abort flag
@@ -72,7 +76,7 @@ constexpr int kOffFull = 0;                              // kTcStages: B stage f
 constexpr int kOffEmpty = kOffFull + 8 * kTcStages;      // kTcStages: B stage consumed (tcgen05.commit)
 constexpr int kOffTFull = kOffEmpty + 8 * kTcStages;     // 2: accumulator ready (tcgen05.commit)
 constexpr int kOffTEmpty = kOffTFull + 16;               // 2: accumulator drained (kEpiWarps arrivals)
-constexpr int kOffAFull = kOffTEmpty + 16;               // 1: A of the unit in TMEM (kEpiWarps arrivals)
+constexpr int kOffAFull = kOffTEmpty + 16;               // 1: A of the unit in TMEM (kLoadWarps arrivals)
 constexpr int kOffAEmpty = kOffAFull + 8;                // 1: all MMAs reading A of the unit complete
 constexpr int kOffDrain = kOffAEmpty + 8;                // 1: all MMAs of this CTA complete
 constexpr int kOffUFull = kOffDrain + 8;                 // kSchedSlots: unit index written
@@ -305,9 +309,9 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         }
         for (int j = 0; j < kSchedSlots; ++j) {
             mbar_init(ufull(j), 1);
-            mbar_init(uempty(j), 1 + kEpiWarps);
+            mbar_init(uempty(j), 1 + kEpiWarps + kLoadWarps);
         }
-        mbar_init(afull, kEpiWarps);
+        mbar_init(afull, kLoadWarps);
         mbar_init(aempty, 1);
         mbar_init(drain, 1);
         *abort_flag = 0u;
@@ -360,6 +364,13 @@ __global__ void __launch_bounds__(kTcThreads, 1)
             decode_unit(us, u, f, i, c0, c1);
             const float* hi = panel + (size_t)f * 2 * half_floats;
             const float* lo = hi + half_floats;
+            // the unit's A rows (read once, by the epilogue warps into TMEM when the unit starts):
+            // bring them into L2 now, about a tile ahead of their use
+            if (lane < 2 * nkc) {
+                const int which = lane / nkc, kb = lane - which * nkc;
+                const float* src = (which == 0 ? hi : lo) + (size_t)((int64_t)kb * rp + i * kTcM) * 32;
+                asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(src), "r"(kTcM * kRowBytes) : "memory");
+            }
             bool ok = true;
             for (int64_t c = c0; ok && c < c1; ++c) {
                 for (int kb = 0; kb < nkc; ++kb) {
@@ -460,12 +471,12 @@ __global__ void __launch_bounds__(kTcThreads, 1)
             mma_commit(drain);
             mbar_drain(drain, 0);
         }
-    } else if (warp >= 2) {
-        // ---- epilogue: warp -> TMEM lane quadrant (warp % 4) and 32-column quarter ----
-        const int q = warp & 3, quarter = (warp - 2) >> 2;
+    } else if (warp >= 2 && warp < 2 + kEpiWarps) {
+        // ---- epilogue: warp -> TMEM lane quadrant (warp % 4) and 64-column half, two 32x32 boxes ----
+        const int q = warp & 3, half = (warp - 2) >> 2;
         const uint32_t stg = stg0 + (uint32_t)(warp - 2) * kStgBytes;
         int ab = 0, js = 0;
-        uint32_t acc_ph = 0, jph = 0, aph = 0;
+        uint32_t acc_ph = 0, jph = 0;
         bool ok = true;
         while (ok) {
             int64_t u = 0;
@@ -479,44 +490,8 @@ __global__ void __launch_bounds__(kTcThreads, 1)
             int f;
             int64_t i, c0, c1;
             decode_unit(us, u, f, i, c0, c1);
-            // A of the unit into TMEM once the previous unit's MMAs are done with it: this warp
-            // writes lanes 32q.. of (hi | lo) x (K 0-63 | 64-127) = columns kTmemAHi + 64 quarter
-            {
-                uint32_t got = 1;
-                if (lane == 0) got = mbar_wait(aempty, aph ^ 1u, abort_flag, err) ? 1u : 0u;
-                got = __shfl_sync(0xffffffffu, got, 0);
-                if (!got) break;
-                aph ^= 1u;
-                tc_fence_after();
-                const int64_t rr = i * kTcM + q * 32 + lane;  // panel row (< rp)
-                const float* src = panel + (size_t)f * 2 * half_floats + (quarter >> 1) * half_floats;
-                for (int h = 0; h < 2; ++h) {
-                    const int kb = 2 * (quarter & 1) + h;
-                    if (kb >= nkc) break;
-                    const float4* row = reinterpret_cast<const float4*>(src + ((size_t)kb * rp + rr) * 32);
-                    float v[32];
-#pragma unroll
-                    for (int c = 0; c < 8; ++c) {
-                        const float4 x = row[c ^ (int)(rr & 7)];
-                        v[4 * c] = x.x;
-                        v[4 * c + 1] = x.y;
-                        v[4 * c + 2] = x.z;
-                        v[4 * c + 3] = x.w;
-                    }
-                    tmem_st32(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(kTmemAHi + 64 * quarter + 32 * h), v);
-                }
-                asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
-                tc_fence_before();
-                __syncwarp();
-                if (lane == 0) mbar_arrive(afull);
-            }
-            const int64_t rs = c_begin + i * kTcM + q * 32;  // first row of this warp's 32-row box
+            const int64_t rs = c_begin + i * kTcM + q * 32;  // first row of this warp's 32-row boxes
             for (int64_t c = c0; c < c1; ++c) {
-                const int64_t cj = c_begin + c * kTcN + quarter * 32;  // first column of the box
-                // lower part at 64-column-block granularity (the diagonal 64x64 blocks in full): a
-                // 32-row box starting at a multiple of 32 is wholly in or wholly out; rows past
-                // `rows` are clipped by the tensor map
-                const bool box = cj < n_pad && rs < rows && rs >= (cj & ~(int64_t)63);
                 uint32_t got = 1;
                 if (lane == 0) got = mbar_wait(tfull(ab), acc_ph, abort_flag, err) ? 1u : 0u;
                 got = __shfl_sync(0xffffffffu, got, 0);
@@ -525,26 +500,36 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                     break;
                 }
                 tc_fence_after();
-                float acc[32];
-                tmem_ld32(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(ab * kTcN + quarter * 32), acc);
-                tc_fence_before();
-                __syncwarp();
-                if (lane == 0) mbar_arrive(tempty(ab));
-                if (box) {
-                    // C += (-acc): the warp's 32 x 32 box staged 128B-swizzled (row `lane`, 16-byte
-                    // chunk j at chunk j ^ (lane % 8): conflict-free), then one TMA reduce-add
-                    if (lane == 0) asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
-                    __syncwarp();
-#pragma unroll
-                    for (int j = 0; j < 8; ++j) {
-                        const uint32_t dst = stg + (uint32_t)lane * 128u + (uint32_t)((j ^ (lane & 7)) * 16);
-                        asm volatile("st.shared.v4.f32 [%0], {%1, %2, %3, %4};" ::"r"(dst), "f"(-acc[4 * j]),
-                                     "f"(-acc[4 * j + 1]), "f"(-acc[4 * j + 2]), "f"(-acc[4 * j + 3])
-                                     : "memory");
+                for (int b = 0; b < 2; ++b) {
+                    const int64_t cj = c_begin + c * kTcN + half * 64 + b * 32;  // first column of the box
+                    // lower part at 64-column-block granularity (the diagonal 64x64 blocks in full): a
+                    // 32-row box starting at a multiple of 32 is wholly in or wholly out; rows past
+                    // `rows` are clipped by the tensor map
+                    const bool box = cj < n_pad && rs < rows && rs >= (cj & ~(int64_t)63);
+                    float acc[32];
+                    tmem_ld32(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(ab * kTcN + half * 64 + b * 32), acc);
+                    if (b == 1) {  // both halves read: the accumulator is free
+                        tc_fence_before();
+                        __syncwarp();
+                        if (lane == 0) mbar_arrive(tempty(ab));
                     }
-                    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-                    __syncwarp();
-                    if (lane == 0) tma_reduce_add_3d(&cmap, stg, (int)cj, (int)rs, f);
+                    if (box) {
+                        // C += (-acc): the box staged 128B-swizzled (row `lane`, 16-byte chunk j at
+                        // chunk j ^ (lane % 8): conflict-free), then one TMA reduce-add; the staging
+                        // buffer is rewritten only after the previous reduce has read it
+                        if (lane == 0) asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
+                        __syncwarp();
+#pragma unroll
+                        for (int j = 0; j < 8; ++j) {
+                            const uint32_t dst = stg + (uint32_t)lane * 128u + (uint32_t)((j ^ (lane & 7)) * 16);
+                            asm volatile("st.shared.v4.f32 [%0], {%1, %2, %3, %4};" ::"r"(dst), "f"(-acc[4 * j]),
+                                         "f"(-acc[4 * j + 1]), "f"(-acc[4 * j + 2]), "f"(-acc[4 * j + 3])
+                                         : "memory");
+                        }
+                        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                        __syncwarp();
+                        if (lane == 0) tma_reduce_add_3d(&cmap, stg, (int)cj, (int)rs, f);
+                    }
                 }
                 if (++ab == 2) {
                     ab = 0;
@@ -552,8 +537,61 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                 }
             }
         }
+    } else if (warp >= 2 + kEpiWarps) {
+        // ---- A loaders: warp -> TMEM lane quadrant (warp % 4), hi (first four warps) or lo; each
+        // fills the unit's A as soon as the previous unit's MMAs release it, the first K slice
+        // loaded before that and the next one in flight while the current one is stored ----
+        const int q = warp & 3, which = (warp - 2 - kEpiWarps) >> 2;
+        int js = 0;
+        uint32_t jph = 0, aph = 0;
+        for (;;) {
+            int64_t u = 0;
+            if (lane == 0) u = take_unit(ufull(js), uempty(js), uslot + js, jph, abort_flag, err);
+            u = __shfl_sync(0xffffffffu, u, 0);
+            if (++js == kSchedSlots) {
+                js = 0;
+                jph ^= 1u;
+            }
+            if (u < 0 || u >= us.total) break;
+            int f;
+            int64_t i, c0, c1;
+            decode_unit(us, u, f, i, c0, c1);
+            const int64_t rr = i * kTcM + q * 32 + lane;  // panel row (< rp)
+            const float* src = panel + (size_t)f * 2 * half_floats + (size_t)which * half_floats;
+            auto load_slice = [&](int kb, float (&v)[32]) {
+                const float4* row = reinterpret_cast<const float4*>(src + ((size_t)kb * rp + rr) * 32);
+#pragma unroll
+                for (int c = 0; c < 8; ++c) {
+                    const float4 x = row[c ^ (int)(rr & 7)];
+                    v[4 * c] = x.x;
+                    v[4 * c + 1] = x.y;
+                    v[4 * c + 2] = x.z;
+                    v[4 * c + 3] = x.w;
+                }
+            };
+            float v[32];
+            load_slice(0, v);
+            uint32_t got = 1;
+            if (lane == 0) got = mbar_wait(aempty, aph ^ 1u, abort_flag, err) ? 1u : 0u;
+            got = __shfl_sync(0xffffffffu, got, 0);
+            if (!got) break;
+            aph ^= 1u;
+            tc_fence_after();
+            for (int kb = 0; kb < nkc; ++kb) {
+                float nv[32];
+                if (kb + 1 < nkc) load_slice(kb + 1, nv);
+                tmem_st32(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(kTmemAHi + 128 * which + 32 * kb), v);
+#pragma unroll
+                for (int j = 0; j < 32; ++j) v[j] = nv[j];
+            }
+            asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(afull);
+        }
     }
-    if (warp >= 2 && lane == 0) asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");  // reduces done
+    if (warp >= 2 && warp < 2 + kEpiWarps && lane == 0)
+        asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");  // this warp's reduces are complete
     tc_fence_before();
     __syncthreads();
     if (warp == 1) {
