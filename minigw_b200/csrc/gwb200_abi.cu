@@ -115,7 +115,8 @@ struct gwb200_handle {
     DevBuf pqo, xdiag, mo, vxc_diag, delta, v, sigx, flag;  // pqo: the (pq|o.) block of the ERI
     // per-call workspaces (grow-only, reused across calls)
     DevBuf xt, dvec, a, linv, qacc, qall, sigma, omega, weight, states, err, qp, qp_scratch, omega_out;
-    DevBuf panel32;   // split FP32 panel of the mixed form's tcgen05 trailing updates
+    DevBuf panel32;   // operand workspace of the tcgen05 trailing updates (mixed: FP32 hi/lo split;
+                      // plain with GWB200_FP64_UPDATE=ozaki: int8 digit slices + exponents)
     DevBuf tc_sched;  // work counter of the tcgen05 update kernel
     PinnedBuf stage_in, stage_out;
     // cached frequency-chunk size for a repeated geometry (avoids cudaMemGetInfo per call)
@@ -134,6 +135,13 @@ namespace {
 bool mixed_update_on_tcgen05() {
     const char* env = std::getenv("GWB200_MIXED_UPDATE");
     return !(env && std::strcmp(env, "mma") == 0);
+}
+
+// The plain form's outer trailing updates run as the int8 tensor-core emulation (kernels_oz.cu)
+// when GWB200_FP64_UPDATE=ozaki, else on the FP64 DMMA pipe.
+bool fp64_update_ozaki() {
+    const char* env = std::getenv("GWB200_FP64_UPDATE");
+    return env && std::strcmp(env, "ozaki") == 0;
 }
 
 // Allocate `b` for `want` bytes: grow-only, or exact and stream-ordered when the handle is limited.
@@ -214,9 +222,11 @@ void compute_forms(gwb200_handle* h, const double* omega, int64_t nfreq, const i
 
     // Frequency chunk size from the HBM budget: tall matrices + scale vectors + 64x64 inverses.
     const bool mixed_tc = mixed && mixed_update_on_tcgen05();
+    const bool fp64_oz = !mixed && !cplx && fp64_update_ozaki();
     const size_t per_freq = mixed ? sizeof(float) * ((size_t)g.stride + kNb * kNb) + sizeof(double) * (g.n_pad + g.m_pad) +
                                         (mixed_tc ? tc_panel_bytes_per_freq(g) : 0)
-                                  : sizeof(double) * planes * ((size_t)g.stride + g.n_pad + kNb * kNb + g.m_pad);
+                                  : sizeof(double) * planes * ((size_t)g.stride + g.n_pad + kNb * kNb + g.m_pad) +
+                                        (fp64_oz ? oz_slice_bytes_per_freq(g) : 0);
     // GWB200_MAX_FREQ_CHUNK caps the chunk (tests use it to exercise the multi-chunk path).
     int64_t cap = 0;
     if (const char* env = std::getenv("GWB200_MAX_FREQ_CHUNK")) cap = std::max<long long>(0, std::atoll(env));
@@ -250,6 +260,10 @@ void compute_forms(gwb200_handle* h, const double* omega, int64_t nfreq, const i
     size_buffer(h, h->qacc, sizeof(double) * planes * (size_t)fc * g.m_pad);
     if (mixed_tc) {
         size_buffer(h, h->panel32, tc_panel_bytes_per_freq(g) * (size_t)fc);
+        h->tc_sched.ensure(sizeof(unsigned long long));
+    }
+    if (fp64_oz) {
+        size_buffer(h, h->panel32, oz_slice_bytes_per_freq(g) * (size_t)fc);
         h->tc_sched.ensure(sizeof(unsigned long long));
     }
 
@@ -290,7 +304,8 @@ void compute_forms(gwb200_handle* h, const double* omega, int64_t nfreq, const i
                                           h->a.as<double>(), s);
             launches += launch_factor_chunk(g, nf, h->a.as<double>(), h->linv.as<double>(), h->qacc.as<double>(),
                                             h->err.as<unsigned long long>(), s, prof.enabled ? &prof : nullptr,
-                                            upd_variant);
+                                            upd_variant, fp64_oz ? h->panel32.p : nullptr,
+                                            h->tc_sched.as<unsigned long long>());
         }
         launches += launch_negate_copy(h->qacc.as<double>(), nf, m, g.m_pad, h->qall.as<double>() + f0 * g.m_pad,
                                        g.m_pad, s);

@@ -119,9 +119,17 @@ int launch_build_tall(const TallGeometry& g, const double* v, const double* xt, 
 // Blocked Cholesky of the tall matrices of nf frequencies (outer blocks of two 64-wide inner
 // blocks); returns launches issued.
 // `variant`: index into the FP64 update kernel table (tune_update_variant); -1: GWB200_UPDATE_VARIANT
-// if set, else the default.
+// if set, else the default.  oz != NULL: the outer trailing updates run as the int8 emulation of
+// kernels_oz.cu with `oz` as its slice workspace (oz_slice_bytes_per_freq(g) per frequency) and
+// `sched` as its work counter.
 int launch_factor_chunk(const TallGeometry& g, int64_t nf, double* a, double* linv, double* qacc,
-                        unsigned long long* err_pivot, cudaStream_t s, UpdateProfiler* prof, int variant);
+                        unsigned long long* err_pivot, cudaStream_t s, UpdateProfiler* prof, int variant,
+                        void* oz = nullptr, unsigned long long* sched = nullptr);
+// kernels_oz.cu: FP64 trailing update C -= P P^T (K = 128 from kb0, columns [c_begin, n_pad), rows
+// [c_begin, rows)) from exact int8 products of 7-digit row slices (tcgen05 kind::i8).  Two launches.
+size_t oz_slice_bytes_per_freq(const TallGeometry& g);
+int launch_update64_oz(const TallGeometry& g, int64_t nf, double* a, int64_t kb0, int64_t c_begin, void* slices,
+                       unsigned long long* sched, unsigned long long* err_pivot, cudaStream_t s);
 // Autotuner of the FP64 trailing-update kernel: GWB200_UPDATE_VARIANT if set, else the fastest
 // variant on this geometry's largest trailing update, timed once per (device, n_pad, rows, nf) per
 // process in the workspace `a` (nf tall matrices) BEFORE the matrices are built there (the timing

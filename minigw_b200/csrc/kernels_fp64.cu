@@ -571,7 +571,8 @@ int tune_update_variant(const TallGeometry& g, int64_t nf, double* a, cudaStream
 const char* update_variant_name(int v) { return (v >= 0 && v < kNumVariants) ? kVariants[v].name : "?"; }
 
 int launch_factor_chunk(const TallGeometry& g, int64_t nf, double* a, double* linv, double* qacc,
-                        unsigned long long* err_pivot, cudaStream_t s, UpdateProfiler* prof, int variant) {
+                        unsigned long long* err_pivot, cudaStream_t s, UpdateProfiler* prof, int variant, void* oz,
+                        unsigned long long* sched) {
     const size_t smem = 2 * 64 * kLds * sizeof(double);
     const size_t smem_potrf = 2 * kNb * (kNb + 1) * sizeof(double);
     GWB_CUDA(cudaFuncSetAttribute(k_trsm_panel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -613,7 +614,15 @@ int launch_factor_chunk(const TallGeometry& g, int64_t nf, double* a, double* li
             }
         }
         const int64_t tc0 = ob + q;
-        if (tc0 < nsq) update(ob * kNb, (int)q, tc0, nsq - tc0);  // outer-block trailing update, K = 64*q
+        if (tc0 < nsq) {  // outer-block trailing update, K = 64*q (= 128 whenever columns remain)
+            if (oz && q == kInner) {
+                if (prof) prof->begin();
+                launches += launch_update64_oz(g, nf, a, ob * kNb, tc0 * kNb, oz, sched, err_pivot, s);
+                if (prof) prof->end((double)nf * update_flops(g, ob * kNb, (int)q, tc0 * kNb, nsq * kNb));
+            } else {
+                update(ob * kNb, (int)q, tc0, nsq - tc0);
+            }
+        }
     }
     return launches;
 }

@@ -1,0 +1,473 @@
+// kernels_oz.cu -- FP64 trailing update emulated on the int8 tensor cores (tcgen05 kind::i8).
+//
+// The plain form's dominant work is C -= P_r . P_c over the trailing lower part after each outer
+// block of K = 128 columns (FP64; kernels_fp64.cu runs it on the FP64 DMMA pipe, 37 TFLOP/s
+// peak).  Here each panel row P_r (128 values) is written as
+//     P_r[k] = 2^e_r * sum_{s=1..7} D_s[r][k] 2^{-7 s} + (remainder below 2^{e_r - 49}),
+// with e_r the smallest power of two above max_k |P_r[k]| and D_s signed 7-bit digits (|D_s| <=
+// 127, truncation of the scaled value, so every digit carries the sign of the value).  The
+// product of two rows is then
+//     P_r . P_c ~= 2^{e_r + e_c} sum_{l=2..8} 2^{-7 l} S_l,   S_l = sum_{s+t=l} D_s[r] . D_t[c],
+// dropping only the terms with s + t > 8 (below 2^{-56} relative to the row maxima).  Each S_l is
+// an exact int32 sum of int8 products (|S_l| <= 7 * 127^2 * 128 < 2^24), accumulated by 28
+// int8 tensor-core products per 32-deep K step; the levels are combined exactly in 64-bit
+// integers into two parts, converted, joined with one FP64 rounding and scaled by exact powers
+// of two.  The error per element is at the level of an FP64
+// dot product of the same rows (measured: screened forms within ~1e-14 relative of the FP64 DMMA
+// path); this is the Ozaki splitting scheme restated for power-of-two row scaling.
+//
+// Two launches per update:
+//   k_slice_panel64  one warp per panel row: e_r, and the 7 digit slices of the row's 128 values,
+//                    each slice a 128-byte row in the 128-byte-swizzled K-major layout
+//                    ([slice][row][128 bytes]) the tensor core reads;
+//   k_update64_oz    persistent, warp-specialised, one CTA per SM (10 warps, 222 KB of shared
+//                    memory, 448 TMEM columns):
+//                      warp 0     producer: units from a global counter handed on through a
+//                                 4-slot mbarrier ring; loads the unit's 7 A slices (128 rows,
+//                                 112 KB, resident for the unit) and streams the B slices (64
+//                                 rows, 8 KB each) through a 5-stage ring;
+//                      warp 1     TMEM allocation; lane 0 issues tcgen05.mma kind::i8 (M = 128,
+//                                 N = 64, K = 32 per instruction, both operands from shared
+//                                 memory) into 7 int32 accumulators, one per level l (columns
+//                                 64 (l - 2));
+//                      warps 2-9  epilogue: warp w reads lane quadrant w % 4, 32 columns (all 7
+//                                 levels of 16 columns per tcgen05.wait::ld), releases the
+//                                 accumulators, combines the levels, scales by 2^{e_r + e_c},
+//                                 stages -value per row (256 bytes) and adds it to C with a bulk
+//                                 reduction (cp.reduce.async.bulk .add.f64) per row.
+// A work unit is (frequency, 128-row tile i, up to kOzSeg column tiles of 64); column tile c of
+// row tile i has work iff c < 2 (i + 1); rows are written from the column tile's first column
+// (the diagonal 64 x 64 blocks in full, as the other update kernels do).  Every mbarrier wait is
+// bounded as in kernels_tc.cu (expiry -> pivot 0 -> GWB200_DEVICE_TIMEOUT).
+#include "internal.cuh"
+#include "tc_common.cuh"
+
+#include <cstdlib>
+
+namespace gwb200 {
+namespace {
+
+using namespace tc;
+
+constexpr int kOzM = 128;                    // accumulator rows = TMEM lanes
+constexpr int kOzN = 64;                     // accumulator columns per level
+constexpr int kOzSlices = 7;                 // digit slices per value
+constexpr int kOzSeg = 32;                   // column tiles per work unit
+constexpr int kOzStages = 5;                 // B ring depth (one slice per stage)
+constexpr int kSchedSlots = 4;
+constexpr int kSliceA = kOzM * 128;          // one slice of 128 rows: 16 KB
+constexpr int kSliceB = kOzN * 128;          // of 64 rows: 8 KB
+constexpr int kEpiWarps = 8;                 // 4 lane quadrants x 2 column halves of 32
+constexpr int kOzThreads = 32 * (2 + kEpiWarps);
+constexpr int kTmemCols = 512;               // 7 levels x 64 columns used
+constexpr int kStgRow = 256 + 16;            // staging row stride: 32 doubles + 16 bytes (banks)
+constexpr int kStgBytes = 32 * kStgRow;      // per epilogue warp
+constexpr int kHeader = 1024;
+constexpr int kOzSmem = kHeader + 1024 + kOzSlices * kSliceA + kOzStages * kSliceB + kEpiWarps * kStgBytes;
+
+constexpr int kOffFull = 0;
+constexpr int kOffEmpty = kOffFull + 8 * kOzStages;
+constexpr int kOffTFull = kOffEmpty + 8 * kOzStages;    // accumulators ready (tcgen05.commit)
+constexpr int kOffTEmpty = kOffTFull + 8;               // accumulators drained (kEpiWarps arrivals)
+constexpr int kOffAFull = kOffTEmpty + 8;               // A slices of the unit loaded (tx bytes)
+constexpr int kOffAEmpty = kOffAFull + 8;               // MMAs of the unit complete
+constexpr int kOffDrain = kOffAEmpty + 8;
+constexpr int kOffUFull = kOffDrain + 8;
+constexpr int kOffUEmpty = kOffUFull + 8 * kSchedSlots;
+constexpr int kOffUnit = kOffUEmpty + 8 * kSchedSlots;
+constexpr int kOffTmem = kOffUnit + 8 * kSchedSlots;
+constexpr int kOffAbort = kOffTmem + 4;
+static_assert(kOffAbort + 4 <= kHeader, "header overflow");
+static_assert(kOzSmem <= 227 * 1024, "shared memory");
+
+// Instruction descriptor, kind::i8: D S32 (bits 4-5 = 2), A and B signed 8-bit (bits 7-9,
+// 10-12 = 1), both K-major, N >> 3 at bits 17-22, M >> 4 at bits 24-28.
+constexpr uint32_t kIdescI8 = (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(kOzN >> 3) << 17) |
+                              ((uint32_t)(kOzM >> 4) << 24);
+
+__device__ __forceinline__ void mma_i8(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
+        "l"(da), "l"(db), "r"(kIdescI8), "r"(accumulate)
+        : "memory");
+}
+
+__device__ __forceinline__ double pow2(int k) {  // 2^k for -1022 <= k <= 1023, exact
+    return __longlong_as_double((long long)(k + 1023) << 52);
+}
+
+// Per frequency: 7 slices of rp rows x 128 bytes, then rp int32 exponents.
+__host__ __device__ constexpr size_t oz_freq_bytes(int64_t rp) {
+    return ((size_t)kOzSlices * rp * 128 + (size_t)rp * 4 + 1023) / 1024 * 1024;
+}
+
+__global__ void __launch_bounds__(256) k_slice_panel64(const double* __restrict__ a, int64_t ld, int64_t stride,
+                                                       int64_t kb0, int64_t c_begin, int64_t rows, int64_t rp,
+                                                       uint8_t* __restrict__ buf) {
+    const int f = blockIdx.y;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int64_t rr = (int64_t)blockIdx.x * 8 + warp;  // panel row
+    if (rr >= rp) return;
+    const int64_t r = c_begin + rr;
+    uint8_t* slices = buf + (size_t)f * oz_freq_bytes(rp);
+    int32_t* exps = reinterpret_cast<int32_t*>(slices + (size_t)kOzSlices * rp * 128);
+    double x[4] = {0.0, 0.0, 0.0, 0.0};
+    if (r < rows) {
+        const double* row = a + (size_t)f * stride + (size_t)r * ld + kb0 + 4 * lane;
+#pragma unroll
+        for (int j = 0; j < 4; ++j) x[j] = row[j];
+    }
+    double m = fmax(fmax(fabs(x[0]), fabs(x[1])), fmax(fabs(x[2]), fabs(x[3])));
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+    int e = 0;
+    if (m > 0.0) frexp(m, &e);  // m = frac * 2^e, frac in [0.5, 1): |x| < 2^e
+    const double inv = pow2(-e);
+    double v[4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) v[j] = x[j] * inv;  // |v| < 1, exact
+    const uint32_t chunk = (uint32_t)(lane >> 2), in_chunk = (uint32_t)(lane & 3) * 4;
+    const size_t pos = (size_t)((chunk ^ (uint32_t)(rr & 7)) * 16 + in_chunk);
+#pragma unroll
+    for (int s = 0; s < kOzSlices; ++s) {
+        uint32_t word = 0;
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const double t = v[j] * 128.0;  // exact
+            const double d = trunc(t);       // |d| <= 127
+            v[j] = t - d;                    // exact
+            word |= ((uint32_t)(int)d & 0xFFu) << (8 * j);
+        }
+        *reinterpret_cast<uint32_t*>(slices + ((size_t)s * rp + rr) * 128 + pos) = word;
+    }
+    if (lane == 0) exps[rr] = e;
+}
+
+struct UnitSpace {
+    int64_t T, NI, NS, per_f, total;
+};
+
+// unit -> (frequency, row tile i, column tiles [c0, c1)); the longest row tiles first
+__device__ __forceinline__ bool decode_unit(const UnitSpace& us, int64_t u, int& f, int64_t& i, int64_t& c0,
+                                            int64_t& c1) {
+    f = (int)(u / us.per_f);
+    const int64_t rem = u - (int64_t)f * us.per_f;
+    const int64_t q = rem / us.NS;
+    i = us.NI - 1 - q;
+    c0 = (rem - q * us.NS) * kOzSeg;
+    c1 = min(c0 + kOzSeg, min(us.T, 2 * i + 2));
+    return c0 < c1;
+}
+
+__global__ void __launch_bounds__(kOzThreads, 1)
+    k_update64_oz(double* __restrict__ a, int64_t ld, int64_t stride, int64_t c_begin, int64_t rows,
+                  const uint8_t* __restrict__ buf, int64_t rp, UnitSpace us, unsigned long long* __restrict__ sched,
+                  unsigned long long* err, int withhold_first_stage) {
+    extern __shared__ __align__(1024) uint8_t osm[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint32_t base = smem_u32(osm);
+    const uint32_t abuf = (base + kHeader + 1023u) & ~1023u;  // 7 A slices, 1024-aligned
+    const uint32_t ring = abuf + kOzSlices * kSliceA;          // B stages
+    const uint32_t stg0 = ring + kOzStages * kSliceB;          // epilogue staging rows
+    volatile uint32_t* abort_flag = reinterpret_cast<volatile uint32_t*>(osm + kOffAbort);
+    volatile int64_t* uslot = reinterpret_cast<volatile int64_t*>(osm + kOffUnit);
+    auto full = [&](int s) { return base + kOffFull + 8 * s; };
+    auto empty = [&](int s) { return base + kOffEmpty + 8 * s; };
+    auto ufull = [&](int j) { return base + kOffUFull + 8 * j; };
+    auto uempty = [&](int j) { return base + kOffUEmpty + 8 * j; };
+    const uint32_t tfull = base + kOffTFull, tempty = base + kOffTEmpty;
+    const uint32_t afull = base + kOffAFull, aempty = base + kOffAEmpty, drain = base + kOffDrain;
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < kOzStages; ++s) {
+            mbar_init(full(s), 1);
+            mbar_init(empty(s), 1);
+        }
+        for (int j = 0; j < kSchedSlots; ++j) {
+            mbar_init(ufull(j), 1);
+            mbar_init(uempty(j), 1 + kEpiWarps);
+        }
+        mbar_init(tfull, 1);
+        mbar_init(tempty, kEpiWarps);
+        mbar_init(afull, 1);
+        mbar_init(aempty, 1);
+        mbar_init(drain, 1);
+        *abort_flag = 0u;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    }
+    if (warp == 1) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(base + kOffTmem),
+                     "r"(kTmemCols)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *reinterpret_cast<volatile uint32_t*>(osm + kOffTmem);
+    const size_t fbytes = oz_freq_bytes(rp);
+
+    if (warp == 0) {
+        // ---- producer ----
+        int s = 0, js = 0;
+        uint32_t ph = 0, aph = 0, jph = 0;
+        uint32_t filled = 0, fill_par = 0;
+        bool a_filled = false;
+        for (;;) {
+            int f = 0;
+            int64_t i = 0, c0 = 0, c1 = 0, u = 0;
+            if (lane == 0) {
+                do {
+                    u = (int64_t)atomicAdd(sched, 1ull);
+                } while (u < us.total && !decode_unit(us, u, f, i, c0, c1));
+                if (u > us.total) u = us.total;
+            }
+            u = __shfl_sync(0xffffffffu, u, 0);
+            uint32_t got = 1;
+            if (lane == 0) {
+                got = mbar_wait(uempty(js), jph ^ 1u, abort_flag, err) ? 1u : 0u;
+                if (got) {
+                    uslot[js] = u;
+                    mbar_arrive(ufull(js));
+                }
+            }
+            got = __shfl_sync(0xffffffffu, got, 0);
+            if (!got) break;
+            if (++js == kSchedSlots) {
+                js = 0;
+                jph ^= 1u;
+            }
+            if (u >= us.total) break;
+            decode_unit(us, u, f, i, c0, c1);
+            const uint8_t* slices = buf + (size_t)f * fbytes;
+            if (lane == 0) got = mbar_wait(aempty, aph ^ 1u, abort_flag, err) ? 1u : 0u;
+            got = __shfl_sync(0xffffffffu, got, 0);
+            if (!got) break;
+            if (lane == 0) mbar_expect_tx(afull, (uint32_t)(kOzSlices * kSliceA));
+            __syncwarp();
+            if (lane < kOzSlices)  // one 16 KB copy per slice
+                bulk_g2s(abuf + lane * kSliceA, slices + ((size_t)lane * rp + i * kOzM) * 128, kSliceA, afull);
+            a_filled = true;
+            aph ^= 1u;
+            bool ok = true;
+            for (int64_t c = c0; ok && c < c1; ++c) {
+                for (int t = 0; t < kOzSlices; ++t) {
+                    if (lane == 0) got = mbar_wait(empty(s), ph ^ 1u, abort_flag, err) ? 1u : 0u;
+                    got = __shfl_sync(0xffffffffu, got, 0);
+                    if (!got) {
+                        ok = false;
+                        break;
+                    }
+                    if (withhold_first_stage && blockIdx.x == 0 && filled == 0) {
+                        withhold_first_stage = 0;  // test of the bounded waits (see kernels_tc.cu)
+                    } else {
+                        if (lane == 0) {
+                            mbar_expect_tx(full(s), (uint32_t)kSliceB);
+                            bulk_g2s(ring + s * kSliceB, slices + ((size_t)t * rp + c * kOzN) * 128, kSliceB, full(s));
+                        }
+                        filled |= 1u << s;
+                        fill_par = (fill_par & ~(1u << s)) | (ph << s);
+                    }
+                    __syncwarp();
+                    if (++s == kOzStages) {
+                        s = 0;
+                        ph ^= 1u;
+                    }
+                }
+            }
+            if (!ok) break;
+        }
+        if (lane == 0) {
+            for (int q = 0; q < kOzStages; ++q)
+                if (filled & (1u << q)) mbar_drain(full(q), (fill_par >> q) & 1u);
+            if (a_filled) mbar_drain(afull, aph ^ 1u);
+        }
+        __syncwarp();
+    } else if (warp == 1 && lane == 0) {
+        // ---- MMA issuer ----
+        int s = 0, js = 0;
+        uint32_t ph = 0, acc_ph = 0, aph = 0, jph = 0;
+        bool issued = false, ok = true;
+        for (;;) {
+            const int64_t u = take_unit(ufull(js), uempty(js), uslot + js, jph, abort_flag, err);
+            if (++js == kSchedSlots) {
+                js = 0;
+                jph ^= 1u;
+            }
+            if (u < 0 || u >= us.total) break;
+            int f;
+            int64_t i, c0, c1;
+            decode_unit(us, u, f, i, c0, c1);
+            if (!mbar_wait(afull, aph, abort_flag, err)) break;
+            aph ^= 1u;
+            for (int64_t c = c0; ok && c < c1; ++c) {
+                if (!mbar_wait(tempty, acc_ph ^ 1u, abort_flag, err)) {
+                    ok = false;
+                    break;
+                }
+                tc_fence_after();
+                for (int t = 0; t < kOzSlices; ++t) {  // B slice t+1 against A slices 1 .. 7-t
+                    if (!mbar_wait(full(s), ph, abort_flag, err)) {
+                        ok = false;
+                        break;
+                    }
+                    tc_fence_after();
+                    const uint32_t bst = ring + s * kSliceB;
+                    for (int sa = 0; sa < kOzSlices - t; ++sa) {
+                        const uint32_t d = tmem + (uint32_t)((sa + t) * kOzN);  // level sa + t + 2
+#pragma unroll
+                        for (int kk = 0; kk < 4; ++kk)
+                            mma_i8(d, smem_desc_sw128(abuf + sa * kSliceA + 32u * kk), smem_desc_sw128(bst + 32u * kk),
+                                   (t > 0 || kk > 0) ? 1u : 0u);
+                    }
+                    mma_commit(empty(s));
+                    issued = true;
+                    if (++s == kOzStages) {
+                        s = 0;
+                        ph ^= 1u;
+                    }
+                }
+                if (!ok) break;
+                mma_commit(tfull);
+                acc_ph ^= 1u;
+            }
+            if (!ok) break;
+            mma_commit(aempty);
+        }
+        if (issued) {
+            mma_commit(drain);
+            mbar_drain(drain, 0);
+        }
+    } else if (warp >= 2) {
+        // ---- epilogue ----
+        const int q = warp & 3, half = (warp - 2) >> 2;
+        const uint32_t stg = stg0 + (uint32_t)(warp - 2) * kStgBytes + (uint32_t)lane * kStgRow;
+        int js = 0;
+        uint32_t acc_ph = 0, jph = 0;
+        bool ok = true, reduced = false;
+        while (ok) {
+            int64_t u = 0;
+            if (lane == 0) u = take_unit(ufull(js), uempty(js), uslot + js, jph, abort_flag, err);
+            u = __shfl_sync(0xffffffffu, u, 0);
+            if (++js == kSchedSlots) {
+                js = 0;
+                jph ^= 1u;
+            }
+            if (u < 0 || u >= us.total) break;
+            int f;
+            int64_t i, c0, c1;
+            decode_unit(us, u, f, i, c0, c1);
+            const uint8_t* slices = buf + (size_t)f * fbytes;
+            const int32_t* exps = reinterpret_cast<const int32_t*>(slices + (size_t)kOzSlices * rp * 128);
+            const int64_t rr = i * kOzM + q * 32 + lane;  // panel row of this lane
+            const int64_t r = c_begin + rr;
+            const int er = exps[rr];
+            for (int64_t c = c0; c < c1; ++c) {
+                const int64_t cj = c_begin + c * kOzN + half * 32;  // this warp's first column
+                const bool valid = r < rows && r >= c_begin + c * kOzN;
+                const int ec_lane = exps[c * kOzN + half * 32 + lane];  // exponent of column cj + lane
+                uint32_t got = 1;
+                if (lane == 0) got = mbar_wait(tfull, acc_ph, abort_flag, err) ? 1u : 0u;
+                got = __shfl_sync(0xffffffffu, got, 0);
+                if (!got) {
+                    ok = false;
+                    break;
+                }
+                acc_ph ^= 1u;
+                tc_fence_after();
+                // levels combined exactly in integers (|S_l| < 2^24): hi = S2 2^21 + S3 2^14 + S4 2^7 + S5
+                // (< 2^46), lo = S6 2^14 + S7 2^7 + S8 (< 2^39); value = hi 2^-35 + lo 2^-56 (one rounding)
+                double tot[32];
+#pragma unroll
+                for (int h16 = 0; h16 < 2; ++h16) {
+                    uint32_t v[kOzSlices][16];
+#pragma unroll
+                    for (int L = 0; L < kOzSlices; ++L)
+                        tmem_ld16_nowait(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(L * kOzN + half * 32 + 16 * h16), v[L]);
+                    tmem_wait_ld();
+                    if (h16 == 1) {  // every level is in registers: the accumulators are free
+                        tc_fence_before();
+                        __syncwarp();
+                        if (lane == 0) mbar_arrive(tempty);
+                    }
+#pragma unroll
+                    for (int j = 0; j < 16; ++j) {
+                        const long long hi = (long long)(int32_t)v[0][j] * (1LL << 21) + (long long)(int32_t)v[1][j] * (1LL << 14) +
+                                             (long long)(int32_t)v[2][j] * (1LL << 7) + (long long)(int32_t)v[3][j];
+                        const long long lo = (long long)(int32_t)v[4][j] * (1LL << 14) + (long long)(int32_t)v[5][j] * (1LL << 7) +
+                                             (long long)(int32_t)v[6][j];
+                        tot[16 * h16 + j] = fma((double)hi, 0x1p-35, (double)lo * 0x1p-56);
+                    }
+                }
+                if (valid) {
+                    if (reduced) asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
+#pragma unroll
+                    for (int j = 0; j < 32; j += 2) {
+                        const int e0 = __shfl_sync(0xffffffffu, ec_lane, j), e1 = __shfl_sync(0xffffffffu, ec_lane, j + 1);
+                        const double v0 = -tot[j] * pow2(er + e0), v1 = -tot[j + 1] * pow2(er + e1);
+                        asm volatile("st.shared.v2.f64 [%0], {%1, %2};" ::"r"(stg + 8u * j), "d"(v0), "d"(v1) : "memory");
+                    }
+                } else {
+#pragma unroll
+                    for (int j = 0; j < 32; j += 2) {  // keep the warp's shuffles converged
+                        (void)__shfl_sync(0xffffffffu, ec_lane, j);
+                        (void)__shfl_sync(0xffffffffu, ec_lane, j + 1);
+                    }
+                }
+                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                if (valid) {
+                    double* dst = a + (size_t)f * stride + (size_t)r * ld + cj;
+                    asm volatile("cp.reduce.async.bulk.global.shared::cta.bulk_group.add.f64 [%0], [%1], 256;" ::"l"(dst),
+                                 "r"(stg)
+                                 : "memory");
+                    asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+                    reduced = true;
+                }
+            }
+        }
+        if (reduced) asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");  // this lane's reductions done
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 1) {
+        __syncwarp();
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols) : "memory");
+    }
+}
+
+} // namespace
+
+size_t oz_slice_bytes_per_freq(const TallGeometry& g) { return oz_freq_bytes((g.rows + kOzM - 1) / kOzM * kOzM); }
+
+int launch_update64_oz(const TallGeometry& g, int64_t nf, double* a, int64_t kb0, int64_t c_begin, void* slices,
+                       unsigned long long* sched, unsigned long long* err, cudaStream_t s) {
+    const int64_t T = (g.n_pad - c_begin) / kOzN;
+    if (T <= 0 || nf <= 0) return 0;
+    const int64_t H = g.rows - c_begin;
+    const int64_t NI = (H + kOzM - 1) / kOzM, rp = NI * kOzM;
+    uint8_t* buf = static_cast<uint8_t*>(slices);
+    k_slice_panel64<<<dim3((unsigned)(rp / 8), (unsigned)nf), 256, 0, s>>>(a, g.ld, g.stride, kb0, c_begin, g.rows, rp,
+                                                                          buf);
+    GWB_LAUNCH("k_slice_panel64");
+    GWB_CUDA(cudaFuncSetAttribute(k_update64_oz, cudaFuncAttributeMaxDynamicSharedMemorySize, kOzSmem));
+    UnitSpace us;
+    us.T = T;
+    us.NI = NI;
+    us.NS = (T + kOzSeg - 1) / kOzSeg;
+    us.per_f = NI * us.NS;
+    us.total = nf * us.per_f;
+    GWB_CUDA(cudaMemsetAsync(sched, 0, sizeof(unsigned long long), s));
+    const char* expire = std::getenv("GWB200_TEST_EXPIRE_WAIT");
+    const int withhold = (expire && expire[0] == '1') ? 1 : 0;
+    const unsigned grid = (unsigned)std::min<int64_t>(us.total, sm_count());
+    k_update64_oz<<<grid, kOzThreads, kOzSmem, s>>>(a, g.ld, g.stride, c_begin, g.rows, buf, rp, us, sched, err,
+                                                     withhold);
+    GWB_LAUNCH("k_update64_oz");
+    return 2;
+}
+
+} // namespace gwb200

@@ -15,8 +15,8 @@
 //   k_update32_tc    a persistent, warp-specialised kernel, one CTA per SM (18 warps, 226 KB of
 //                    shared memory, all 512 TMEM columns):
 //                      warp 0     producer: takes work units from a global counter and hands them
-//                                 to the other roles through a 4-slot mbarrier ring; loads the
-//                                 streams B (128 rows x 32 of K, hi and lo) through a 6-stage ring,
+//                                 to the other roles through a 4-slot mbarrier ring; streams B
+//                                 (128 rows x 32 of K, hi and lo) through a 6-stage ring,
 //                                 and prefetches the unit's A rows into L2;
 //                      warp 1     allocates TMEM; lane 0 issues tcgen05.mma kind::tf32 (M = 128,
 //                                 N = 128, K = 8 per instruction) with A from TMEM (the unit's 128
@@ -40,6 +40,7 @@
 // abort flag, records 0 in the pivot word (read back by the host as GWB200_DEVICE_TIMEOUT), waits
 // (bounded) for its own bulk copies and MMAs, frees its TMEM and returns.
 #include "internal.cuh"
+#include "tc_common.cuh"
 
 #include <cuda.h>
 #include <cudaTypedefs.h>
@@ -49,6 +50,8 @@
 
 namespace gwb200 {
 namespace {
+
+using namespace tc;
 
 constexpr int kTcM = 128;                   // accumulator rows = TMEM lanes = A rows per unit
 constexpr int kTcN = 128;                   // accumulator columns per tile
@@ -69,7 +72,6 @@ constexpr int kHeader = 1024;        // mbarriers, unit ring, TMEM address, abor
 // 128-byte swizzle is applied to shared-memory address bits, so every slice is 1024-aligned)
 constexpr int kStgBytes = 32 * 32 * 4;       // per epilogue warp: 32 rows x 32 floats, 128B-swizzled
 constexpr int kTcSmem = kHeader + 1024 + kTcStages * kStageBytes + kEpiWarps * kStgBytes;
-constexpr unsigned long long kWaitNs = 2000000000ull;
 
 // header layout (byte offsets)
 constexpr int kOffFull = 0;                              // kTcStages: B stage filled (tx bytes)
@@ -88,76 +90,6 @@ constexpr int kOffAbort = kOffTmem + 4;                  // u32 abort flag
 static_assert(kOffAbort + 4 <= kHeader, "header overflow");
 static_assert(kTcSmem <= 227 * 1024, "shared memory");
 
-__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
-
-__device__ __forceinline__ unsigned long long globaltimer() {
-    unsigned long long t;
-    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-    return t;
-}
-
-__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
-}
-__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
-    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
-}
-__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
-}
-__device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity) {
-    uint32_t ok;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-        "selp.b32 %0, 1, 0, p;\n\t}"
-        : "=r"(ok)
-        : "r"(bar), "r"(parity)
-        : "memory");
-    return ok != 0;
-}
-// Wait for the phase of parity `parity` to complete; false on abort or expiry (which raises abort
-// and records the timeout).
-__device__ __noinline__ bool mbar_wait(uint32_t bar, uint32_t parity, volatile uint32_t* abort_flag,
-                                       unsigned long long* err) {
-    if (mbar_try(bar, parity)) return true;
-    const unsigned long long t0 = globaltimer();
-    for (;;) {
-        if (mbar_try(bar, parity)) return true;
-        if (*abort_flag) return false;
-        if (globaltimer() - t0 > kWaitNs) {
-            *abort_flag = 1u;
-            atomicMin(err, 0ull);
-            return false;
-        }
-    }
-}
-// Bounded wait used only while draining: no abort check, no error record.
-__device__ __forceinline__ void mbar_drain(uint32_t bar, uint32_t parity) {
-    if (mbar_try(bar, parity)) return;
-    const unsigned long long t0 = globaltimer();
-    while (!mbar_try(bar, parity) && globaltimer() - t0 < kWaitNs) {
-    }
-}
-
-__device__ __forceinline__ void bulk_g2s(uint32_t dst, const void* src, uint32_t bytes, uint32_t bar) {
-    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
-                 "l"(src), "r"(bytes), "r"(bar)
-                 : "memory");
-}
-
-__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
-__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
-
-// Shared-memory matrix descriptor, K-major, 128-byte swizzle: rows of 128 bytes (32 floats of K),
-// 8-row groups of 1024 bytes (SBO), 16-byte chunk c of row r stored at chunk c ^ (r % 8); the
-// start address advances by 32 bytes per 8-deep K step inside the 128-byte row; LBO (unused for
-// swizzled K-major) 16 bytes; version 1 (bit 46), base offset 0 (1024-aligned slices), layout
-// type 2 = SWIZZLE_128B (bits 61-63).
-__device__ __forceinline__ uint64_t smem_desc_sw128(uint32_t addr) {
-    return (uint64_t)((addr >> 4) & 0x3FFFu) | ((uint64_t)(16 >> 4) << 16) | ((uint64_t)(1024 >> 4) << 32) |
-           (1ull << 46) | (2ull << 61);
-}
 // Instruction descriptor, kind::tf32: D FP32 (bits 4-5 = 1), A and B TF32 (bits 7-9, 10-12 = 2),
 // both K-major (bits 15, 16 = 0), N >> 3 at bits 17-22, M >> 4 at bits 24-28.
 constexpr uint32_t kIdescTf32 =
@@ -191,25 +123,6 @@ __device__ __forceinline__ void tma_reduce_add_3d(const CUtensorMap* map, uint32
                  : "memory");
     asm volatile("cp.async.bulk.commit_group;" ::: "memory");
 }
-__device__ __forceinline__ void mma_commit(uint32_t bar) {
-    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar) : "memory");
-}
-
-__device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32]) {
-    uint32_t r[32];
-    asm volatile(
-        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
-        "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
-        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
-          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
-          "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
-          "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
-        : "r"(taddr));
-    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-#pragma unroll
-    for (int j = 0; j < 32; ++j) v[j] = __uint_as_float(r[j]);
-}
-
 __device__ __forceinline__ float rna_tf32(float x) {
     uint32_t r;
     asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
@@ -267,15 +180,6 @@ __device__ __forceinline__ bool decode_unit(const UnitSpace& us, int64_t u, int&
     c0 = (rem - q * us.NS) * kTcSeg;
     c1 = min(c0 + kTcSeg, min(us.T, i + 1));
     return c0 < c1;
-}
-
-// Consumer side of the unit ring: the next unit index (>= total: no more work), or -1 on abort.
-__device__ __forceinline__ int64_t take_unit(uint32_t ufull, uint32_t uempty, const volatile int64_t* slot,
-                                             uint32_t parity, volatile uint32_t* abort_flag, unsigned long long* err) {
-    if (!mbar_wait(ufull, parity, abort_flag, err)) return -1;
-    const int64_t u = *slot;
-    mbar_arrive(uempty);
-    return u;
 }
 
 __global__ void __launch_bounds__(kTcThreads, 1)
@@ -599,17 +503,6 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         tc_fence_after();
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols) : "memory");
     }
-}
-
-int sm_count() {
-    static int n = 0;
-    static std::once_flag once;
-    std::call_once(once, [] {
-        int dev = 0;
-        cudaGetDevice(&dev);
-        if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n <= 0) n = 148;
-    });
-    return n;
 }
 
 } // namespace

@@ -397,6 +397,53 @@ def test_tcgen05_update_bit_identical_to_mma_sync(backend, monkeypatch, nmo, noc
     assert np.abs(q_tc - q64).max() <= 2e-5 * np.abs(q64).max()
 
 
+@pytest.mark.parametrize("nmo,nocc,nst,nfreq,chunk", [
+    (40, 10, 4, 6, None),     # n = 300
+    (80, 20, 6, 8, "3"),      # n = 1200, three frequency chunks
+    (150, 30, 4, 16, None),   # n = 3600
+])
+def test_int8_emulated_fp64_update_matches_dmma(backend, monkeypatch, nmo, nocc, nst, nfreq, chunk):
+    """The plain form's trailing update emulated on the int8 tensor cores (kernels_oz.cu, 7-digit
+    row slices, exact int32 products) gives the screened forms of the FP64 DMMA update to 1e-12
+    relative (measured ~8e-14), deterministically."""
+    from minigw_b200 import generate_transformed_legendre_grid
+    from minigw_b200.synthetic import make_input
+
+    if chunk:
+        monkeypatch.setenv("GWB200_MAX_FREQ_CHUNK", chunk)
+    inp = make_input(nmo, nocc, seed=nmo)
+    om, _ = generate_transformed_legendre_grid(nfreq)
+    states = list(range(nocc - nst // 2, nocc - nst // 2 + nst))
+    backend.load_system(inp)
+    q64, st64 = backend.screened_forms(om, states)
+    monkeypatch.setenv("GWB200_FP64_UPDATE", "ozaki")
+    qo, sto = backend.screened_forms(om, states)
+    qo2, _ = backend.screened_forms(om, states)
+    assert sto["kernel_launches"] > st64["kernel_launches"]  # the int8 path ran (two launches per update)
+    assert np.abs(qo - q64).max() <= 1e-12 * np.abs(q64).max()
+    np.testing.assert_array_equal(qo, qo2)
+
+
+def test_int8_emulated_update_expired_wait(backend, monkeypatch):
+    """The int8 update's bounded waits: a withheld operand stage ends in GWB200_DEVICE_TIMEOUT and
+    the context stays usable."""
+    from minigw_b200 import GwB200Error, generate_transformed_legendre_grid
+    from minigw_b200.synthetic import make_input
+
+    backend.load_system(make_input(40, 10, seed=3))
+    om, _ = generate_transformed_legendre_grid(4)
+    monkeypatch.setenv("GWB200_FP64_UPDATE", "ozaki")
+    monkeypatch.setenv("GWB200_TEST_EXPIRE_WAIT", "1")
+    with pytest.raises(GwB200Error) as e:
+        backend.screened_forms(om, [9, 10])
+    assert e.value.status == "GWB200_DEVICE_TIMEOUT"
+    monkeypatch.delenv("GWB200_TEST_EXPIRE_WAIT")
+    qo, _ = backend.screened_forms(om, [9, 10])
+    monkeypatch.delenv("GWB200_FP64_UPDATE")
+    q64, _ = backend.screened_forms(om, [9, 10])
+    assert np.abs(qo - q64).max() <= 1e-12 * np.abs(q64).max()
+
+
 def test_tcgen05_expired_wait_reports_device_timeout(backend, monkeypatch):
     """Every mbarrier wait of the tcgen05 update is bounded.  With one operand stage withheld
     (test hook), the wait for it expires after about two seconds: the call returns
