@@ -288,6 +288,7 @@ __global__ void __launch_bounds__(kOzThreads, 1)
         __syncwarp();
     } else if (warp == 1 && lane == 0) {
         // ---- MMA issuer ----
+        const uint64_t desc_a0 = smem_desc_sw128(abuf), desc_b0 = smem_desc_sw128(ring);
         int s = 0, js = 0;
         uint32_t ph = 0, acc_ph = 0, aph = 0, jph = 0;
         bool issued = false, ok = true;
@@ -309,19 +310,25 @@ __global__ void __launch_bounds__(kOzThreads, 1)
                     break;
                 }
                 tc_fence_after();
+#pragma unroll
                 for (int t = 0; t < kOzSlices; ++t) {  // B slice t+1 against A slices 1 .. 7-t
                     if (!mbar_wait(full(s), ph, abort_flag, err)) {
                         ok = false;
                         break;
                     }
                     tc_fence_after();
-                    const uint32_t bst = ring + s * kSliceB;
-                    for (int sa = 0; sa < kOzSlices - t; ++sa) {
-                        const uint32_t d = tmem + (uint32_t)((sa + t) * kOzN);  // level sa + t + 2
+                    // descriptors differ from the stage / A bases only in the address field
+                    // (bytes >> 4, below 2^14 for shared memory): constant offsets, no carries
+                    const uint64_t db0 = desc_b0 + (uint64_t)((uint32_t)(s * kSliceB) >> 4);
 #pragma unroll
-                        for (int kk = 0; kk < 4; ++kk)
-                            mma_i8(d, smem_desc_sw128(abuf + sa * kSliceA + 32u * kk), smem_desc_sw128(bst + 32u * kk),
-                                   (t > 0 || kk > 0) ? 1u : 0u);
+                    for (int sa = 0; sa < kOzSlices; ++sa) {
+                        if (sa < kOzSlices - t) {
+                            const uint32_t d = tmem + (uint32_t)((sa + t) * kOzN);  // level sa + t + 2
+#pragma unroll
+                            for (int kk = 0; kk < 4; ++kk)
+                                mma_i8(d, desc_a0 + (uint64_t)((sa * kSliceA + 32 * kk) >> 4), db0 + (uint64_t)(2 * kk),
+                                       (t > 0 || kk > 0) ? 1u : 0u);
+                        }
                     }
                     mma_commit(empty(s));
                     issued = true;
@@ -378,9 +385,11 @@ __global__ void __launch_bounds__(kOzThreads, 1)
                 }
                 acc_ph ^= 1u;
                 tc_fence_after();
-                // levels combined exactly in integers (|S_l| < 2^24): hi = S2 2^21 + S3 2^14 + S4 2^7 + S5
-                // (< 2^46), lo = S6 2^14 + S7 2^7 + S8 (< 2^39); value = hi 2^-35 + lo 2^-56 (one rounding)
-                double tot[32];
+                // Levels combined exactly: adjacent pairs in int32 (S_l <= (l-1) 127^2 128, so
+                // S2 2^7 + S3, S4 2^7 + S5, S6 2^7 + S7 < 2^31), then hi = (S2 2^7 + S3) 2^14 +
+                // S4 2^7 + S5 < 2^43 and lo = (S6 2^7 + S7) 2^7 + S8 < 2^39 in int64; value =
+                // hi 2^-35 + lo 2^-56 with one rounding, scaled by 2^{e_r + e_c}.
+                double val[32];
 #pragma unroll
                 for (int h16 = 0; h16 < 2; ++h16) {
                     uint32_t v[kOzSlices][16];
@@ -395,27 +404,21 @@ __global__ void __launch_bounds__(kOzThreads, 1)
                     }
 #pragma unroll
                     for (int j = 0; j < 16; ++j) {
-                        const long long hi = (long long)(int32_t)v[0][j] * (1LL << 21) + (long long)(int32_t)v[1][j] * (1LL << 14) +
-                                             (long long)(int32_t)v[2][j] * (1LL << 7) + (long long)(int32_t)v[3][j];
-                        const long long lo = (long long)(int32_t)v[4][j] * (1LL << 14) + (long long)(int32_t)v[5][j] * (1LL << 7) +
-                                             (long long)(int32_t)v[6][j];
-                        tot[16 * h16 + j] = fma((double)hi, 0x1p-35, (double)lo * 0x1p-56);
+                        const int32_t p23 = (int32_t)v[0][j] * 128 + (int32_t)v[1][j];
+                        const int32_t p45 = (int32_t)v[2][j] * 128 + (int32_t)v[3][j];
+                        const int32_t p67 = (int32_t)v[4][j] * 128 + (int32_t)v[5][j];
+                        const long long hi = (long long)p23 * (1LL << 14) + p45;
+                        const long long lo = (long long)p67 * 128 + (int32_t)v[6][j];
+                        const int ej = __shfl_sync(0xffffffffu, ec_lane, 16 * h16 + j);
+                        val[16 * h16 + j] = -fma((double)hi, 0x1p-35, (double)lo * 0x1p-56) * pow2(er + ej);
                     }
                 }
-                if (valid) {
+                if (valid) {  // stage the row (256 bytes), then one bulk reduction
                     if (reduced) asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
 #pragma unroll
-                    for (int j = 0; j < 32; j += 2) {
-                        const int e0 = __shfl_sync(0xffffffffu, ec_lane, j), e1 = __shfl_sync(0xffffffffu, ec_lane, j + 1);
-                        const double v0 = -tot[j] * pow2(er + e0), v1 = -tot[j + 1] * pow2(er + e1);
-                        asm volatile("st.shared.v2.f64 [%0], {%1, %2};" ::"r"(stg + 8u * j), "d"(v0), "d"(v1) : "memory");
-                    }
-                } else {
-#pragma unroll
-                    for (int j = 0; j < 32; j += 2) {  // keep the warp's shuffles converged
-                        (void)__shfl_sync(0xffffffffu, ec_lane, j);
-                        (void)__shfl_sync(0xffffffffu, ec_lane, j + 1);
-                    }
+                    for (int j = 0; j < 32; j += 2)
+                        asm volatile("st.shared.v2.f64 [%0], {%1, %2};" ::"r"(stg + 8u * j), "d"(val[j]), "d"(val[j + 1])
+                                     : "memory");
                 }
                 asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
                 if (valid) {
