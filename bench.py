@@ -147,6 +147,15 @@ def cpu_reference_sample(inp, wl, omegas, weights, pairs: int, threads: int):
             "solves_per_s": 1.0 / (wl.nfreq ** 2 * per_pair)}
 
 
+def traffic_oz(workload: str):
+    """DRAM bytes per k_update64_oz launch from the committed ncu capture, if one exists."""
+    try:
+        return json.loads((ROOT / "profiles" / "k_update64_oz_traffic.json").read_text())["workloads"][workload][
+            "bytes_per_launch"]
+    except (OSError, ValueError, KeyError):
+        return None
+
+
 def hbm_peak_gbs() -> float:
     """Measured HBM copy bandwidth of this pool's B200s (MEASURED_PEAKS.json), else the fallback."""
     try:
@@ -324,7 +333,7 @@ def run_b200(args, wl):
     traffic = None
     try:  # DRAM bytes per launch of the dominant kernel from the committed ncu capture of this workload
         tr = json.loads((ROOT / "profiles" / "k_update_traffic.json").read_text())["workloads"].get(wl.name, {})
-        if "bytes_per_launch" in tr and args.precision == "fp64":
+        if "bytes_per_launch" in tr and args.precision == "fp64" and 0 <= stats[0].get("update_kernel", 0) < 6:
             traffic = tr["bytes_per_launch"]
     except (OSError, ValueError, KeyError):
         pass
@@ -365,6 +374,22 @@ def run_b200(args, wl):
         "gpu_launches": int(launches),
         "clocks": clock_info,
     }
+    kernel_used = stats[0].get("update_kernel", -1)
+    if args.precision == "fp64" and kernel_used == 6 and achieved:
+        # the autotuner chose the int8 tensor-core emulation of the FP64 update (k_slice_panel64 +
+        # k_update64_oz, timed together): bound by the FP64 C read+write, 16 bytes per updated
+        # element per K = 128 pass, i.e. flops_update / 16 bytes; the int8 work is 28 products of
+        # 7-digit slices per FP64 product
+        gbs = upd_flops / 16.0 / (upd_ms * 1e-3) / 1e9
+        result["roofline"] = {
+            "bound": "hbm", "kernel": "k_update64_oz (FP64 trailing update emulated on int8 tcgen05, with "
+                                      "k_slice_panel64)",
+            "achieved": gbs, "peak": hbm_peak_gbs(), "unit": "GB/s", "frac": gbs / hbm_peak_gbs(),
+            "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)",
+            "tflops_fp64_equivalent": achieved, "int8_tops": achieved * 28.0,
+            "vs_fp64_dmma_peak": achieved / peak_fp64, "launches": upd_n, "traffic": traffic_oz(wl.name),
+            "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum per k_update64_oz launch "
+                              "(profiles/k_update64_oz_traffic.json)" if traffic_oz(wl.name) else None}
     if args.precision == "mixed" and achieved:
         # the tcgen05 3xTF32 trailing update (k_split_panel32 + k_update32_tc, timed together) is
         # bound by the FP32 C read+write, 8 bytes per updated element per K = 128 pass, i.e.

@@ -64,6 +64,10 @@ typedef struct gwb200_stats {
     double device_ms_update;
     int64_t update_launches;
     double flops_update;
+    /* The trailing-update kernel the screening used: 0-5 one of the FP64 DMMA variants, 6 the
+     * int8 tensor-core emulation of the FP64 update, 7 the mixed form's tcgen05 3xTF32 update, 8 the
+     * mixed form's mma.sync update, -1 none (no outer trailing update, or eta != 0). */
+    int64_t update_kernel;
 } gwb200_stats;
 
 typedef struct gwb200_handle gwb200_handle;

@@ -66,6 +66,7 @@ class Stats(C.Structure):
         ("device_ms_update", C.c_double),
         ("update_launches", C.c_int64),
         ("flops_update", C.c_double),
+        ("update_kernel", C.c_int64),
     ]
 
     def as_dict(self) -> dict:

@@ -137,12 +137,6 @@ bool mixed_update_on_tcgen05() {
     return !(env && std::strcmp(env, "mma") == 0);
 }
 
-// The plain form's outer trailing updates run as the int8 tensor-core emulation (kernels_oz.cu)
-// when GWB200_FP64_UPDATE=ozaki, else on the FP64 DMMA pipe.
-bool fp64_update_ozaki() {
-    const char* env = std::getenv("GWB200_FP64_UPDATE");
-    return env && std::strcmp(env, "ozaki") == 0;
-}
 
 // Allocate `b` for `want` bytes: grow-only, or exact and stream-ordered when the handle is limited.
 void size_buffer(gwb200_handle* h, DevBuf& b, size_t want) {
@@ -222,7 +216,9 @@ void compute_forms(gwb200_handle* h, const double* omega, int64_t nfreq, const i
 
     // Frequency chunk size from the HBM budget: tall matrices + scale vectors + 64x64 inverses.
     const bool mixed_tc = mixed && mixed_update_on_tcgen05();
-    const bool fp64_oz = !mixed && !cplx && fp64_update_ozaki();
+    // plain form: the int8 emulation of the outer updates is a candidate of the update autotuner
+    // (its slice workspace is part of the budget) unless GWB200_FP64_UPDATE=dmma
+    const bool fp64_oz = !mixed && !cplx && fp64_update_mode() != 1;
     const size_t per_freq = mixed ? sizeof(float) * ((size_t)g.stride + kNb * kNb) + sizeof(double) * (g.n_pad + g.m_pad) +
                                         (mixed_tc ? tc_panel_bytes_per_freq(g) : 0)
                                   : sizeof(double) * planes * ((size_t)g.stride + g.n_pad + kNb * kNb + g.m_pad) +
@@ -299,7 +295,9 @@ void compute_forms(gwb200_handle* h, const double* omega, int64_t nfreq, const i
                                               mixed_tc ? h->panel32.as<float>() : nullptr,
                                               h->tc_sched.as<unsigned long long>());
         } else {
-            if (upd_variant < 0) upd_variant = tune_update_variant(g, nf, h->a.as<double>(), s);
+            if (upd_variant < 0)
+                upd_variant = tune_update_variant(g, nf, h->a.as<double>(), s, fp64_oz ? h->panel32.p : nullptr,
+                                                  h->tc_sched.as<unsigned long long>(), h->err.as<unsigned long long>());
             launches += launch_build_tall(g, h->v.as<double>(), h->xt.as<double>(), h->dvec.as<double>(), nf,
                                           h->a.as<double>(), s);
             launches += launch_factor_chunk(g, nf, h->a.as<double>(), h->linv.as<double>(), h->qacc.as<double>(),
@@ -314,6 +312,8 @@ void compute_forms(gwb200_handle* h, const double* omega, int64_t nfreq, const i
     GWB_CUDA(cudaEventRecord(h->ev[2], s));
     if (st) {
         const double nd = (double)g.n, md = (double)m;
+        st->update_kernel = -1;
+        if (g.n_pad / kNb > 2 && !cplx) st->update_kernel = mixed ? (mixed_tc ? 7 : 8) : upd_variant;
         st->flops_screening = (double)nfreq * (nd * nd * nd / 3.0 + nd * nd * md + 3.0 * nd * md);
         st->frequency_chunks = chunks;
         st->kernel_launches = launches;

@@ -119,9 +119,9 @@ int launch_build_tall(const TallGeometry& g, const double* v, const double* xt, 
 // Blocked Cholesky of the tall matrices of nf frequencies (outer blocks of two 64-wide inner
 // blocks); returns launches issued.
 // `variant`: index into the FP64 update kernel table (tune_update_variant); -1: GWB200_UPDATE_VARIANT
-// if set, else the default.  oz != NULL: the outer trailing updates run as the int8 emulation of
+// if set, else the default; kUpdateOzaki: the outer trailing updates run as the int8 emulation of
 // kernels_oz.cu with `oz` as its slice workspace (oz_slice_bytes_per_freq(g) per frequency) and
-// `sched` as its work counter.
+// `sched` as its work counter (look-left updates on the default DMMA kernel).
 int launch_factor_chunk(const TallGeometry& g, int64_t nf, double* a, double* linv, double* qacc,
                         unsigned long long* err_pivot, cudaStream_t s, UpdateProfiler* prof, int variant,
                         void* oz = nullptr, unsigned long long* sched = nullptr);
@@ -134,7 +134,12 @@ int launch_update64_oz(const TallGeometry& g, int64_t nf, double* a, int64_t kb0
 // variant on this geometry's largest trailing update, timed once per (device, n_pad, rows, nf) per
 // process in the workspace `a` (nf tall matrices) BEFORE the matrices are built there (the timing
 // overwrites it).  The default is kept unless another variant is more than 3% faster.
-int tune_update_variant(const TallGeometry& g, int64_t nf, double* a, cudaStream_t s);
+// oz != NULL adds the int8 emulation of the outer updates (kernels_oz.cu) as a candidate
+// (kUpdateOzaki), timed with the slicing; GWB200_FP64_UPDATE=dmma / =ozaki force either side.
+constexpr int kUpdateOzaki = 6;
+int fp64_update_mode();
+int tune_update_variant(const TallGeometry& g, int64_t nf, double* a, cudaStream_t s, void* oz = nullptr,
+                        unsigned long long* sched = nullptr, unsigned long long* err_pivot = nullptr);
 const char* update_variant_name(int v);
 // Contraction of the screened forms of nf_int integration frequencies onto nf_out output
 // frequencies (the full grid; a shard of integration frequencies gives a partial sum).

@@ -14,6 +14,7 @@
 
 #include <array>
 #include <cstdio>
+#include <cstring>
 #include <map>
 #include <mutex>
 
@@ -430,6 +431,17 @@ const UpdateVariant kVariants[] = {
 };
 constexpr int kNumVariants = (int)(sizeof(kVariants) / sizeof(kVariants[0]));
 
+}  // namespace
+
+int fp64_update_mode() {  // GWB200_FP64_UPDATE: 1 = dmma (FP64 pipe only), 2 = ozaki (int8 emulation), 0 = tuned
+    const char* env = std::getenv("GWB200_FP64_UPDATE");
+    if (env && std::strcmp(env, "dmma") == 0) return 1;
+    if (env && std::strcmp(env, "ozaki") == 0) return 2;
+    return 0;
+}
+
+namespace {
+
 int env_update_variant() {  // GWB200_UPDATE_VARIANT forces a variant; -1 if unset or out of range
     if (const char* env = std::getenv("GWB200_UPDATE_VARIANT")) {
         const int e = std::atoi(env);
@@ -450,7 +462,7 @@ void launch_variant(int v, const TallGeometry& g, int64_t nf, double* a, int64_t
 }
 
 std::mutex g_tune_mu;
-std::map<std::array<int64_t, 4>, int> g_tuned;  // (device, n_pad, rows, nf) -> variant
+std::map<std::array<int64_t, 5>, int> g_tuned;  // (device, n_pad, rows, nf, int8 candidate) -> variant
 
 // q_out[f, j] = -qacc[f, j]  (x^T W_c x = -||L^{-1} D^1/2 x||^2).
 __global__ void k_negate_copy(const double* __restrict__ qacc, int nf, int m, int64_t ldq_in, double* __restrict__ q,
@@ -519,14 +531,17 @@ static double update_flops(const TallGeometry& g, int64_t kb0, int nk, int64_t c
     return 2.0 * (double)kt * (lower + (double)g.m * cols);
 }
 
-int tune_update_variant(const TallGeometry& g, int64_t nf, double* a, cudaStream_t s) {
+int tune_update_variant(const TallGeometry& g, int64_t nf, double* a, cudaStream_t s, void* oz,
+                        unsigned long long* sched, unsigned long long* err_pivot) {
     const int forced = env_update_variant();
     if (forced >= 0) return forced;
     const int64_t nsq = g.n_pad / kNb;
     if (nsq <= 2) return kDefaultUpdateVariant;  // no outer trailing update to tune on
+    if (oz && fp64_update_mode() == 2) return kUpdateOzaki;
+    if (fp64_update_mode() == 1) oz = nullptr;  // the FP64 pipe only
     int dev = 0;
     GWB_CUDA(cudaGetDevice(&dev));
-    const std::array<int64_t, 4> key = {dev, g.n_pad, g.rows, nf};
+    const std::array<int64_t, 5> key = {dev, g.n_pad, g.rows, nf, oz ? 1 : 0};
     std::lock_guard<std::mutex> lk(g_tune_mu);
     auto it = g_tuned.find(key);
     if (it != g_tuned.end()) return it->second;
@@ -537,7 +552,7 @@ int tune_update_variant(const TallGeometry& g, int64_t nf, double* a, cudaStream
     GWB_CUDA(cudaEventCreate(&e0));
     GWB_CUDA(cudaEventCreate(&e1));
     float best_ms = 0.f, def_ms = 0.f;
-    float times[kNumVariants] = {};
+    float times[kNumVariants + 1] = {};
     int best = kDefaultUpdateVariant;
     for (int v = 0; v < kNumVariants; ++v) {
         GWB_CUDA(cudaFuncSetAttribute(kVariants[v].fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kVariants[v].smem));
@@ -555,6 +570,22 @@ int tune_update_variant(const TallGeometry& g, int64_t nf, double* a, cudaStream
             best = v;
         }
     }
+    if (oz) {  // the int8 emulation of the outer update (kernels_oz.cu), slicing included
+        launch_update64_oz(g, nf, a, 0, 2 * kNb, oz, sched, err_pivot, s);  // warm-up
+        GWB_CUDA(cudaEventRecord(e0, s));
+        for (int r = 0; r < 2; ++r) launch_update64_oz(g, nf, a, 0, 2 * kNb, oz, sched, err_pivot, s);
+        GWB_CUDA(cudaEventRecord(e1, s));
+        GWB_CUDA(cudaEventSynchronize(e1));
+        float ms = 0.f;
+        GWB_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+        times[kUpdateOzaki] = ms;
+        if (ms < best_ms) {
+            best_ms = ms;
+            best = kUpdateOzaki;
+        }
+        // the timing left garbage exponents in the pivot word only if a wait expired: reset it
+        GWB_CUDA(cudaMemsetAsync(err_pivot, 0xFF, sizeof(unsigned long long), s));
+    }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     if (def_ms <= 1.03f * best_ms) best = kDefaultUpdateVariant;  // keep the default unless clearly beaten
@@ -563,12 +594,16 @@ int tune_update_variant(const TallGeometry& g, int64_t nf, double* a, cudaStream
         std::fprintf(stderr, "gwb200: update kernel for n_pad=%lld rows=%lld nf=%lld:", (long long)g.n_pad,
                      (long long)g.rows, (long long)nf);
         for (int v = 0; v < kNumVariants; ++v) std::fprintf(stderr, " %s %.3f ms", kVariants[v].name, times[v] / 2);
-        std::fprintf(stderr, " -> %s\n", kVariants[best].name);
+        if (oz) std::fprintf(stderr, " int8_emulation %.3f ms", times[kUpdateOzaki] / 2);
+        std::fprintf(stderr, " -> %s\n", update_variant_name(best));
     }
     return best;
 }
 
-const char* update_variant_name(int v) { return (v >= 0 && v < kNumVariants) ? kVariants[v].name : "?"; }
+const char* update_variant_name(int v) {
+    if (v == kUpdateOzaki) return "int8_emulation";
+    return (v >= 0 && v < kNumVariants) ? kVariants[v].name : "?";
+}
 
 int launch_factor_chunk(const TallGeometry& g, int64_t nf, double* a, double* linv, double* qacc,
                         unsigned long long* err_pivot, cudaStream_t s, UpdateProfiler* prof, int variant, void* oz,
@@ -576,6 +611,7 @@ int launch_factor_chunk(const TallGeometry& g, int64_t nf, double* a, double* li
     const size_t smem = 2 * 64 * kLds * sizeof(double);
     const size_t smem_potrf = 2 * kNb * (kNb + 1) * sizeof(double);
     GWB_CUDA(cudaFuncSetAttribute(k_trsm_panel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    const bool use_oz = oz && variant == kUpdateOzaki;  // outer updates emulated; look-left on DMMA
     if (variant < 0 || variant >= kNumVariants)  // untuned caller: GWB200_UPDATE_VARIANT, else the default
         variant = env_update_variant() >= 0 ? env_update_variant() : kDefaultUpdateVariant;
     const UpdateVariant& uv = kVariants[variant];
@@ -585,15 +621,18 @@ int launch_factor_chunk(const TallGeometry& g, int64_t nf, double* a, double* li
     const int64_t nrt = g.rows / kNb;    // all tile rows
     constexpr int64_t kInner = 2;        // 64-wide inner blocks per outer block
     int launches = 0;
+    // with the int8-emulated outer updates, the profiler times those alone (the look-left updates
+    // that stay on DMMA are a few percent of the flops)
+    UpdateProfiler* lprof = use_oz ? nullptr : prof;
     auto update = [&](int64_t kb0, int nk, int64_t tc0, int64_t T) {
         const int64_t L = nsq - tc0;
         const int64_t tiles = T * L - T * (T - 1) / 2 + T * (nrt - nsq);
         if (tiles <= 0) return;
         dim3 grid((unsigned)tiles, (unsigned)nf);
-        if (prof) prof->begin();
+        if (lprof) lprof->begin();
         uv.fn<<<grid, uv.threads, uv.smem, s>>>(a, g.ld, g.stride, kb0, nk, tc0, T, nsq);
         GWB_LAUNCH("k_update");
-        if (prof) prof->end((double)nf * update_flops(g, kb0, nk, tc0 * kNb, (tc0 + T) * kNb));
+        if (lprof) lprof->end((double)nf * update_flops(g, kb0, nk, tc0 * kNb, (tc0 + T) * kNb));
         ++launches;
     };
     for (int64_t ob = 0; ob < nsq; ob += kInner) {
@@ -615,7 +654,7 @@ int launch_factor_chunk(const TallGeometry& g, int64_t nf, double* a, double* li
         }
         const int64_t tc0 = ob + q;
         if (tc0 < nsq) {  // outer-block trailing update, K = 64*q (= 128 whenever columns remain)
-            if (oz && q == kInner) {
+            if (use_oz && q == kInner) {
                 if (prof) prof->begin();
                 launches += launch_update64_oz(g, nf, a, ob * kNb, tc0 * kNb, oz, sched, err_pivot, s);
                 if (prof) prof->end((double)nf * update_flops(g, ob * kNb, (int)q, tc0 * kNb, nsq * kNb));

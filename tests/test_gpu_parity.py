@@ -405,7 +405,8 @@ def test_tcgen05_update_bit_identical_to_mma_sync(backend, monkeypatch, nmo, noc
 def test_int8_emulated_fp64_update_matches_dmma(backend, monkeypatch, nmo, nocc, nst, nfreq, chunk):
     """The plain form's trailing update emulated on the int8 tensor cores (kernels_oz.cu, 7-digit
     row slices, exact int32 products) gives the screened forms of the FP64 DMMA update to 1e-12
-    relative (measured ~8e-14), deterministically."""
+    relative (measured ~8e-14), deterministically.  (Without GWB200_FP64_UPDATE the autotuner
+    picks between the two per geometry.)"""
     from minigw_b200 import generate_transformed_legendre_grid
     from minigw_b200.synthetic import make_input
 
@@ -415,6 +416,7 @@ def test_int8_emulated_fp64_update_matches_dmma(backend, monkeypatch, nmo, nocc,
     om, _ = generate_transformed_legendre_grid(nfreq)
     states = list(range(nocc - nst // 2, nocc - nst // 2 + nst))
     backend.load_system(inp)
+    monkeypatch.setenv("GWB200_FP64_UPDATE", "dmma")
     q64, st64 = backend.screened_forms(om, states)
     monkeypatch.setenv("GWB200_FP64_UPDATE", "ozaki")
     qo, sto = backend.screened_forms(om, states)
