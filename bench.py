@@ -333,7 +333,7 @@ def run_b200(args, wl):
     traffic = None
     try:  # DRAM bytes per launch of the dominant kernel from the committed ncu capture of this workload
         tr = json.loads((ROOT / "profiles" / "k_update_traffic.json").read_text())["workloads"].get(wl.name, {})
-        if "bytes_per_launch" in tr and args.precision == "fp64" and 0 <= stats[0].get("update_kernel", 0) < 6:
+        if "bytes_per_launch" in tr and args.precision == "fp64" and 0 <= be.update_kernel() < 6:
             traffic = tr["bytes_per_launch"]
     except (OSError, ValueError, KeyError):
         pass
@@ -374,7 +374,7 @@ def run_b200(args, wl):
         "gpu_launches": int(launches),
         "clocks": clock_info,
     }
-    kernel_used = stats[0].get("update_kernel", -1)
+    kernel_used = be.update_kernel()
     if args.precision == "fp64" and kernel_used == 6 and achieved:
         # the autotuner chose the int8 tensor-core emulation of the FP64 update (k_slice_panel64 +
         # k_update64_oz, timed together): bound by the FP64 C read+write, 16 bytes per updated

@@ -64,10 +64,6 @@ typedef struct gwb200_stats {
     double device_ms_update;
     int64_t update_launches;
     double flops_update;
-    /* The trailing-update kernel the screening used: 0-5 one of the FP64 DMMA variants, 6 the
-     * int8 tensor-core emulation of the FP64 update, 7 the mixed form's tcgen05 3xTF32 update, 8 the
-     * mixed form's mma.sync update, -1 none (no outer trailing update, or eta != 0). */
-    int64_t update_kernel;
 } gwb200_stats;
 
 typedef struct gwb200_handle gwb200_handle;
@@ -250,6 +246,12 @@ int gwb200_server_destroy(gwb200_server* s);
 /* Measured FP64 tensor (DMMA) throughput of this device in TFLOP/s, from a short
  * microbenchmark of mma.sync f64 (used as the roofline denominator of the plain form). */
 int gwb200_fp64_peak_tflops(gwb200_handle* h, double* tflops);
+
+/* The trailing-update kernel the last screening call on this handle used (no counterpart in the
+ * reference; for rooflines and diagnostics): 0-5 one of the FP64 DMMA variants, 6 the int8
+ * tensor-core emulation of the FP64 update, 7 the mixed form's tcgen05 3xTF32 update, 8 the mixed
+ * form's mma.sync update, -1 none (no outer trailing update, eta != 0, or no call yet). */
+int gwb200_update_kernel(gwb200_handle* h, int64_t* kernel);
 
 #ifdef __cplusplus
 }

@@ -38,6 +38,7 @@ EXPORTS = (
     "gwb200_load_system", "gwb200_run_g0w0", "gwb200_sigma_c_shard",
     "gwb200_sigma_c", "gwb200_screened_forms", "gwb200_screened_forms_complex", "gwb200_sigma_x_diag", "gwb200_qp", "gwb200_pade_sweep",
     "gwb200_grid", "gwb200_read_input_h5", "gwb200_screened_forms_noalloc", "gwb200_fp64_peak_tflops",
+    "gwb200_update_kernel",
 )
 
 
@@ -66,7 +67,6 @@ class Stats(C.Structure):
         ("device_ms_update", C.c_double),
         ("update_launches", C.c_int64),
         ("flops_update", C.c_double),
-        ("update_kernel", C.c_int64),
     ]
 
     def as_dict(self) -> dict:
@@ -123,6 +123,7 @@ def _load() -> C.CDLL:
     lib.gwb200_read_input_h5.argtypes = [C.c_char_p, _ip, _ip, _dp, _dp, _dp, _dp]
     lib.gwb200_screened_forms_noalloc.argtypes = [C.c_int64, C.c_int64, _vp, _vp, _vp, _vp, C.c_int64, _vp, _vp]
     lib.gwb200_fp64_peak_tflops.argtypes = [_vp, _dp]
+    lib.gwb200_update_kernel.argtypes = [_vp, _ip]
     for name in EXPORTS:
         if name not in ("gwb200_last_error", "gwb200_version"):
             getattr(lib, name).restype = C.c_int

@@ -124,6 +124,7 @@ struct gwb200_handle {
     int64_t mem_limit = 0;          // 0: no cap
     cudaMemPool_t pool = nullptr;   // pool for exact-size buffers (set by a server), else the default
     int64_t chunk_fc = 0;
+    int64_t last_update_kernel = -1;  // gwb200_update_kernel
 };
 
 void gwb200_attach_pool(gwb200_handle* h, cudaMemPool_t pool) { h->pool = pool; }
@@ -297,7 +298,8 @@ void compute_forms(gwb200_handle* h, const double* omega, int64_t nfreq, const i
         } else {
             if (upd_variant < 0)
                 upd_variant = tune_update_variant(g, nf, h->a.as<double>(), s, fp64_oz ? h->panel32.p : nullptr,
-                                                  h->tc_sched.as<unsigned long long>(), h->err.as<unsigned long long>());
+                                                  h->tc_sched.as<unsigned long long>(), h->err.as<unsigned long long>(),
+                                                  /*timed=*/h->mem_limit <= 0);
             launches += launch_build_tall(g, h->v.as<double>(), h->xt.as<double>(), h->dvec.as<double>(), nf,
                                           h->a.as<double>(), s);
             launches += launch_factor_chunk(g, nf, h->a.as<double>(), h->linv.as<double>(), h->qacc.as<double>(),
@@ -310,10 +312,10 @@ void compute_forms(gwb200_handle* h, const double* omega, int64_t nfreq, const i
         ++chunks;
     }
     GWB_CUDA(cudaEventRecord(h->ev[2], s));
+    h->last_update_kernel = -1;
+    if (g.n_pad / kNb > 2 && !cplx) h->last_update_kernel = mixed ? (mixed_tc ? 7 : 8) : upd_variant;
     if (st) {
         const double nd = (double)g.n, md = (double)m;
-        st->update_kernel = -1;
-        if (g.n_pad / kNb > 2 && !cplx) st->update_kernel = mixed ? (mixed_tc ? 7 : 8) : upd_variant;
         st->flops_screening = (double)nfreq * (nd * nd * nd / 3.0 + nd * nd * md + 3.0 * nd * md);
         st->frequency_chunks = chunks;
         st->kernel_launches = launches;
@@ -727,6 +729,14 @@ int gwb200_fp64_peak_tflops(gwb200_handle* h, double* tflops) {
         check_handle(h);
         if (!tflops) fail(GWB200_BAD_ARGUMENT, "null output");
         *tflops = measure_fp64_peak_tflops(h->stream);
+    });
+}
+
+int gwb200_update_kernel(gwb200_handle* h, int64_t* kernel) {
+    return guarded([&] {
+        if (!h) fail(GWB200_BAD_ARGUMENT, "null gwb200_handle");
+        if (!kernel) fail(GWB200_BAD_ARGUMENT, "null output");
+        *kernel = h->last_update_kernel;
     });
 }
 

@@ -131,15 +131,19 @@ size_t oz_slice_bytes_per_freq(const TallGeometry& g);
 int launch_update64_oz(const TallGeometry& g, int64_t nf, double* a, int64_t kb0, int64_t c_begin, void* slices,
                        unsigned long long* sched, unsigned long long* err_pivot, cudaStream_t s);
 // Autotuner of the FP64 trailing-update kernel: GWB200_UPDATE_VARIANT if set, else the fastest
-// variant on this geometry's largest trailing update, timed once per (device, n_pad, rows, nf) per
-// process in the workspace `a` (nf tall matrices) BEFORE the matrices are built there (the timing
-// overwrites it).  The default is kept unless another variant is more than 3% faster.
+// candidate on this geometry's largest trailing update, timed once per (device, n_pad, rows, nf)
+// per process in the workspace `a` (nf tall matrices) BEFORE the matrices are built there (the
+// timing overwrites it).  The default is kept unless another candidate is more than 3% faster.
 // oz != NULL adds the int8 emulation of the outer updates (kernels_oz.cu) as a candidate
 // (kUpdateOzaki), timed with the slicing; GWB200_FP64_UPDATE=dmma / =ozaki force either side.
+// Timed candidates: the default DMMA kernel and the int8 emulation (all six DMMA variants with
+// GWB200_TUNE_ALL=1).  timed == false (memory-capped handles, whose requests rarely repeat a
+// geometry): no timing, the int8 emulation iff n_pad x nf >= 48K.
 constexpr int kUpdateOzaki = 6;
 int fp64_update_mode();
 int tune_update_variant(const TallGeometry& g, int64_t nf, double* a, cudaStream_t s, void* oz = nullptr,
-                        unsigned long long* sched = nullptr, unsigned long long* err_pivot = nullptr);
+                        unsigned long long* sched = nullptr, unsigned long long* err_pivot = nullptr,
+                        bool timed = true);
 const char* update_variant_name(int v);
 // Contraction of the screened forms of nf_int integration frequencies onto nf_out output
 // frequencies (the full grid; a shard of integration frequencies gives a partial sum).

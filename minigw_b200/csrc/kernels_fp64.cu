@@ -462,7 +462,7 @@ void launch_variant(int v, const TallGeometry& g, int64_t nf, double* a, int64_t
 }
 
 std::mutex g_tune_mu;
-std::map<std::array<int64_t, 5>, int> g_tuned;  // (device, n_pad, rows, nf, int8 candidate) -> variant
+std::map<std::array<int64_t, 6>, int> g_tuned;  // (device, n_pad, rows, nf, int8 candidate, all) -> variant
 
 // q_out[f, j] = -qacc[f, j]  (x^T W_c x = -||L^{-1} D^1/2 x||^2).
 __global__ void k_negate_copy(const double* __restrict__ qacc, int nf, int m, int64_t ldq_in, double* __restrict__ q,
@@ -532,58 +532,61 @@ static double update_flops(const TallGeometry& g, int64_t kb0, int nk, int64_t c
 }
 
 int tune_update_variant(const TallGeometry& g, int64_t nf, double* a, cudaStream_t s, void* oz,
-                        unsigned long long* sched, unsigned long long* err_pivot) {
+                        unsigned long long* sched, unsigned long long* err_pivot, bool timed) {
     const int forced = env_update_variant();
     if (forced >= 0) return forced;
     const int64_t nsq = g.n_pad / kNb;
     if (nsq <= 2) return kDefaultUpdateVariant;  // no outer trailing update to tune on
     if (oz && fp64_update_mode() == 2) return kUpdateOzaki;
     if (fp64_update_mode() == 1) oz = nullptr;  // the FP64 pipe only
+    if (!timed)  // rule from the timed choices: the int8 emulation wins once n_pad x frequencies >= 48K
+        return (oz && g.n_pad * nf >= 48 * 1024) ? kUpdateOzaki : kDefaultUpdateVariant;
+    const char* all_env = std::getenv("GWB200_TUNE_ALL");
+    const bool all = all_env && all_env[0] == '1';  // every DMMA variant, not only the default
     int dev = 0;
     GWB_CUDA(cudaGetDevice(&dev));
-    const std::array<int64_t, 5> key = {dev, g.n_pad, g.rows, nf, oz ? 1 : 0};
+    const std::array<int64_t, 6> key = {dev, g.n_pad, g.rows, nf, oz ? 1 : 0, all ? 1 : 0};
     std::lock_guard<std::mutex> lk(g_tune_mu);
     auto it = g_tuned.find(key);
     if (it != g_tuned.end()) return it->second;
-    // Time every variant on the largest trailing update of this geometry (K = 128 from column 0
+    // Time the candidates on the largest trailing update of this geometry (K = 128 from column 0
     // onto columns [128, n_pad) and all RHS rows), in the workspace before the tall matrix is built
     // there: the values are irrelevant to the timing and are overwritten afterwards.
     cudaEvent_t e0, e1;
     GWB_CUDA(cudaEventCreate(&e0));
     GWB_CUDA(cudaEventCreate(&e1));
-    float best_ms = 0.f, def_ms = 0.f;
     float times[kNumVariants + 1] = {};
-    int best = kDefaultUpdateVariant;
-    for (int v = 0; v < kNumVariants; ++v) {
-        GWB_CUDA(cudaFuncSetAttribute(kVariants[v].fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kVariants[v].smem));
-        launch_variant(v, g, nf, a, 0, 2, 2, nsq - 2, s);  // warm-up
+    auto time_it = [&](auto&& launch) {
+        launch();  // warm-up
         GWB_CUDA(cudaEventRecord(e0, s));
-        for (int r = 0; r < 2; ++r) launch_variant(v, g, nf, a, 0, 2, 2, nsq - 2, s);
+        launch();
         GWB_CUDA(cudaEventRecord(e1, s));
         GWB_CUDA(cudaEventSynchronize(e1));
         float ms = 0.f;
         GWB_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+        return ms;
+    };
+    float best_ms = 0.f, def_ms = 0.f;
+    int best = -1;
+    for (int v = 0; v < kNumVariants; ++v) {
+        if (!all && v != kDefaultUpdateVariant) continue;
+        GWB_CUDA(cudaFuncSetAttribute(kVariants[v].fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kVariants[v].smem));
+        const float ms = time_it([&] { launch_variant(v, g, nf, a, 0, 2, 2, nsq - 2, s); });
         times[v] = ms;
         if (v == kDefaultUpdateVariant) def_ms = ms;
-        if (v == 0 || ms < best_ms) {
+        if (best < 0 || ms < best_ms) {
             best_ms = ms;
             best = v;
         }
     }
     if (oz) {  // the int8 emulation of the outer update (kernels_oz.cu), slicing included
-        launch_update64_oz(g, nf, a, 0, 2 * kNb, oz, sched, err_pivot, s);  // warm-up
-        GWB_CUDA(cudaEventRecord(e0, s));
-        for (int r = 0; r < 2; ++r) launch_update64_oz(g, nf, a, 0, 2 * kNb, oz, sched, err_pivot, s);
-        GWB_CUDA(cudaEventRecord(e1, s));
-        GWB_CUDA(cudaEventSynchronize(e1));
-        float ms = 0.f;
-        GWB_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+        const float ms = time_it([&] { launch_update64_oz(g, nf, a, 0, 2 * kNb, oz, sched, err_pivot, s); });
         times[kUpdateOzaki] = ms;
         if (ms < best_ms) {
             best_ms = ms;
             best = kUpdateOzaki;
         }
-        // the timing left garbage exponents in the pivot word only if a wait expired: reset it
+        // a wait that expired during the timing would have recorded pivot 0: start clean
         GWB_CUDA(cudaMemsetAsync(err_pivot, 0xFF, sizeof(unsigned long long), s));
     }
     cudaEventDestroy(e0);
@@ -593,8 +596,9 @@ int tune_update_variant(const TallGeometry& g, int64_t nf, double* a, cudaStream
     if (const char* verbose = std::getenv("GWB200_VERBOSE"); verbose && verbose[0] == '1') {
         std::fprintf(stderr, "gwb200: update kernel for n_pad=%lld rows=%lld nf=%lld:", (long long)g.n_pad,
                      (long long)g.rows, (long long)nf);
-        for (int v = 0; v < kNumVariants; ++v) std::fprintf(stderr, " %s %.3f ms", kVariants[v].name, times[v] / 2);
-        if (oz) std::fprintf(stderr, " int8_emulation %.3f ms", times[kUpdateOzaki] / 2);
+        for (int v = 0; v < kNumVariants; ++v)
+            if (all || v == kDefaultUpdateVariant) std::fprintf(stderr, " %s %.3f ms", kVariants[v].name, times[v]);
+        if (oz) std::fprintf(stderr, " int8_emulation %.3f ms", times[kUpdateOzaki]);
         std::fprintf(stderr, " -> %s\n", update_variant_name(best));
     }
     return best;

@@ -252,6 +252,12 @@ class B200Backend:
         check(lib.gwb200_fp64_peak_tflops(self._h, C.byref(v)))
         return v.value
 
+    def update_kernel(self) -> int:
+        """Trailing-update kernel of the last screening call (gwb200_update_kernel codes)."""
+        v = C.c_int64()
+        check(lib.gwb200_update_kernel(self._h, C.byref(v)))
+        return v.value
+
 
 def selected_states(nmo: int, settings: GwSettings) -> list[int]:
     """src/gw/gw.cpp:28-40 (plus the explicit list extension)."""
