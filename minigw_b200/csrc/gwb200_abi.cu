@@ -125,17 +125,29 @@ struct gwb200_handle {
     cudaMemPool_t pool = nullptr;   // pool for exact-size buffers (set by a server), else the default
     int64_t chunk_fc = 0;
     int64_t last_update_kernel = -1;  // gwb200_update_kernel
+    int persistent_ctas = 0;          // > 0: cap of the persistent kernels' grids (GPU shared by slots)
 };
 
 void gwb200_attach_pool(gwb200_handle* h, cudaMemPool_t pool) { h->pool = pool; }
+void gwb200_share_sms(gwb200_handle* h, int ways) {
+    int dev = 0, sms = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+        sms = 148;
+    h->persistent_ctas = ways > 1 ? std::max(1, sms / ways) : 0;
+}
 
 namespace {
 
-// The mixed form's outer trailing updates run on tcgen05 unless GWB200_MIXED_UPDATE=mma selects the
-// mma.sync kernel (same 3xTF32 arithmetic; kept for comparison).
-bool mixed_update_on_tcgen05() {
+// The mixed form's outer trailing updates: GWB200_MIXED_UPDATE=tc / =mma force the tcgen05 or the
+// mma.sync kernel (same 3xTF32 arithmetic); by default tcgen05, except on memory-capped handles
+// (the serving loop's slots), where the persistent tcgen05 kernel would hold every SM while the
+// other slots' requests wait: measured, the non-persistent kernels serve 90.6 requests/s against 60
+// (persistent kernels with grids shared between slots) and 41.6 (unshared).
+bool mixed_update_on_tcgen05(const gwb200_handle* h) {
     const char* env = std::getenv("GWB200_MIXED_UPDATE");
-    return !(env && std::strcmp(env, "mma") == 0);
+    if (env && std::strcmp(env, "mma") == 0) return false;
+    if (env && std::strcmp(env, "tc") == 0) return true;
+    return h->mem_limit <= 0;
 }
 
 
@@ -216,10 +228,11 @@ void compute_forms(gwb200_handle* h, const double* omega, int64_t nfreq, const i
     GWB_CUDA(cudaMemsetAsync(h->err.p, 0xFF, sizeof(unsigned long long), s));
 
     // Frequency chunk size from the HBM budget: tall matrices + scale vectors + 64x64 inverses.
-    const bool mixed_tc = mixed && mixed_update_on_tcgen05();
+    const bool mixed_tc = mixed && mixed_update_on_tcgen05(h);
     // plain form: the int8 emulation of the outer updates is a candidate of the update autotuner
-    // (its slice workspace is part of the budget) unless GWB200_FP64_UPDATE=dmma
-    const bool fp64_oz = !mixed && !cplx && fp64_update_mode() != 1;
+    // (its slice workspace is part of the budget) unless GWB200_FP64_UPDATE=dmma; memory-capped
+    // handles use it only when it is forced (GWB200_FP64_UPDATE=ozaki)
+    const bool fp64_oz = !mixed && !cplx && fp64_update_mode() != 1 && (h->mem_limit <= 0 || fp64_update_mode() == 2);
     const size_t per_freq = mixed ? sizeof(float) * ((size_t)g.stride + kNb * kNb) + sizeof(double) * (g.n_pad + g.m_pad) +
                                         (mixed_tc ? tc_panel_bytes_per_freq(g) : 0)
                                   : sizeof(double) * planes * ((size_t)g.stride + g.n_pad + kNb * kNb + g.m_pad) +
@@ -294,7 +307,7 @@ void compute_forms(gwb200_handle* h, const double* omega, int64_t nfreq, const i
             launches += launch_factor_chunk32(g, nf, h->a.as<float>(), h->linv.as<float>(), h->qacc.as<double>(),
                                               h->err.as<unsigned long long>(), s, prof.enabled ? &prof : nullptr,
                                               mixed_tc ? h->panel32.as<float>() : nullptr,
-                                              h->tc_sched.as<unsigned long long>());
+                                              h->tc_sched.as<unsigned long long>(), h->persistent_ctas);
         } else {
             if (upd_variant < 0)
                 upd_variant = tune_update_variant(g, nf, h->a.as<double>(), s, fp64_oz ? h->panel32.p : nullptr,
@@ -305,7 +318,7 @@ void compute_forms(gwb200_handle* h, const double* omega, int64_t nfreq, const i
             launches += launch_factor_chunk(g, nf, h->a.as<double>(), h->linv.as<double>(), h->qacc.as<double>(),
                                             h->err.as<unsigned long long>(), s, prof.enabled ? &prof : nullptr,
                                             upd_variant, fp64_oz ? h->panel32.p : nullptr,
-                                            h->tc_sched.as<unsigned long long>());
+                                            h->tc_sched.as<unsigned long long>(), h->persistent_ctas);
         }
         launches += launch_negate_copy(h->qacc.as<double>(), nf, m, g.m_pad, h->qall.as<double>() + f0 * g.m_pad,
                                        g.m_pad, s);

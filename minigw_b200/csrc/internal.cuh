@@ -14,6 +14,9 @@
 int gwb200_fail_status(int code, const char* message);
 // Exact-size buffers of a memory-limited handle come from `pool` (gwb200_abi.cu; used by the server).
 void gwb200_attach_pool(gwb200_handle* h, cudaMemPool_t pool);
+// A handle that shares the GPU with `ways` concurrent streams caps its persistent kernels'
+// grids at SMs / ways, so that the other streams' kernels keep running beside them.
+void gwb200_share_sms(gwb200_handle* h, int ways);
 
 namespace gwb200 {
 
@@ -124,12 +127,13 @@ int launch_build_tall(const TallGeometry& g, const double* v, const double* xt, 
 // `sched` as its work counter (look-left updates on the default DMMA kernel).
 int launch_factor_chunk(const TallGeometry& g, int64_t nf, double* a, double* linv, double* qacc,
                         unsigned long long* err_pivot, cudaStream_t s, UpdateProfiler* prof, int variant,
-                        void* oz = nullptr, unsigned long long* sched = nullptr);
+                        void* oz = nullptr, unsigned long long* sched = nullptr, int max_ctas = 0);
 // kernels_oz.cu: FP64 trailing update C -= P P^T (K = 128 from kb0, columns [c_begin, n_pad), rows
 // [c_begin, rows)) from exact int8 products of 7-digit row slices (tcgen05 kind::i8).  Two launches.
 size_t oz_slice_bytes_per_freq(const TallGeometry& g);
+// max_ctas > 0 caps the persistent grid (a handle that shares the GPU with other streams).
 int launch_update64_oz(const TallGeometry& g, int64_t nf, double* a, int64_t kb0, int64_t c_begin, void* slices,
-                       unsigned long long* sched, unsigned long long* err_pivot, cudaStream_t s);
+                       unsigned long long* sched, unsigned long long* err_pivot, cudaStream_t s, int max_ctas = 0);
 // Autotuner of the FP64 trailing-update kernel: GWB200_UPDATE_VARIANT if set, else the fastest
 // candidate on this geometry's largest trailing update, timed once per (device, n_pad, rows, nf)
 // per process in the workspace `a` (nf tall matrices) BEFORE the matrices are built there (the
@@ -137,8 +141,8 @@ int launch_update64_oz(const TallGeometry& g, int64_t nf, double* a, int64_t kb0
 // oz != NULL adds the int8 emulation of the outer updates (kernels_oz.cu) as a candidate
 // (kUpdateOzaki), timed with the slicing; GWB200_FP64_UPDATE=dmma / =ozaki force either side.
 // Timed candidates: the default DMMA kernel and the int8 emulation (all six DMMA variants with
-// GWB200_TUNE_ALL=1).  timed == false (memory-capped handles, whose requests rarely repeat a
-// geometry): no timing, the int8 emulation iff n_pad x nf >= 48K.
+// GWB200_TUNE_ALL=1).  timed == false (memory-capped handles, whose requests run side by side and
+// rarely repeat a geometry): no timing, the default DMMA kernel.
 constexpr int kUpdateOzaki = 6;
 int fp64_update_mode();
 int tune_update_variant(const TallGeometry& g, int64_t nf, double* a, cudaStream_t s, void* oz = nullptr,
@@ -171,14 +175,15 @@ int launch_build_tall32(const TallGeometry& g, const double* v, const double* xt
 // split-panel workspace (tc_panel_bytes_per_freq(g) bytes per frequency); NULL: mma.sync.
 int launch_factor_chunk32(const TallGeometry& g, int64_t nf, float* a, float* linv, double* qacc,
                           unsigned long long* err_pivot, cudaStream_t s, UpdateProfiler* prof, float* panel,
-                          unsigned long long* sched);
+                          unsigned long long* sched, int max_ctas = 0);
 // kernels_tc.cu: tcgen05 3xTF32 trailing update C -= P P^T of the mixed form (K = kdim columns from
 // kb0, output columns [c_begin, n_pad), rows [c_begin, rows)).  Two launches; `sched` is one
 // device word the kernel's work counter lives in.  A device wait that expires records pivot 0 in
 // err_pivot.
 size_t tc_panel_bytes_per_freq(const TallGeometry& g);
 int launch_update32_tc(const TallGeometry& g, int64_t nf, float* a, int64_t kb0, int kdim, int64_t c_begin,
-                       float* panel, unsigned long long* sched, unsigned long long* err_pivot, cudaStream_t s);
+                       float* panel, unsigned long long* sched, unsigned long long* err_pivot, cudaStream_t s,
+                       int max_ctas = 0);
 // kernels_c64.cu: eta != 0 (complex symmetric M = I - S V S, S = diag(Pi0)^1/2).  Planes a_re/a_im
 // of geometry g; svec 2*n_pad, linv 2*64*64, qacc 2*m_pad doubles per frequency.
 int launch_factor_chunk_c(const TallGeometry& g, int64_t nf, const double* delta, const double* omega, double eta,

@@ -290,7 +290,7 @@ int launch_build_tall32(const TallGeometry& g, const double* v, const double* xt
 
 int launch_factor_chunk32(const TallGeometry& g, int64_t nf, float* a, float* linv, double* qacc,
                           unsigned long long* err_pivot, cudaStream_t s, UpdateProfiler* prof, float* panel,
-                          unsigned long long* sched) {
+                          unsigned long long* sched, int max_ctas) {
     const size_t smem_tile = 2 * 64 * kLdf * sizeof(float);
     const size_t smem_update = 4 * 64 * kLdkf * sizeof(float);
     const size_t smem_potrf = 2 * kNb * (kNb + 1) * sizeof(double);
@@ -333,7 +333,8 @@ int launch_factor_chunk32(const TallGeometry& g, int64_t nf, float* a, float* li
         if (tc0 < nsq) {
             if (panel) {  // outer trailing update on tcgen05
                 if (prof) prof->begin();
-                launches += launch_update32_tc(g, nf, a, ob * kNb, (int)(q * kNb), tc0 * kNb, panel, sched, err_pivot, s);
+                launches += launch_update32_tc(g, nf, a, ob * kNb, (int)(q * kNb), tc0 * kNb, panel, sched, err_pivot, s,
+                                                max_ctas);
                 if (prof) prof->end((double)nf * update_flops32(g, ob * kNb, (int)q, tc0 * kNb, nsq * kNb));
             } else {
                 update(ob * kNb, (int)q, tc0, nsq - tc0);

@@ -539,8 +539,10 @@ int tune_update_variant(const TallGeometry& g, int64_t nf, double* a, cudaStream
     if (nsq <= 2) return kDefaultUpdateVariant;  // no outer trailing update to tune on
     if (oz && fp64_update_mode() == 2) return kUpdateOzaki;
     if (fp64_update_mode() == 1) oz = nullptr;  // the FP64 pipe only
-    if (!timed)  // rule from the timed choices: the int8 emulation wins once n_pad x frequencies >= 48K
-        return (oz && g.n_pad * nf >= 48 * 1024) ? kUpdateOzaki : kDefaultUpdateVariant;
+    // Untimed (memory-capped handles: the serving loop's slots, whose requests run side by side):
+    // the non-persistent DMMA kernel, which leaves SMs to the other slots' kernels (the persistent
+    // int8 kernel holds one CTA on every SM it gets); GWB200_FP64_UPDATE=ozaki still forces it.
+    if (!timed) return kDefaultUpdateVariant;
     const char* all_env = std::getenv("GWB200_TUNE_ALL");
     const bool all = all_env && all_env[0] == '1';  // every DMMA variant, not only the default
     int dev = 0;
@@ -611,7 +613,7 @@ const char* update_variant_name(int v) {
 
 int launch_factor_chunk(const TallGeometry& g, int64_t nf, double* a, double* linv, double* qacc,
                         unsigned long long* err_pivot, cudaStream_t s, UpdateProfiler* prof, int variant, void* oz,
-                        unsigned long long* sched) {
+                        unsigned long long* sched, int max_ctas) {
     const size_t smem = 2 * 64 * kLds * sizeof(double);
     const size_t smem_potrf = 2 * kNb * (kNb + 1) * sizeof(double);
     GWB_CUDA(cudaFuncSetAttribute(k_trsm_panel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -660,7 +662,7 @@ int launch_factor_chunk(const TallGeometry& g, int64_t nf, double* a, double* li
         if (tc0 < nsq) {  // outer-block trailing update, K = 64*q (= 128 whenever columns remain)
             if (use_oz && q == kInner) {
                 if (prof) prof->begin();
-                launches += launch_update64_oz(g, nf, a, ob * kNb, tc0 * kNb, oz, sched, err_pivot, s);
+                launches += launch_update64_oz(g, nf, a, ob * kNb, tc0 * kNb, oz, sched, err_pivot, s, max_ctas);
                 if (prof) prof->end((double)nf * update_flops(g, ob * kNb, (int)q, tc0 * kNb, nsq * kNb));
             } else {
                 update(ob * kNb, (int)q, tc0, nsq - tc0);

@@ -447,7 +447,7 @@ __global__ void __launch_bounds__(kOzThreads, 1)
 size_t oz_slice_bytes_per_freq(const TallGeometry& g) { return oz_freq_bytes((g.rows + kOzM - 1) / kOzM * kOzM); }
 
 int launch_update64_oz(const TallGeometry& g, int64_t nf, double* a, int64_t kb0, int64_t c_begin, void* slices,
-                       unsigned long long* sched, unsigned long long* err, cudaStream_t s) {
+                       unsigned long long* sched, unsigned long long* err, cudaStream_t s, int max_ctas) {
     const int64_t T = (g.n_pad - c_begin) / kOzN;
     if (T <= 0 || nf <= 0) return 0;
     const int64_t H = g.rows - c_begin;
@@ -466,7 +466,7 @@ int launch_update64_oz(const TallGeometry& g, int64_t nf, double* a, int64_t kb0
     GWB_CUDA(cudaMemsetAsync(sched, 0, sizeof(unsigned long long), s));
     const char* expire = std::getenv("GWB200_TEST_EXPIRE_WAIT");
     const int withhold = (expire && expire[0] == '1') ? 1 : 0;
-    const unsigned grid = (unsigned)std::min<int64_t>(us.total, sm_count());
+    const unsigned grid = (unsigned)std::min<int64_t>(us.total, max_ctas > 0 ? std::min(max_ctas, sm_count()) : sm_count());
     k_update64_oz<<<grid, kOzThreads, kOzSmem, s>>>(a, g.ld, g.stride, c_begin, g.rows, buf, rp, us, sched, err,
                                                      withhold);
     GWB_LAUNCH("k_update64_oz");

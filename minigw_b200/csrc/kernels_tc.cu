@@ -513,7 +513,7 @@ size_t tc_panel_bytes_per_freq(const TallGeometry& g) {
 }
 
 int launch_update32_tc(const TallGeometry& g, int64_t nf, float* a, int64_t kb0, int kdim, int64_t c_begin,
-                       float* panel, unsigned long long* sched, unsigned long long* err, cudaStream_t s) {
+                       float* panel, unsigned long long* sched, unsigned long long* err, cudaStream_t s, int max_ctas) {
     if (kdim <= 0 || kdim > 128 || kdim % kTcKc != 0)
         fail(GWB200_BAD_SHAPE, "tcgen05 update: K must be 32, 64, 96 or 128");
     const int64_t T = (g.n_pad - c_begin + kTcN - 1) / kTcN;  // the last column tile may be 64 wide
@@ -556,7 +556,7 @@ int launch_update32_tc(const TallGeometry& g, int64_t nf, float* a, int64_t kb0,
     us.per_f = NI * us.NS;
     us.total = nf * us.per_f;
     GWB_CUDA(cudaMemsetAsync(sched, 0, sizeof(unsigned long long), s));
-    const unsigned grid = (unsigned)std::min<int64_t>(us.total, sm_count());
+    const unsigned grid = (unsigned)std::min<int64_t>(us.total, max_ctas > 0 ? std::min(max_ctas, sm_count()) : sm_count());
     // GWB200_TEST_EXPIRE_WAIT=1 (tests only): one CTA withholds its first operand stage, so a
     // device wait expires and the call reports GWB200_DEVICE_TIMEOUT with the context intact.
     const char* expire = std::getenv("GWB200_TEST_EXPIRE_WAIT");

@@ -76,7 +76,10 @@ void worker_main(gwb200_server* s) {
     gwb200_handle* h = nullptr;
     int rc = gwb200_create(s->device, &h);
     if (rc == GWB200_OK) rc = gwb200_set_memory_limit(h, (int64_t)s->slot_budget);
-    if (rc == GWB200_OK) gwb200_attach_pool(h, s->pool);
+    if (rc == GWB200_OK) {
+        gwb200_attach_pool(h, s->pool);
+        gwb200_share_sms(h, s->slots);
+    }
     {
         std::lock_guard<std::mutex> lk(s->mu);
         if (rc != GWB200_OK && s->start_error.empty()) s->start_error = gwb200_last_error();
@@ -147,6 +150,18 @@ int gwb200_server_create(int device, int slots, int64_t hbm_budget_bytes, gwb200
         int off = 0, on = 1;
         cudaMemPoolSetAttribute(s->pool, cudaMemPoolReuseAllowInternalDependencies, &off);
         cudaMemPoolSetAttribute(s->pool, cudaMemPoolReuseAllowOpportunistic, &on);
+        // Map the whole budget now (one allocation, freed at once; the release threshold keeps it
+        // in the pool): growing the pool while requests run stalled every slot for about a second
+        // whenever a new peak of concurrent use was reached.  Best effort: on failure the pool
+        // grows on demand as before.
+        cudaStream_t st = nullptr;
+        if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) == cudaSuccess) {
+            void* p = nullptr;
+            if (cudaMallocFromPoolAsync(&p, (size_t)hbm_budget_bytes, s->pool, st) == cudaSuccess) cudaFreeAsync(p, st);
+            cudaStreamSynchronize(st);
+            cudaStreamDestroy(st);
+        }
+        cudaGetLastError();
     }
     for (int i = 0; i < slots; ++i) s->workers.emplace_back(worker_main, s);
     {
