@@ -426,6 +426,31 @@ def test_int8_emulated_fp64_update_matches_dmma(backend, monkeypatch, nmo, nocc,
     np.testing.assert_array_equal(qo, qo2)
 
 
+def test_update_kernel_reports_the_choice(backend, monkeypatch):
+    """gwb200_update_kernel names the trailing-update kernel of the last screening call: a DMMA
+    variant (0-5), the int8 emulation (6), the mixed form's tcgen05 (7) or mma.sync (8) update, or
+    -1 when there is no outer trailing update."""
+    from minigw_b200 import generate_transformed_legendre_grid
+    from minigw_b200.synthetic import make_input
+
+    om, _ = generate_transformed_legendre_grid(4)
+    backend.load_system(make_input(14, 4, seed=1))  # n = 40: one 64-block, no trailing update
+    backend.screened_forms(om, [3, 4])
+    assert backend.update_kernel() == -1
+    backend.load_system(make_input(40, 10, seed=3))  # n = 300: trailing updates
+    monkeypatch.setenv("GWB200_FP64_UPDATE", "dmma")
+    backend.screened_forms(om, [9, 10])
+    assert 0 <= backend.update_kernel() <= 5
+    monkeypatch.setenv("GWB200_FP64_UPDATE", "ozaki")
+    backend.screened_forms(om, [9, 10])
+    assert backend.update_kernel() == 6
+    backend.screened_forms(om, [9, 10], precision="mixed")
+    assert backend.update_kernel() == 7
+    monkeypatch.setenv("GWB200_MIXED_UPDATE", "mma")
+    backend.screened_forms(om, [9, 10], precision="mixed")
+    assert backend.update_kernel() == 8
+
+
 def test_int8_emulated_update_expired_wait(backend, monkeypatch):
     """The int8 update's bounded waits: a withheld operand stage ends in GWB200_DEVICE_TIMEOUT and
     the context stays usable."""
