@@ -23,14 +23,16 @@
 //   k_update64_oz    persistent, warp-specialised, one CTA per SM (10 warps, 222 KB of shared
 //                    memory, 448 TMEM columns):
 //                      warp 0     producer: units from a global counter handed on through a
-//                                 4-slot mbarrier ring; loads the unit's 7 A slices (128 rows,
-//                                 112 KB, resident for the unit) and streams the B slices (64
-//                                 rows, 8 KB each) through a 5-stage ring;
+//                                 4-slot mbarrier ring; loads the unit's A slices 3-7 (128 rows,
+//                                 80 KB, resident for the unit) and streams the B slices (64
+//                                 rows, 8 KB each) through a 9-stage ring;
 //                      warp 1     TMEM allocation; lane 0 issues tcgen05.mma kind::i8 (M = 128,
-//                                 N = 64, K = 32 per instruction, both operands from shared
-//                                 memory) into 7 int32 accumulators, one per level l (columns
-//                                 64 (l - 2));
-//                      warps 2-9  epilogue: warp w reads lane quadrant w % 4, 32 columns (all 7
+//                                 N = 64, K = 32 per instruction; A slices 1-2, which take part
+//                                 in 13 of the 28 products, from TMEM (columns 448-511), the
+//                                 others and B from shared memory) into 7 int32 accumulators,
+//                                 one per level l (columns 64 (l - 2));
+//                      warps 2-9  epilogue: at each unit start, write A slices 1-2 into TMEM;
+//                                 per tile, warp w reads lane quadrant w % 4, 32 columns (all 7
 //                                 levels of 16 columns per tcgen05.wait::ld), releases the
 //                                 accumulators, combines the levels, scales by 2^{e_r + e_c},
 //                                 stages -value per row (256 bytes) and adds it to C with a bulk
@@ -53,25 +55,28 @@ constexpr int kOzM = 128;                    // accumulator rows = TMEM lanes
 constexpr int kOzN = 64;                     // accumulator columns per level
 constexpr int kOzSlices = 7;                 // digit slices per value
 constexpr int kOzSeg = 32;                   // column tiles per work unit
-constexpr int kOzStages = 5;                 // B ring depth (one slice per stage)
+constexpr int kOzStages = 9;                 // B ring depth (one slice per stage)
+constexpr int kOzTmemSlices = 2;             // A slices 1-2 (13 of the 28 products) read from TMEM
 constexpr int kSchedSlots = 4;
 constexpr int kSliceA = kOzM * 128;          // one slice of 128 rows: 16 KB
 constexpr int kSliceB = kOzN * 128;          // of 64 rows: 8 KB
 constexpr int kEpiWarps = 8;                 // 4 lane quadrants x 2 column halves of 32
 constexpr int kOzThreads = 32 * (2 + kEpiWarps);
-constexpr int kTmemCols = 512;               // 7 levels x 64 columns used
+constexpr int kTmemCols = 512;               // 7 levels x 64 columns, then A slices 1-2 (32 each)
+constexpr int kTmemA = kOzSlices * kOzN;     // first column of the A slices held in TMEM
 constexpr int kStgRow = 256 + 16;            // staging row stride: 32 doubles + 16 bytes (banks)
 constexpr int kStgBytes = 32 * kStgRow;      // per epilogue warp
 constexpr int kHeader = 1024;
-constexpr int kOzSmem = kHeader + 1024 + kOzSlices * kSliceA + kOzStages * kSliceB + kEpiWarps * kStgBytes;
+constexpr int kOzSmem = kHeader + 1024 + (kOzSlices - kOzTmemSlices) * kSliceA + kOzStages * kSliceB + kEpiWarps * kStgBytes;
 
 constexpr int kOffFull = 0;
 constexpr int kOffEmpty = kOffFull + 8 * kOzStages;
 constexpr int kOffTFull = kOffEmpty + 8 * kOzStages;    // accumulators ready (tcgen05.commit)
 constexpr int kOffTEmpty = kOffTFull + 8;               // accumulators drained (kEpiWarps arrivals)
-constexpr int kOffAFull = kOffTEmpty + 8;               // A slices of the unit loaded (tx bytes)
+constexpr int kOffAFull = kOffTEmpty + 8;               // A slices 3-7 of the unit in smem (tx bytes)
 constexpr int kOffAEmpty = kOffAFull + 8;               // MMAs of the unit complete
-constexpr int kOffDrain = kOffAEmpty + 8;
+constexpr int kOffATmem = kOffAEmpty + 8;               // A slices 1-2 in TMEM (kEpiWarps arrivals)
+constexpr int kOffDrain = kOffATmem + 8;
 constexpr int kOffUFull = kOffDrain + 8;
 constexpr int kOffUEmpty = kOffUFull + 8 * kSchedSlots;
 constexpr int kOffUnit = kOffUEmpty + 8 * kSchedSlots;
@@ -91,6 +96,26 @@ __device__ __forceinline__ void mma_i8(uint32_t tmem_d, uint64_t da, uint64_t db
         "setp.ne.b32 p, %4, 0;\n\t"
         "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
         "l"(da), "l"(db), "r"(kIdescI8), "r"(accumulate)
+        : "memory");
+}
+
+// A from TMEM (lane = row, 4 consecutive K bytes per 32-bit column), B from shared memory.
+__device__ __forceinline__ void mma_i8_ts(uint32_t tmem_d, uint32_t tmem_a, uint64_t db, uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::i8 [%0], [%1], %2, %3, p;\n\t}" ::"r"(tmem_d),
+        "r"(tmem_a), "l"(db), "r"(kIdescI8), "r"(accumulate)
+        : "memory");
+}
+__device__ __forceinline__ void tmem_st32u(uint32_t taddr, const uint32_t (&v)[32]) {
+    asm volatile(
+        "tcgen05.st.sync.aligned.32x32b.x32.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16,"
+        "%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31,%32};" ::"r"(taddr),
+        "r"(v[0]), "r"(v[1]), "r"(v[2]), "r"(v[3]), "r"(v[4]), "r"(v[5]), "r"(v[6]), "r"(v[7]), "r"(v[8]), "r"(v[9]),
+        "r"(v[10]), "r"(v[11]), "r"(v[12]), "r"(v[13]), "r"(v[14]), "r"(v[15]), "r"(v[16]), "r"(v[17]), "r"(v[18]),
+        "r"(v[19]), "r"(v[20]), "r"(v[21]), "r"(v[22]), "r"(v[23]), "r"(v[24]), "r"(v[25]), "r"(v[26]), "r"(v[27]),
+        "r"(v[28]), "r"(v[29]), "r"(v[30]), "r"(v[31])
         : "memory");
 }
 
@@ -169,7 +194,7 @@ __global__ void __launch_bounds__(kOzThreads, 1)
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const uint32_t base = smem_u32(osm);
     const uint32_t abuf = (base + kHeader + 1023u) & ~1023u;  // 7 A slices, 1024-aligned
-    const uint32_t ring = abuf + kOzSlices * kSliceA;          // B stages
+    const uint32_t ring = abuf + (kOzSlices - kOzTmemSlices) * kSliceA;  // B stages (A slices 3-7 before)
     const uint32_t stg0 = ring + kOzStages * kSliceB;          // epilogue staging rows
     volatile uint32_t* abort_flag = reinterpret_cast<volatile uint32_t*>(osm + kOffAbort);
     volatile int64_t* uslot = reinterpret_cast<volatile int64_t*>(osm + kOffUnit);
@@ -179,6 +204,7 @@ __global__ void __launch_bounds__(kOzThreads, 1)
     auto uempty = [&](int j) { return base + kOffUEmpty + 8 * j; };
     const uint32_t tfull = base + kOffTFull, tempty = base + kOffTEmpty;
     const uint32_t afull = base + kOffAFull, aempty = base + kOffAEmpty, drain = base + kOffDrain;
+    const uint32_t atmem = base + kOffATmem;
 
     if (threadIdx.x == 0) {
         for (int s = 0; s < kOzStages; ++s) {
@@ -192,6 +218,7 @@ __global__ void __launch_bounds__(kOzThreads, 1)
         mbar_init(tfull, 1);
         mbar_init(tempty, kEpiWarps);
         mbar_init(afull, 1);
+        mbar_init(atmem, kEpiWarps);
         mbar_init(aempty, 1);
         mbar_init(drain, 1);
         *abort_flag = 0u;
@@ -246,10 +273,11 @@ __global__ void __launch_bounds__(kOzThreads, 1)
             if (lane == 0) got = mbar_wait(aempty, aph ^ 1u, abort_flag, err) ? 1u : 0u;
             got = __shfl_sync(0xffffffffu, got, 0);
             if (!got) break;
-            if (lane == 0) mbar_expect_tx(afull, (uint32_t)(kOzSlices * kSliceA));
+            if (lane == 0) mbar_expect_tx(afull, (uint32_t)((kOzSlices - kOzTmemSlices) * kSliceA));
             __syncwarp();
-            if (lane < kOzSlices)  // one 16 KB copy per slice
-                bulk_g2s(abuf + lane * kSliceA, slices + ((size_t)lane * rp + i * kOzM) * 128, kSliceA, afull);
+            if (lane < kOzSlices - kOzTmemSlices)  // one 16 KB copy per smem slice (slices 3-7)
+                bulk_g2s(abuf + lane * kSliceA, slices + ((size_t)(lane + kOzTmemSlices) * rp + i * kOzM) * 128, kSliceA,
+                         afull);
             a_filled = true;
             aph ^= 1u;
             bool ok = true;
@@ -303,6 +331,8 @@ __global__ void __launch_bounds__(kOzThreads, 1)
             int64_t i, c0, c1;
             decode_unit(us, u, f, i, c0, c1);
             if (!mbar_wait(afull, aph, abort_flag, err)) break;
+            if (!mbar_wait(atmem, aph, abort_flag, err)) break;
+            tc_fence_after();
             aph ^= 1u;
             for (int64_t c = c0; ok && c < c1; ++c) {
                 if (!mbar_wait(tempty, acc_ph ^ 1u, abort_flag, err)) {
@@ -325,9 +355,14 @@ __global__ void __launch_bounds__(kOzThreads, 1)
                         if (sa < kOzSlices - t) {
                             const uint32_t d = tmem + (uint32_t)((sa + t) * kOzN);  // level sa + t + 2
 #pragma unroll
-                            for (int kk = 0; kk < 4; ++kk)
-                                mma_i8(d, desc_a0 + (uint64_t)((sa * kSliceA + 32 * kk) >> 4), db0 + (uint64_t)(2 * kk),
-                                       (t > 0 || kk > 0) ? 1u : 0u);
+                            for (int kk = 0; kk < 4; ++kk) {
+                                if (sa < kOzTmemSlices)  // A slice from TMEM: 32 bytes of K = 8 columns
+                                    mma_i8_ts(d, tmem + (uint32_t)(kTmemA + 32 * sa + 8 * kk), db0 + (uint64_t)(2 * kk),
+                                              (t > 0 || kk > 0) ? 1u : 0u);
+                                else
+                                    mma_i8(d, desc_a0 + (uint64_t)(((sa - kOzTmemSlices) * kSliceA + 32 * kk) >> 4),
+                                           db0 + (uint64_t)(2 * kk), (t > 0 || kk > 0) ? 1u : 0u);
+                            }
                         }
                     }
                     mma_commit(empty(s));
@@ -353,7 +388,7 @@ __global__ void __launch_bounds__(kOzThreads, 1)
         const int q = warp & 3, half = (warp - 2) >> 2;
         const uint32_t stg = stg0 + (uint32_t)(warp - 2) * kStgBytes + (uint32_t)lane * kStgRow;
         int js = 0;
-        uint32_t acc_ph = 0, jph = 0;
+        uint32_t acc_ph = 0, jph = 0, aph = 0;
         bool ok = true, reduced = false;
         while (ok) {
             int64_t u = 0;
@@ -370,6 +405,30 @@ __global__ void __launch_bounds__(kOzThreads, 1)
             const uint8_t* slices = buf + (size_t)f * fbytes;
             const int32_t* exps = reinterpret_cast<const int32_t*>(slices + (size_t)kOzSlices * rp * 128);
             const int64_t rr = i * kOzM + q * 32 + lane;  // panel row of this lane
+            {   // A slices 1-2 of the unit into TMEM (warp half h writes slice h + 1 of its lane
+                // quadrant) once the previous unit's MMAs are done with them
+                uint32_t got = 1;
+                if (lane == 0) got = mbar_wait(aempty, aph ^ 1u, abort_flag, err) ? 1u : 0u;
+                got = __shfl_sync(0xffffffffu, got, 0);
+                if (!got) break;
+                aph ^= 1u;
+                tc_fence_after();
+                const uint4* row = reinterpret_cast<const uint4*>(slices + ((size_t)half * rp + rr) * 128);
+                uint32_t w[32];
+#pragma unroll
+                for (int c = 0; c < 8; ++c) {  // undo the 128-byte swizzle of the slice row
+                    const uint4 x = row[c ^ (int)(rr & 7)];
+                    w[4 * c] = x.x;
+                    w[4 * c + 1] = x.y;
+                    w[4 * c + 2] = x.z;
+                    w[4 * c + 3] = x.w;
+                }
+                tmem_st32u(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(kTmemA + 32 * half), w);
+                asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+                tc_fence_before();
+                __syncwarp();
+                if (lane == 0) mbar_arrive(atmem);
+            }
             const int64_t r = c_begin + rr;
             const int er = exps[rr];
             for (int64_t c = c0; c < c1; ++c) {
