@@ -42,7 +42,8 @@ def parse_args():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
     ap.add_argument("--workload", choices=sorted(WORKLOAD_TEXT), default="cfg3")
-    ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64")
+    ap.add_argument("--precision", choices=["fp64", "mixed"], default=None,
+                    help="default: fp64 for the single-molecule workloads, mixed for --batch")
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-pairs", type=int, default=0, help="reference (f_n, f') pairs per CPU sample (0 = auto)")
@@ -51,6 +52,11 @@ def parse_args():
                          "continuous-batching server at swept rates; reports p50/p99 latency and solves/s")
     ap.add_argument("--requests", type=int, default=24, help="requests per serving rate")
     ap.add_argument("--slots", type=int, default=4, help="concurrent server slots (serving mode)")
+    ap.add_argument("--batch", action="store_true",
+                    help="uneven molecule batch (config 4): --molecules molecules with nmo uniform in 20..160, "
+                         "nocc=round(nmo/6), 64 freq, 12 Pade, HOMO and LUMO, solved by gwb200_run_g0w0_batch "
+                         "(shared launches, autotuned buckets) and by one gwb200_run_g0w0 per molecule")
+    ap.add_argument("--molecules", type=int, default=64, help="molecules per batch (--batch)")
     ap.add_argument("--split-frequencies", action="store_true",
                     help="N>1: split one solve's integration frequencies over the ranks (strong scaling; one "
                          "NCCL all-reduce of the partial Sigma_c per solve) instead of one replica per rank")
@@ -516,10 +522,111 @@ def run_serving(args):
     return 0
 
 
+def run_batch(args):
+    """Config 4: `--molecules` synthetic molecules (seeded) with nmo uniform in 20..160, nocc =
+    round(nmo/6), 64 frequencies, 12 Pade parameters, HOMO and LUMO.  A step solves every molecule
+    (Sigma_c(iw), Pade, QP; results read back to the host): once through gwb200_run_g0w0_batch
+    (buckets of molecules factored by shared launches; plan timed on the first call) and once as
+    one gwb200_run_g0w0 per molecule, both on the same stream with the ERIs resident (loaded once,
+    as a serving process keeps them)."""
+    import numpy as np
+    import torch
+
+    from minigw_b200 import B200Backend, run_g0w0_batch
+    from minigw_b200.synthetic import make_input_on_device
+
+    prec = args.precision or "mixed"
+    nfreq, npade = 64, 12
+    rng = np.random.default_rng(args.seed)
+    nmos = [int(x) for x in rng.integers(20, 161, size=args.molecules)]
+    torch.cuda.set_device(0)
+    stream = torch.cuda.Stream(device=0)
+    bes, states, shapes = [], [], []
+    for i, nmo in enumerate(nmos):
+        nocc = max(1, int(round(nmo / 6)))
+        inp = make_input_on_device(nmo, nocc, seed=args.seed + 2000 + i, device=0, pin=False)
+        be = B200Backend(0)
+        be.set_stream(stream.cuda_stream)
+        be.load_system(inp)
+        del inp
+        bes.append(be)
+        states.append([nocc - 1, nocc])
+        shapes.append((nmo, nocc, nocc * (nmo - nocc)))
+    torch.cuda.empty_cache()
+
+    def per_molecule():
+        return [be.run_g0w0(nfreq, npade, st, precision=prec) for be, st in zip(bes, states)]
+
+    def batched():
+        return run_g0w0_batch(bes, nfreq, npade, states, precision=prec)
+
+    def timed(fn):
+        for _ in range(max(3, args.warmup)):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        out = []
+        e0.record(stream)
+        for _ in range(args.steps):
+            out.append(fn())
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / args.steps, out
+
+    ms_each, outs_each = timed(per_molecule)
+    clocks = ClockSampler(0)
+    clocks.start()
+    time.sleep(1.5)
+    ms_batch, outs_batch = timed(batched)
+    clock_info = clocks.stop()
+    last = outs_batch[-1]
+    same = all(np.array_equal(a["sigma"], s) for a, s in zip(outs_each[-1], last["sigma"]))
+    flops_true = last["stats"]["flops_screening"]
+    launches_batch = last["stats"]["kernel_launches"]
+    launches_each = sum(r["stats"]["kernel_launches"] for r in outs_each[-1])
+    h2d = 16 * nfreq + 8 * sum(len(s) for s in states)
+    d2h = sum(16 * nmo * nfreq + 8 * nmo for nmo in nmos) + 8
+    result = {
+        "metric": "gw_solves_per_s", "value": args.molecules * 1e3 / ms_batch, "unit": "GW solves/s", "n_gpus": 1,
+        "steps": args.steps, "warmup": max(3, args.warmup), "ms_per_step": ms_batch, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64" if prec == "fp64" else "f32 (3xTF32) + f64",
+        "data": f"synthetic (seeded generator, seed {args.seed}; GEMM of the ERI on the GPU)",
+        "config": {"workload": f"cfg4: uneven molecule batch of {args.molecules}, nmo uniform 20..160, "
+                               "nocc=round(nmo/6), 64 freq, 12 Pade, HOMO and LUMO",
+                   "precision": prec, "nmo": nmos, "nph_min": min(s[2] for s in shapes),
+                   "nph_max": max(s[2] for s in shapes), "buckets": last["buckets"],
+                   "l2": "inputs larger than L2 (the batched eps(iw) matrices of a step total tens of GB)"},
+        "per_molecule_launches": {"value": args.molecules * 1e3 / ms_each, "unit": "GW solves/s",
+                                  "ms_per_step": ms_each, "gpu_launches": int(launches_each)},
+        "speedup_vs_per_molecule": ms_each / ms_batch,
+        "bit_identical_to_per_molecule": bool(same),
+        "screening": {"device_ms": last["stats"]["device_ms_screening"], "flops_true": flops_true,
+                      "tflops_true": flops_true / (last["stats"]["device_ms_screening"] * 1e-3) / 1e12},
+        "e2e": {"value": args.molecules * 1e3 / ms_batch, "unit": "GW solves/s", "h2d_bytes_per_step": int(h2d),
+                "d2h_bytes_per_step": int(d2h),
+                "note": "the batch call as a user makes it: grid, state lists and group tables uploaded, Sigma_c "
+                        "and QP energies read back every step; the ERIs stay resident"},
+        "gpu_launches": int(launches_batch),
+        "clocks": clock_info,
+    }
+    if prec == "mixed":  # error of the mixed batch against the FP64 batch (untimed)
+        ref = run_g0w0_batch(bes, nfreq, npade, states, precision="fp64")
+        dqp = max(float(np.abs(q32[st] - q64[st]).max()) for q32, q64, st in zip(last["qp"], ref["qp"], states))
+        rel = max(float(np.abs(a - b).max() / np.abs(b).max()) for a, b in zip(last["sigma"], ref["sigma"]))
+        result["mixed_vs_fp64"] = {"sigma_c_max_rel_err": rel, "qp_max_abs_err_meV": dqp * 27.211386245988e3}
+    for be in bes:
+        be.close()
+    print(json.dumps(result))
+    return 0
+
+
 def main() -> int:
     args = parse_args()
     if args.serving:
         return run_serving(args)
+    if args.batch:
+        return run_batch(args)
+    args.precision = args.precision or "fp64"
     from minigw_b200.synthetic import WORKLOADS
 
     wl = WORKLOADS[args.workload]

@@ -243,6 +243,32 @@ int gwb200_server_wait(gwb200_server* s, int64_t ticket, int* status, double* qu
 /* Finish every queued request, stop the workers, release their handles. */
 int gwb200_server_destroy(gwb200_server* s);
 
+/* ---- Batched solves: many molecules of uneven size in shared launches (no reference counterpart;
+ * the reference runs one molecule per process, src/main.cpp:68-103) ----
+ * systems[i] holds molecule i (gwb200_load_system), all on one device, no handle twice.  Every
+ * molecule is solved as gwb200_run_g0w0(systems[i], nfreq, npade, states[i], nstates[i], 0, precision,
+ * ...) would solve it, eta = 0.  The molecules are sorted by size and grouped into buckets; a
+ * bucket's matrices (every member x every frequency) take the bucket's largest geometry (identity /
+ * zero padding, exact) and are factored by one launch sequence.  Bucket boundaries: a cost model
+ * (block-step latency against padded work) gives candidate plans, timed on the first call of a batch
+ * signature (sorted sizes, nfreq, precision); the fastest is kept for later calls in the process
+ * (GWB200_BATCH_PLAN=model|each|single skips the timing).  All work runs on systems[0]'s stream
+ * with systems[0]'s workspaces.  Outputs (either array, or any entry, may be NULL): sigma_out[i]
+ * nmo_i x nfreq complex row-major, qp_out[i] nmo_i (NaN where not requested).  *nbuckets_out: the
+ * buckets used.  stats: totals of the call (flops at the true sizes, device times, launches). */
+int gwb200_run_g0w0_batch(gwb200_handle* const* systems, int64_t nsys, int64_t nfreq, int64_t npade,
+                          const int64_t* const* states, const int64_t* nstates, int precision,
+                          double* const* sigma_out, double* const* qp_out, int64_t* nbuckets_out,
+                          gwb200_stats* stats);
+
+/* The cost model's bucket plan alone (host only, no device): bucket_of[i] in 0..*nbuckets-1 for
+ * molecules of nph[i] x ncols[i] (buckets in ascending size), budget_bytes of device memory for the
+ * batched matrices, step_us / tflops the model's block-step latency and padded-work rate
+ * (<= 0: the defaults). */
+int gwb200_plan_buckets(int64_t nsys, const int64_t* nph, const int64_t* ncols, int64_t nfreq, int precision,
+                        int64_t budget_bytes, double step_us, double tflops, int64_t* bucket_of,
+                        int64_t* nbuckets);
+
 /* Measured FP64 tensor (DMMA) throughput of this device in TFLOP/s, from a short
  * microbenchmark of mma.sync f64 (used as the roofline denominator of the plain form). */
 int gwb200_fp64_peak_tflops(gwb200_handle* h, double* tflops);

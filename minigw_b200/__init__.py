@@ -17,13 +17,16 @@ from .gw import (
     output_final_energy_table,
     output_self_energy_after_pade,
     output_self_energy_before_pade,
+    plan_buckets,
     read_gw_input_hdf5,
     run_g0w0,
+    run_g0w0_batch,
     selected_states,
 )
 
 __all__ = [
     "FP64", "MIXED", "STATUS", "GwB200Error", "version", "B200Backend", "B200Server", "GwInput", "GwResult", "GwSettings",
     "GwTimings", "generate_transformed_legendre_grid", "output_final_energy_table", "output_self_energy_after_pade",
-    "output_self_energy_before_pade", "read_gw_input_hdf5", "run_g0w0", "selected_states",
+    "output_self_energy_before_pade", "plan_buckets", "read_gw_input_hdf5", "run_g0w0", "run_g0w0_batch",
+    "selected_states",
 ]

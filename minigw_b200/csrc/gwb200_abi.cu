@@ -7,7 +7,10 @@
 #include <cstdlib>
 #include <cstring>
 #include <limits>
+#include <map>
+#include <mutex>
 #include <new>
+#include <numeric>
 #include <string>
 #include <vector>
 
@@ -118,6 +121,7 @@ struct gwb200_handle {
     DevBuf panel32;   // operand workspace of the tcgen05 trailing updates (mixed: FP32 hi/lo split;
                       // plain with GWB200_FP64_UPDATE=ozaki: int8 digit slices + exponents)
     DevBuf tc_sched;  // work counter of the tcgen05 update kernel
+    DevBuf batch_desc;  // BatchGroup tables of gwb200_run_g0w0_batch (when this handle leads a batch)
     PinnedBuf stage_in, stage_out;
     // cached frequency-chunk size for a repeated geometry (avoids cudaMemGetInfo per call)
     int64_t chunk_key[5] = {-1, -1, -1, -1, -1};
@@ -394,6 +398,130 @@ void qp_on_device(gwb200_handle* h, int64_t nfreq, int64_t npade, int64_t nstate
               h->qp_scratch.p, s);
 }
 
+// ---- many molecules in shared launches (gwb200_run_g0w0_batch; kernels in kernels_batch.cu) ----
+
+// Batch work runs on the lead handle's stream; the members' own streams come back on exit.
+struct StreamSwap {
+    std::vector<gwb200_handle*> hs;
+    std::vector<cudaStream_t> saved;
+    ~StreamSwap() {
+        for (size_t i = 0; i < hs.size(); ++i) hs[i]->stream = saved[i];
+    }
+};
+
+// One launch sequence of a bucket: `nmat` matrices of geometry g, described by groups
+// [group0, group0 + ngroups) of the device table.
+struct BatchChunk {
+    TallGeometry g;
+    int64_t nmat, group0, ngroups;
+};
+
+// Chunks of one bucket plan (bucket sizes over `order`, the molecules sorted by size), at most
+// `budget` bytes of batched matrices at once; appends the groups (device pointers of each member).
+std::vector<BatchChunk> batch_chunks(const std::vector<gwb200_handle*>& hs, const std::vector<int64_t>& ms,
+                                     const std::vector<int>& order, const std::vector<int64_t>& sizes, int64_t nfreq,
+                                     bool mixed, bool oz, size_t budget, std::vector<BatchGroup>& groups) {
+    std::vector<BatchChunk> chunks;
+    size_t pos = 0;
+    for (int64_t bsz : sizes) {
+        int64_t nmax = 0, mmax = 0;
+        for (int64_t t = 0; t < bsz; ++t) {
+            const int i = order[pos + (size_t)t];
+            nmax = std::max(nmax, hs[(size_t)i]->n);
+            mmax = std::max(mmax, ms[(size_t)i]);
+        }
+        const TallGeometry g = make_geometry(nmax, mmax);
+        const int64_t fit = std::max<int64_t>(1, (int64_t)(budget / batch_bytes_per_matrix(g, mixed, oz)));
+        BatchChunk cur{g, 0, (int64_t)groups.size(), 0};
+        for (int64_t t = 0; t < bsz; ++t) {
+            const int i = order[pos + (size_t)t];
+            gwb200_handle* h = hs[(size_t)i];
+            const TallGeometry gi = make_geometry(h->n, ms[(size_t)i]);
+            for (int64_t f0 = 0; f0 < nfreq;) {
+                if (cur.nmat == fit) {
+                    chunks.push_back(cur);
+                    cur = BatchChunk{g, 0, (int64_t)groups.size(), 0};
+                }
+                const int64_t nf = std::min(nfreq - f0, fit - cur.nmat);
+                BatchGroup gr{};
+                gr.v = h->v.as<double>();
+                gr.xt = h->xt.as<double>();
+                gr.dvec = h->dvec.as<double>() + f0 * gi.n_pad;
+                gr.q_out = h->qall.as<double>() + f0 * gi.m_pad;
+                gr.n = h->n;
+                gr.m = ms[(size_t)i];
+                gr.n_pad = gi.n_pad;
+                gr.ldq_out = gi.m_pad;
+                gr.mat0 = cur.nmat;
+                gr.nf = nf;
+                groups.push_back(gr);
+                ++cur.ngroups;
+                cur.nmat += nf;
+                f0 += nf;
+            }
+        }
+        if (cur.nmat > 0) chunks.push_back(cur);
+        pos += (size_t)bsz;
+    }
+    return chunks;
+}
+
+// Workspace bytes of a set of chunks: the largest tall matrices, inverses, accumulators, operands.
+struct BatchNeed {
+    size_t a = 0, linv = 0, qacc = 0, panel = 0;
+    size_t total() const { return a + linv + qacc + panel; }
+};
+void batch_need(const std::vector<BatchChunk>& chunks, bool mixed, bool oz, BatchNeed& need) {
+    const size_t el = mixed ? sizeof(float) : sizeof(double);
+    for (const BatchChunk& c : chunks) {
+        const size_t nm = (size_t)c.nmat;
+        need.a = std::max(need.a, el * nm * (size_t)c.g.stride);
+        need.linv = std::max(need.linv, el * nm * kNb * kNb);
+        need.qacc = std::max(need.qacc, sizeof(double) * nm * (size_t)c.g.m_pad);
+        const size_t op = mixed ? tc_panel_bytes_per_freq(c.g) : (oz ? oz_slice_bytes_per_freq(c.g) : 0);
+        need.panel = std::max(need.panel, op * nm);
+    }
+}
+
+// The screening of one plan on the lead handle's stream (build, factor, forms per chunk).
+int64_t batch_screen(gwb200_handle* w, const std::vector<BatchChunk>& chunks, const BatchGroup* dgroups,
+                     const std::vector<int>& variants, bool mixed, bool mixed_tc, bool oz) {
+    cudaStream_t s = w->stream;
+    int64_t launches = 0;
+    for (size_t k = 0; k < chunks.size(); ++k) {
+        const BatchChunk& c = chunks[k];
+        const BatchGroup* gp = dgroups + c.group0;
+        GWB_CUDA(cudaMemsetAsync(w->qacc.p, 0, sizeof(double) * (size_t)c.nmat * c.g.m_pad, s));
+        launches += launch_build_tall_batch(c.g, gp, c.ngroups, mixed, w->a.p, s);
+        if (mixed)
+            launches += launch_factor_chunk32(c.g, c.nmat, w->a.as<float>(), w->linv.as<float>(), w->qacc.as<double>(),
+                                              w->err.as<unsigned long long>(), s, nullptr,
+                                              mixed_tc ? w->panel32.as<float>() : nullptr,
+                                              w->tc_sched.as<unsigned long long>(), w->persistent_ctas);
+        else
+            launches += launch_factor_chunk(c.g, c.nmat, w->a.as<double>(), w->linv.as<double>(), w->qacc.as<double>(),
+                                            w->err.as<unsigned long long>(), s, nullptr, variants[k],
+                                            oz ? w->panel32.p : nullptr, w->tc_sched.as<unsigned long long>(),
+                                            w->persistent_ctas);
+        launches += launch_forms_scatter(gp, c.ngroups, w->qacc.as<double>(), c.g.m_pad, s);
+    }
+    return launches;
+}
+
+// Latency of one 64-wide block step and the sustained rate of the padded work, the cost model's
+// defaults (measured on config-4-like batches; GWB200_BATCH_STEP_US / GWB200_BATCH_TFLOPS override).
+double batch_step_us(bool mixed) {
+    if (const char* e = std::getenv("GWB200_BATCH_STEP_US")) return std::max(0.0, std::atof(e));
+    return mixed ? 60.0 : 80.0;
+}
+double batch_tflops(bool mixed) {
+    if (const char* e = std::getenv("GWB200_BATCH_TFLOPS")) return std::max(1e-3, std::atof(e));
+    return mixed ? 90.0 : 40.0;
+}
+
+std::mutex g_batch_mu;
+std::map<std::vector<int64_t>, std::vector<int64_t>> g_batch_plans;  // batch signature -> bucket sizes
+
 } // namespace
 
 extern "C" {
@@ -438,7 +566,7 @@ int gwb200_destroy(gwb200_handle* h) {
     h->stage_out.release();
     for (DevBuf* b : {&h->pqo, &h->xdiag, &h->mo, &h->vxc_diag, &h->delta, &h->v, &h->sigx, &h->flag, &h->xt, &h->dvec, &h->a,
                       &h->linv, &h->qacc, &h->qall, &h->sigma, &h->omega, &h->weight, &h->states, &h->err, &h->qp,
-                      &h->qp_scratch, &h->omega_out, &h->panel32, &h->tc_sched})
+                      &h->qp_scratch, &h->omega_out, &h->panel32, &h->tc_sched, &h->batch_desc})
         b->release();
     for (auto& e : h->ev)
         if (e) cudaEventDestroy(e);
@@ -742,6 +870,295 @@ int gwb200_fp64_peak_tflops(gwb200_handle* h, double* tflops) {
         check_handle(h);
         if (!tflops) fail(GWB200_BAD_ARGUMENT, "null output");
         *tflops = measure_fp64_peak_tflops(h->stream);
+    });
+}
+
+namespace {
+// Molecule order of a batch: ascending (n, m), ties by position.
+std::vector<int> batch_order(const std::vector<int64_t>& ns, const std::vector<int64_t>& ms) {
+    std::vector<int> order(ns.size());
+    std::iota(order.begin(), order.end(), 0);
+    std::sort(order.begin(), order.end(), [&](int x, int y) {
+        if (ns[(size_t)x] != ns[(size_t)y]) return ns[(size_t)x] < ns[(size_t)y];
+        if (ms[(size_t)x] != ms[(size_t)y]) return ms[(size_t)x] < ms[(size_t)y];
+        return x < y;
+    });
+    return order;
+}
+} // namespace
+
+int gwb200_plan_buckets(int64_t nsys, const int64_t* nph, const int64_t* ncols, int64_t nfreq, int precision,
+                        int64_t budget_bytes, double step_us, double tflops, int64_t* bucket_of, int64_t* nbuckets) {
+    return guarded([&] {
+        if (nsys <= 0 || !nph || !ncols || !bucket_of || !nbuckets) fail(GWB200_BAD_ARGUMENT, "empty or null batch");
+        if (nfreq <= 0 || budget_bytes <= 0) fail(GWB200_BAD_SHAPE, "nfreq and the budget must be positive");
+        if (precision != GWB200_FP64 && precision != GWB200_MIXED) fail(GWB200_BAD_ARGUMENT, "unknown precision");
+        const bool mixed = precision == GWB200_MIXED;
+        std::vector<int64_t> ns(nph, nph + nsys), ms(ncols, ncols + nsys);
+        for (int64_t i = 0; i < nsys; ++i)
+            if (ns[(size_t)i] <= 0 || ms[(size_t)i] <= 0) fail(GWB200_BAD_SHAPE, "nph and ncols must be positive");
+        const std::vector<int> order = batch_order(ns, ms);
+        std::vector<int64_t> n_sorted, m_sorted;
+        for (int i : order) {
+            n_sorted.push_back(ns[(size_t)i]);
+            m_sorted.push_back(ms[(size_t)i]);
+        }
+        const std::vector<int64_t> sizes =
+            plan_buckets(n_sorted, m_sorted, nfreq, mixed, (size_t)budget_bytes, step_us > 0 ? step_us : batch_step_us(mixed),
+                         tflops > 0 ? tflops : batch_tflops(mixed));
+        size_t pos = 0;
+        for (size_t b = 0; b < sizes.size(); ++b)
+            for (int64_t t = 0; t < sizes[b]; ++t) bucket_of[order[pos++]] = (int64_t)b;
+        *nbuckets = (int64_t)sizes.size();
+    });
+}
+
+int gwb200_run_g0w0_batch(gwb200_handle* const* systems, int64_t nsys, int64_t nfreq, int64_t npade,
+                          const int64_t* const* states, const int64_t* nstates, int precision, double* const* sigma_out,
+                          double* const* qp_out, int64_t* nbuckets_out, gwb200_stats* stats) {
+    return guarded([&] {
+        if (!systems || nsys <= 0) fail(GWB200_BAD_ARGUMENT, "empty batch");
+        if (!states || !nstates) fail(GWB200_BAD_ARGUMENT, "null state lists");
+        if (nfreq <= 0) fail(GWB200_BAD_SHAPE, "--freq-points must be positive");
+        if (npade <= 0) fail(GWB200_BAD_SHAPE, "--pade-params must be positive");
+        if (precision != GWB200_FP64 && precision != GWB200_MIXED) fail(GWB200_BAD_ARGUMENT, "unknown precision");
+        std::vector<gwb200_handle*> hs(systems, systems + nsys);
+        for (gwb200_handle* h : hs)
+            if (!h) fail(GWB200_BAD_ARGUMENT, "null handle in the batch");
+        gwb200_handle* w = hs[0];
+        check_system(w);
+        {
+            std::vector<gwb200_handle*> uniq(hs);
+            std::sort(uniq.begin(), uniq.end());
+            if (std::adjacent_find(uniq.begin(), uniq.end()) != uniq.end())
+                fail(GWB200_BAD_ARGUMENT, "a handle appears twice in the batch");
+        }
+        std::vector<int64_t> ns((size_t)nsys), ms((size_t)nsys);
+        for (int64_t i = 0; i < nsys; ++i) {
+            gwb200_handle* h = hs[(size_t)i];
+            if (!h->loaded) fail(GWB200_NO_SYSTEM, "no system loaded: call gwb200_load_system first");
+            if (h->device != w->device) fail(GWB200_BAD_ARGUMENT, "the systems of a batch must share one device");
+            check_states(h, states[i], nstates[i]);
+            if (h->bad_gap)
+                fail(GWB200_NONPOSITIVE_GAP, "some e_a - e_i <= 0: chi0(iw) is not negative definite, eps(iw) is not SPD");
+            ns[(size_t)i] = h->n;
+            ms[(size_t)i] = nstates[i] * h->nmo;
+        }
+        const bool mixed = precision == GWB200_MIXED;
+        const bool mixed_tc = mixed && mixed_update_on_tcgen05(w);
+        const bool oz = !mixed && fp64_update_mode() != 1 && (w->mem_limit <= 0 || fp64_update_mode() == 2);
+        gwb200_stats local{};
+        gwb200_stats* st = stats ? stats : &local;
+        *st = gwb200_stats{};
+        for (gwb200_handle* h : hs)
+            if (h->stream != w->stream) GWB_CUDA(cudaStreamSynchronize(h->stream));
+        StreamSwap swap;
+        swap.hs = hs;
+        for (gwb200_handle* h : hs) swap.saved.push_back(h->stream);
+        for (gwb200_handle* h : hs) h->stream = w->stream;
+        cudaStream_t s = w->stream;
+
+        // members' own buffers first (they are not part of the batched-matrix budget)
+        const size_t nb_om = sizeof(double) * nfreq;
+        size_t nb_states = 0;
+        for (int64_t i = 0; i < nsys; ++i) {
+            gwb200_handle* h = hs[(size_t)i];
+            const TallGeometry gi = make_geometry(h->n, ms[(size_t)i]);
+            h->omega.ensure(nb_om);
+            h->weight.ensure(nb_om);
+            h->states.ensure(sizeof(int64_t) * nstates[i]);
+            size_buffer(h, h->xt, sizeof(double) * (size_t)ms[(size_t)i] * h->n);
+            size_buffer(h, h->dvec, sizeof(double) * (size_t)nfreq * gi.n_pad);
+            size_buffer(h, h->qall, sizeof(double) * (size_t)nfreq * gi.m_pad);
+            h->complex_forms = false;
+            nb_states += sizeof(int64_t) * nstates[i];
+        }
+        w->err.ensure(sizeof(unsigned long long));
+        w->tc_sched.ensure(sizeof(unsigned long long));
+        w->chunk_key[0] = -1;  // the lead handle's workspaces are resized below
+
+        // plans: cached per batch signature, else timed candidates (GWB200_BATCH_PLAN=tuned, the
+        // default), the cost model alone (=model), one bucket per molecule (=each), one bucket (=single)
+        const std::vector<int> order = batch_order(ns, ms);
+        std::vector<int64_t> n_sorted, m_sorted;
+        for (int i : order) {
+            n_sorted.push_back(ns[(size_t)i]);
+            m_sorted.push_back(ms[(size_t)i]);
+        }
+        size_t free_b = 0, total_b = 0;
+        GWB_CUDA(cudaMemGetInfo(&free_b, &total_b));
+        const size_t avail = free_b + w->a.bytes + w->linv.bytes + w->qacc.bytes + w->panel32.bytes;
+        const char* mode_env = std::getenv("GWB200_BATCH_PLAN");
+        const std::string mode = mode_env ? mode_env : "tuned";
+        std::vector<int64_t> key = {(int64_t)w->device, (int64_t)precision, (int64_t)oz, (int64_t)mixed_tc, nfreq};
+        key.insert(key.end(), n_sorted.begin(), n_sorted.end());
+        key.insert(key.end(), m_sorted.begin(), m_sorted.end());
+        std::vector<std::vector<int64_t>> cands;
+        bool cached = false;
+        if (mode == "each") {
+            cands.push_back(std::vector<int64_t>((size_t)nsys, 1));
+        } else if (mode == "single") {
+            cands.push_back({nsys});
+        } else {
+            if (mode == "tuned") {
+                std::lock_guard<std::mutex> lk(g_batch_mu);
+                auto it = g_batch_plans.find(key);
+                if (it != g_batch_plans.end()) {
+                    cands.push_back(it->second);
+                    cached = true;
+                }
+            }
+            if (!cached) {
+                const double tau = batch_step_us(mixed), rate = batch_tflops(mixed);
+                const size_t b0 = (size_t)(0.85 * (double)avail);
+                for (double mult : (mode == "tuned" ? std::vector<double>{1.0, 0.25, 4.0} : std::vector<double>{1.0})) {
+                    std::vector<int64_t> p = plan_buckets(n_sorted, m_sorted, nfreq, mixed, b0, tau * mult, rate);
+                    if (std::find(cands.begin(), cands.end(), p) == cands.end()) cands.push_back(p);
+                }
+                if (mode == "tuned") {
+                    std::vector<int64_t> each((size_t)nsys, 1);
+                    if (std::find(cands.begin(), cands.end(), each) == cands.end()) cands.push_back(each);
+                }
+            }
+        }
+        // chunks of every candidate inside one budget (all candidates share the workspaces)
+        const TallGeometry gmax = make_geometry(n_sorted.back(), *std::max_element(m_sorted.begin(), m_sorted.end()));
+        if (batch_bytes_per_matrix(gmax, mixed, oz) > avail)
+            fail(GWB200_OOM, "not enough device memory for one frequency of the largest eps(iw) in the batch");
+        size_t budget = (size_t)(0.85 * (double)avail);
+        std::vector<std::vector<BatchChunk>> chunks;
+        std::vector<BatchGroup> groups;
+        BatchNeed need;
+        for (int attempt = 0;; ++attempt) {
+            chunks.clear();
+            groups.clear();
+            need = BatchNeed{};
+            for (const auto& p : cands) {
+                chunks.push_back(batch_chunks(hs, ms, order, p, nfreq, mixed, oz, budget, groups));
+                batch_need(chunks.back(), mixed, oz, need);
+            }
+            if (need.total() <= (size_t)(0.9 * (double)avail) || attempt >= 12) break;
+            budget = (size_t)(0.7 * (double)budget);
+        }
+        size_buffer(w, w->a, need.a);
+        size_buffer(w, w->linv, need.linv);
+        size_buffer(w, w->qacc, need.qacc);
+        if (need.panel) size_buffer(w, w->panel32, need.panel);
+        w->batch_desc.ensure(sizeof(BatchGroup) * groups.size());
+        // FP64: the update kernel of each chunk geometry (timed before anything is built: the
+        // autotuner overwrites the workspace)
+        std::vector<std::vector<int>> variants(cands.size());
+        for (size_t c = 0; c < cands.size(); ++c)
+            for (const BatchChunk& ch : chunks[c])
+                variants[c].push_back(mixed ? -1
+                                            : tune_update_variant(ch.g, ch.nmat, w->a.as<double>(), s,
+                                                                  oz ? w->panel32.p : nullptr,
+                                                                  w->tc_sched.as<unsigned long long>(),
+                                                                  w->err.as<unsigned long long>(), w->mem_limit <= 0));
+
+        // uploads through the lead handle's pinned staging buffer: grid, state lists, group tables
+        std::vector<double> omega((size_t)nfreq), weight((size_t)nfreq);
+        transformed_legendre_grid(nfreq, omega.data(), weight.data());
+        const size_t nb_groups = sizeof(BatchGroup) * groups.size();
+        w->stage_in.ensure(2 * nb_om + nb_states + nb_groups);
+        char* sp = w->stage_in.as<char>();
+        std::memcpy(sp, omega.data(), nb_om);
+        std::memcpy(sp + nb_om, weight.data(), nb_om);
+        std::memcpy(sp + 2 * nb_om + nb_states, groups.data(), nb_groups);
+        GWB_CUDA(cudaMemcpyAsync(w->batch_desc.p, sp + 2 * nb_om + nb_states, nb_groups, cudaMemcpyHostToDevice, s));
+        GWB_CUDA(cudaMemsetAsync(w->err.p, 0xFF, sizeof(unsigned long long), s));
+        GWB_CUDA(cudaEventRecord(w->ev[0], s));
+        int64_t launches = 0;
+        size_t off = 2 * nb_om;
+        for (int64_t i = 0; i < nsys; ++i) {
+            gwb200_handle* h = hs[(size_t)i];
+            const size_t nb_st = sizeof(int64_t) * nstates[i];
+            std::memcpy(sp + off, states[i], nb_st);
+            GWB_CUDA(cudaMemcpyAsync(h->omega.p, sp, nb_om, cudaMemcpyHostToDevice, s));
+            GWB_CUDA(cudaMemcpyAsync(h->weight.p, sp + nb_om, nb_om, cudaMemcpyHostToDevice, s));
+            GWB_CUDA(cudaMemcpyAsync(h->states.p, sp + off, nb_st, cudaMemcpyHostToDevice, s));
+            off += nb_st;
+            launches += launch_gather_panel(h->pqo.as<double>(), h->nmo, h->nocc, h->states.as<int64_t>(), nstates[i],
+                                            h->xt.as<double>(), s);
+            launches += launch_scale_vectors(h->delta.as<double>(), h->n, make_geometry(h->n, ms[(size_t)i]).n_pad,
+                                             h->omega.as<double>(), nfreq, h->dvec.as<double>(), s);
+        }
+        GWB_CUDA(cudaEventRecord(w->ev[1], s));
+        const BatchGroup* dgroups = w->batch_desc.as<BatchGroup>();
+        size_t pick = 0;
+        if (cands.size() > 1) {  // time each candidate plan once, keep the fastest for this signature
+            float best = std::numeric_limits<float>::infinity();
+            for (size_t c = 0; c < cands.size(); ++c) {
+                GWB_CUDA(cudaEventRecord(w->ev[4], s));
+                batch_screen(w, chunks[c], dgroups, variants[c], mixed, mixed_tc, oz);
+                GWB_CUDA(cudaEventRecord(w->ev[5], s));
+                GWB_CUDA(cudaEventSynchronize(w->ev[5]));
+                const float t = elapsed(w->ev[4], w->ev[5]);
+                if (t < best) {
+                    best = t;
+                    pick = c;
+                }
+            }
+            std::lock_guard<std::mutex> lk(g_batch_mu);
+            g_batch_plans[key] = cands[pick];
+        }
+        GWB_CUDA(cudaEventRecord(w->ev[4], s));
+        launches += batch_screen(w, chunks[pick], dgroups, variants[pick], mixed, mixed_tc, oz);
+        GWB_CUDA(cudaEventRecord(w->ev[2], s));
+        st->kernel_launches = launches;
+        for (int64_t i = 0; i < nsys; ++i) {
+            contract_on_device(hs[(size_t)i], nfreq, nstates[i], st);
+            qp_on_device(hs[(size_t)i], nfreq, npade, nstates[i]);
+            st->kernel_launches += 2;
+        }
+        GWB_CUDA(cudaEventRecord(w->ev[3], s));
+        // results and the pivot word back in one synchronisation
+        size_t nb_out = sizeof(unsigned long long);
+        for (gwb200_handle* h : hs) nb_out += sizeof(double) * (2 * (size_t)h->nmo * nfreq + h->nmo);
+        w->stage_out.ensure(nb_out);
+        char* op = w->stage_out.as<char>();
+        GWB_CUDA(cudaMemcpyAsync(op, w->err.p, sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
+        size_t o = sizeof(unsigned long long);
+        for (gwb200_handle* h : hs) {
+            const size_t nb_sig = sizeof(double) * 2 * (size_t)h->nmo * nfreq, nb_qp = sizeof(double) * h->nmo;
+            GWB_CUDA(cudaMemcpyAsync(op + o, h->sigma.p, nb_sig, cudaMemcpyDeviceToHost, s));
+            GWB_CUDA(cudaMemcpyAsync(op + o + nb_sig, h->qp.p, nb_qp, cudaMemcpyDeviceToHost, s));
+            o += nb_sig + nb_qp;
+        }
+        GWB_CUDA(cudaStreamSynchronize(s));
+        unsigned long long piv = 0;
+        std::memcpy(&piv, op, sizeof(piv));
+        if (piv == 0) fail(GWB200_DEVICE_TIMEOUT, "a device-side wait of the tcgen05 update expired; results discarded");
+        if (piv != std::numeric_limits<unsigned long long>::max()) {
+            st->info = (int64_t)piv;
+            fail(GWB200_NOT_SPD, "eps(iw) of a batch member is not positive definite: Cholesky pivot " +
+                                     std::to_string(piv) + " <= 0");
+        }
+        o = sizeof(unsigned long long);
+        for (int64_t i = 0; i < nsys; ++i) {
+            const gwb200_handle* h = hs[(size_t)i];
+            const size_t nb_sig = sizeof(double) * 2 * (size_t)h->nmo * nfreq, nb_qp = sizeof(double) * h->nmo;
+            if (sigma_out && sigma_out[i]) std::memcpy(sigma_out[i], op + o, nb_sig);
+            if (qp_out && qp_out[i]) std::memcpy(qp_out[i], op + o + nb_sig, nb_qp);
+            o += nb_sig + nb_qp;
+        }
+        double flops = 0.0;
+        int64_t nmax = 0, mmax = 0;
+        for (int64_t i = 0; i < nsys; ++i) {
+            const double nd = (double)ns[(size_t)i], md = (double)ms[(size_t)i];
+            flops += (double)nfreq * (nd * nd * nd / 3.0 + nd * nd * md + 3.0 * nd * md);
+            nmax = std::max(nmax, ns[(size_t)i]);
+            mmax = std::max(mmax, ms[(size_t)i]);
+        }
+        st->flops_screening = flops;
+        st->frequency_chunks = (int64_t)chunks[pick].size();
+        st->nph = nmax;
+        st->ncols = mmax;
+        st->device_ms_gather = elapsed(w->ev[0], w->ev[1]);
+        st->device_ms_screening = elapsed(w->ev[4], w->ev[2]);
+        st->device_ms_contract = elapsed(w->ev[2], w->ev[3]);
+        st->device_ms_total = elapsed(w->ev[0], w->ev[3]);
+        if (nbuckets_out) *nbuckets_out = (int64_t)cands[pick].size();
     });
 }
 

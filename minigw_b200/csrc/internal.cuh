@@ -195,6 +195,25 @@ int launch_sigma_contract_c(const double* qall, int64_t nf_int, int64_t nstates,
                             const int64_t* states, const double* mo, double fermi, const double* omega_int,
                             const double* weight_int, const double* omega_out, int64_t nf_out, double* sigma,
                             cudaStream_t s);
+// kernels_batch.cu: one molecule's run of consecutive matrices in a batched chunk (device table).
+struct BatchGroup {
+    const double* v;     // V_ph, n x n
+    const double* xt;    // (D-independent) panel rows, m x n
+    const double* dvec;  // scale vectors of the group's first frequency, then one per frequency (n_pad apart)
+    double* q_out;       // forms of the group's first frequency, ldq_out apart
+    int64_t n, m, n_pad, ldq_out;
+    int64_t mat0, nf;    // first matrix of the chunk this group fills, and how many (frequencies)
+};
+int launch_build_tall_batch(const TallGeometry& g, const BatchGroup* groups, int64_t ngroups, bool fp32, void* a,
+                            cudaStream_t s);
+int launch_forms_scatter(const BatchGroup* groups, int64_t ngroups, const double* qacc, int64_t ldq, cudaStream_t s);
+// device bytes of one batched matrix (tall matrix, 64x64 inverse, scale vector, norm accumulators,
+// tcgen05 / int8 operand workspace)
+size_t batch_bytes_per_matrix(const TallGeometry& g, bool mixed, bool fp64_oz);
+// bucket sizes over the molecules sorted by (n, m): minimises block-step latency + padded work
+std::vector<int64_t> plan_buckets(const std::vector<int64_t>& n_sorted, const std::vector<int64_t>& m_sorted,
+                                  int64_t nfreq, bool mixed, size_t budget, double step_us, double tflops);
+
 // noalloc.cu
 size_t noalloc_scratch_bytes();
 void screened_forms_noalloc(int64_t n, int64_t m, const double* d_v, const double* d_xt, const double* d_delta,

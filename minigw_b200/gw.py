@@ -23,7 +23,7 @@ from typing import Optional, Sequence
 import ctypes as C
 import numpy as np
 
-from ._lib import FP64, MIXED, GwB200Error, Request, Stats, check, dptr, iptr, lib
+from ._lib import FP64, MIXED, GwB200Error, Request, Stats, _dp, _ip, check, dptr, iptr, lib
 
 HARTREE_TO_EV = 27.211386245988  # include/types.hpp:12
 
@@ -257,6 +257,41 @@ class B200Backend:
         v = C.c_int64()
         check(lib.gwb200_update_kernel(self._h, C.byref(v)))
         return v.value
+
+
+def run_g0w0_batch(backends: list[B200Backend], nfreq: int, npade: int, states: list, precision="mixed"):
+    """Solve every loaded backend's molecule (eta = 0) through shared launches (gwb200_run_g0w0_batch).
+
+    Work runs on backends[0]'s stream and workspaces.  Returns per-molecule Sigma_c(iw) and QP
+    energies, the number of buckets the molecules were grouped into, and the call's stats."""
+    n = len(backends)
+    hs = (C.c_void_p * n)(*[b._h for b in backends])
+    st_arrays = [np.ascontiguousarray(s, dtype=np.int64) for s in states]
+    if len(st_arrays) != n:
+        raise GwB200Error(7, "one state list per molecule is required")
+    st_ptrs = (_ip * n)(*[iptr(a) for a in st_arrays])
+    nst = np.array([a.shape[0] for a in st_arrays], dtype=np.int64)
+    sig = [np.zeros((b.nmo, nfreq), dtype=np.complex128) for b in backends]
+    qp = [np.zeros(b.nmo) for b in backends]
+    sig_ptrs = (_dp * n)(*[dptr(a) for a in sig])
+    qp_ptrs = (_dp * n)(*[dptr(a) for a in qp])
+    nb = C.c_int64()
+    stats = Stats()
+    check(lib.gwb200_run_g0w0_batch(hs, n, int(nfreq), int(npade), st_ptrs, iptr(nst), _precision_code(precision),
+                                    sig_ptrs, qp_ptrs, C.byref(nb), C.byref(stats)))
+    return {"sigma": sig, "qp": qp, "buckets": nb.value, "stats": stats.as_dict()}
+
+
+def plan_buckets(nph, ncols, nfreq: int, precision="mixed", budget_bytes: int = 64 << 30, step_us: float = 0.0,
+                 tflops: float = 0.0) -> tuple[np.ndarray, int]:
+    """Bucket index of every molecule under the batch cost model (host only)."""
+    n = np.ascontiguousarray(nph, dtype=np.int64)
+    m = np.ascontiguousarray(ncols, dtype=np.int64)
+    out = np.zeros(n.shape[0], dtype=np.int64)
+    nb = C.c_int64()
+    check(lib.gwb200_plan_buckets(n.shape[0], iptr(n), iptr(m), int(nfreq), _precision_code(precision),
+                                  int(budget_bytes), float(step_us), float(tflops), iptr(out), C.byref(nb)))
+    return out, nb.value
 
 
 def selected_states(nmo: int, settings: GwSettings) -> list[int]:
