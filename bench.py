@@ -595,6 +595,7 @@ def run_batch(args):
                                "nocc=round(nmo/6), 64 freq, 12 Pade, HOMO and LUMO",
                    "precision": prec, "nmo": nmos, "nph_min": min(s[2] for s in shapes),
                    "nph_max": max(s[2] for s in shapes), "buckets": last["buckets"],
+                   "streams": int(os.environ.get("GWB200_BATCH_STREAMS", "4")),
                    "l2": "inputs larger than L2 (the batched eps(iw) matrices of a step total tens of GB)"},
         "per_molecule_launches": {"value": args.molecules * 1e3 / ms_each, "unit": "GW solves/s",
                                   "ms_per_step": ms_each, "gpu_launches": int(launches_each)},

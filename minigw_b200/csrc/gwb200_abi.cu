@@ -79,6 +79,16 @@ struct PinnedBuf {
     }
 };
 
+// One stream of a batched solve (gwb200_run_g0w0_batch) with its own workspaces; lane 0 runs on
+// the lead handle's stream.
+struct BatchLane {
+    cudaStream_t stream = nullptr;  // lanes >= 1 (created on first use)
+    cudaEvent_t done = nullptr;
+    DevBuf a, linv, qacc, panel, sched;
+    size_t bytes() const { return a.bytes + linv.bytes + qacc.bytes + panel.bytes; }
+};
+constexpr int kMaxBatchLanes = 4;
+
 template <class F>
 int guarded(F&& body) {
     try {
@@ -122,6 +132,8 @@ struct gwb200_handle {
                       // plain with GWB200_FP64_UPDATE=ozaki: int8 digit slices + exponents)
     DevBuf tc_sched;  // work counter of the tcgen05 update kernel
     DevBuf batch_desc;  // BatchGroup tables of gwb200_run_g0w0_batch (when this handle leads a batch)
+    BatchLane lanes[kMaxBatchLanes];  // streams + workspaces of the batches this handle leads
+    cudaEvent_t batch_fork = nullptr;
     PinnedBuf stage_in, stage_out;
     // cached frequency-chunk size for a repeated geometry (avoids cudaMemGetInfo per call)
     int64_t chunk_key[5] = {-1, -1, -1, -1, -1};
@@ -417,10 +429,11 @@ struct BatchChunk {
 };
 
 // Chunks of one bucket plan (bucket sizes over `order`, the molecules sorted by size), at most
-// `budget` bytes of batched matrices at once; appends the groups (device pointers of each member).
+// `budget` bytes (and, if cap > 0, cap matrices) at once; appends the groups (device pointers of
+// each member).
 std::vector<BatchChunk> batch_chunks(const std::vector<gwb200_handle*>& hs, const std::vector<int64_t>& ms,
                                      const std::vector<int>& order, const std::vector<int64_t>& sizes, int64_t nfreq,
-                                     bool mixed, bool oz, size_t budget, std::vector<BatchGroup>& groups) {
+                                     bool mixed, bool oz, size_t budget, int64_t cap, std::vector<BatchGroup>& groups) {
     std::vector<BatchChunk> chunks;
     size_t pos = 0;
     for (int64_t bsz : sizes) {
@@ -431,7 +444,8 @@ std::vector<BatchChunk> batch_chunks(const std::vector<gwb200_handle*>& hs, cons
             mmax = std::max(mmax, ms[(size_t)i]);
         }
         const TallGeometry g = make_geometry(nmax, mmax);
-        const int64_t fit = std::max<int64_t>(1, (int64_t)(budget / batch_bytes_per_matrix(g, mixed, oz)));
+        int64_t fit = std::max<int64_t>(1, (int64_t)(budget / batch_bytes_per_matrix(g, mixed, oz)));
+        if (cap > 0) fit = std::min(fit, cap);
         BatchChunk cur{g, 0, (int64_t)groups.size(), 0};
         for (int64_t t = 0; t < bsz; ++t) {
             const int i = order[pos + (size_t)t];
@@ -483,29 +497,50 @@ void batch_need(const std::vector<BatchChunk>& chunks, bool mixed, bool oz, Batc
     }
 }
 
-// The screening of one plan on the lead handle's stream (build, factor, forms per chunk).
-int64_t batch_screen(gwb200_handle* w, const std::vector<BatchChunk>& chunks, const BatchGroup* dgroups,
+// The chunks `idx` of a plan on one lane (build, factor, forms per chunk), on stream `s`.
+int64_t batch_screen(gwb200_handle* w, BatchLane& lane, cudaStream_t s, int max_ctas,
+                     const std::vector<BatchChunk>& chunks, const std::vector<size_t>& idx, const BatchGroup* dgroups,
                      const std::vector<int>& variants, bool mixed, bool mixed_tc, bool oz) {
-    cudaStream_t s = w->stream;
     int64_t launches = 0;
-    for (size_t k = 0; k < chunks.size(); ++k) {
+    unsigned long long* err = w->err.as<unsigned long long>();
+    unsigned long long* sched = lane.sched.as<unsigned long long>();
+    for (size_t k : idx) {
         const BatchChunk& c = chunks[k];
         const BatchGroup* gp = dgroups + c.group0;
-        GWB_CUDA(cudaMemsetAsync(w->qacc.p, 0, sizeof(double) * (size_t)c.nmat * c.g.m_pad, s));
-        launches += launch_build_tall_batch(c.g, gp, c.ngroups, mixed, w->a.p, s);
+        GWB_CUDA(cudaMemsetAsync(lane.qacc.p, 0, sizeof(double) * (size_t)c.nmat * c.g.m_pad, s));
+        launches += launch_build_tall_batch(c.g, gp, c.ngroups, mixed, lane.a.p, s);
         if (mixed)
-            launches += launch_factor_chunk32(c.g, c.nmat, w->a.as<float>(), w->linv.as<float>(), w->qacc.as<double>(),
-                                              w->err.as<unsigned long long>(), s, nullptr,
-                                              mixed_tc ? w->panel32.as<float>() : nullptr,
-                                              w->tc_sched.as<unsigned long long>(), w->persistent_ctas);
+            launches += launch_factor_chunk32(c.g, c.nmat, lane.a.as<float>(), lane.linv.as<float>(),
+                                              lane.qacc.as<double>(), err, s, nullptr,
+                                              mixed_tc ? lane.panel.as<float>() : nullptr, sched, max_ctas);
         else
-            launches += launch_factor_chunk(c.g, c.nmat, w->a.as<double>(), w->linv.as<double>(), w->qacc.as<double>(),
-                                            w->err.as<unsigned long long>(), s, nullptr, variants[k],
-                                            oz ? w->panel32.p : nullptr, w->tc_sched.as<unsigned long long>(),
-                                            w->persistent_ctas);
-        launches += launch_forms_scatter(gp, c.ngroups, w->qacc.as<double>(), c.g.m_pad, s);
+            launches += launch_factor_chunk(c.g, c.nmat, lane.a.as<double>(), lane.linv.as<double>(),
+                                            lane.qacc.as<double>(), err, s, nullptr, variants[k],
+                                            oz ? lane.panel.p : nullptr, sched, max_ctas);
+        launches += launch_forms_scatter(gp, c.ngroups, lane.qacc.as<double>(), c.g.m_pad, s);
     }
     return launches;
+}
+
+// Chunks to lanes: longest modelled time first, each to the least loaded lane.
+std::vector<std::vector<size_t>> batch_assign(const std::vector<BatchChunk>& chunks, int lanes, double step_us,
+                                              double tflops) {
+    std::vector<std::pair<double, size_t>> cost;
+    for (size_t k = 0; k < chunks.size(); ++k) {
+        const double N = (double)chunks[k].g.n_pad, M = (double)chunks[k].g.m_pad;
+        cost.push_back({(N / kNb) * step_us * 1e-6 + (double)chunks[k].nmat * (N * N * N / 3.0 + N * N * M) / (tflops * 1e12),
+                        k});
+    }
+    std::stable_sort(cost.begin(), cost.end(), [](const auto& x, const auto& y) { return x.first > y.first; });
+    std::vector<std::vector<size_t>> out((size_t)lanes);
+    std::vector<double> load((size_t)lanes, 0.0);
+    for (const auto& [c, k] : cost) {
+        const size_t l = (size_t)(std::min_element(load.begin(), load.end()) - load.begin());
+        out[l].push_back(k);
+        load[l] += c;
+    }
+    for (auto& v : out) std::sort(v.begin(), v.end());
+    return out;
 }
 
 // Latency of one 64-wide block step and the sustained rate of the padded work, the cost model's
@@ -568,6 +603,13 @@ int gwb200_destroy(gwb200_handle* h) {
                       &h->linv, &h->qacc, &h->qall, &h->sigma, &h->omega, &h->weight, &h->states, &h->err, &h->qp,
                       &h->qp_scratch, &h->omega_out, &h->panel32, &h->tc_sched, &h->batch_desc})
         b->release();
+    for (BatchLane& l : h->lanes) {
+        if (l.stream) cudaStreamSynchronize(l.stream);
+        for (DevBuf* b : {&l.a, &l.linv, &l.qacc, &l.panel, &l.sched}) b->release();
+        if (l.done) cudaEventDestroy(l.done);
+        if (l.stream) cudaStreamDestroy(l.stream);
+    }
+    if (h->batch_fork) cudaEventDestroy(h->batch_fork);
     for (auto& e : h->ev)
         if (e) cudaEventDestroy(e);
     if (h->own_stream) cudaStreamDestroy(h->own_stream);
@@ -974,8 +1016,23 @@ int gwb200_run_g0w0_batch(gwb200_handle* const* systems, int64_t nsys, int64_t n
             nb_states += sizeof(int64_t) * nstates[i];
         }
         w->err.ensure(sizeof(unsigned long long));
-        w->tc_sched.ensure(sizeof(unsigned long long));
-        w->chunk_key[0] = -1;  // the lead handle's workspaces are resized below
+        // lanes: GWB200_BATCH_STREAMS concurrent streams (default 4, at most one per molecule), each
+        // with its own workspaces; GWB200_BATCH_SHARE_SMS=1 caps each lane's persistent update
+        // kernels at SMs / lanes CTAs (default: every lane's grid covers the GPU; those kernels take
+        // their work units from a counter and never wait on one another, so they need not be
+        // co-resident).  Measured on the 64-molecule config-4 batch (mixed): 1 lane 261-274 ms,
+        // 2 lanes 233-244, 4 lanes 221-224.
+        int lanes = kMaxBatchLanes;
+        if (const char* e = std::getenv("GWB200_BATCH_STREAMS")) lanes = std::atoi(e);
+        lanes = std::max(1, std::min<int>({kMaxBatchLanes, lanes, (int)nsys}));
+        const char* share_env = std::getenv("GWB200_BATCH_SHARE_SMS");
+        const bool share = share_env && std::strcmp(share_env, "1") == 0;
+        int lane_ctas = w->persistent_ctas;
+        if (lanes > 1 && share) {
+            int sms = 148;
+            GWB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, w->device));
+            lane_ctas = std::max(1, (w->persistent_ctas > 0 ? w->persistent_ctas : sms) / lanes);
+        }
 
         // plans: cached per batch signature, else timed candidates (GWB200_BATCH_PLAN=tuned, the
         // default), the cost model alone (=model), one bucket per molecule (=each), one bucket (=single)
@@ -987,10 +1044,13 @@ int gwb200_run_g0w0_batch(gwb200_handle* const* systems, int64_t nsys, int64_t n
         }
         size_t free_b = 0, total_b = 0;
         GWB_CUDA(cudaMemGetInfo(&free_b, &total_b));
-        const size_t avail = free_b + w->a.bytes + w->linv.bytes + w->qacc.bytes + w->panel32.bytes;
+        size_t held = 0;
+        for (const BatchLane& l : w->lanes) held += l.bytes();
+        const size_t avail = free_b + held;
         const char* mode_env = std::getenv("GWB200_BATCH_PLAN");
         const std::string mode = mode_env ? mode_env : "tuned";
-        std::vector<int64_t> key = {(int64_t)w->device, (int64_t)precision, (int64_t)oz, (int64_t)mixed_tc, nfreq};
+        std::vector<int64_t> key = {(int64_t)w->device, (int64_t)precision, (int64_t)oz, (int64_t)mixed_tc, nfreq,
+                                    (int64_t)lanes, (int64_t)lane_ctas};
         key.insert(key.end(), n_sorted.begin(), n_sorted.end());
         key.insert(key.end(), m_sorted.begin(), m_sorted.end());
         std::vector<std::vector<int64_t>> cands;
@@ -1010,7 +1070,7 @@ int gwb200_run_g0w0_batch(gwb200_handle* const* systems, int64_t nsys, int64_t n
             }
             if (!cached) {
                 const double tau = batch_step_us(mixed), rate = batch_tflops(mixed);
-                const size_t b0 = (size_t)(0.85 * (double)avail);
+                const size_t b0 = (size_t)(0.85 * (double)avail / lanes);
                 for (double mult : (mode == "tuned" ? std::vector<double>{1.0, 0.25, 4.0} : std::vector<double>{1.0})) {
                     std::vector<int64_t> p = plan_buckets(n_sorted, m_sorted, nfreq, mixed, b0, tau * mult, rate);
                     if (std::find(cands.begin(), cands.end(), p) == cands.end()) cands.push_back(p);
@@ -1025,7 +1085,10 @@ int gwb200_run_g0w0_batch(gwb200_handle* const* systems, int64_t nsys, int64_t n
         const TallGeometry gmax = make_geometry(n_sorted.back(), *std::max_element(m_sorted.begin(), m_sorted.end()));
         if (batch_bytes_per_matrix(gmax, mixed, oz) > avail)
             fail(GWB200_OOM, "not enough device memory for one frequency of the largest eps(iw) in the batch");
-        size_t budget = (size_t)(0.85 * (double)avail);
+        size_t budget = (size_t)(0.85 * (double)avail / lanes);  // per lane
+        // GWB200_MAX_FREQ_CHUNK caps the matrices per launch sequence (tests use it to split buckets)
+        int64_t cap = 0;
+        if (const char* env = std::getenv("GWB200_MAX_FREQ_CHUNK")) cap = std::max<long long>(0, std::atoll(env));
         std::vector<std::vector<BatchChunk>> chunks;
         std::vector<BatchGroup> groups;
         BatchNeed need;
@@ -1034,26 +1097,37 @@ int gwb200_run_g0w0_batch(gwb200_handle* const* systems, int64_t nsys, int64_t n
             groups.clear();
             need = BatchNeed{};
             for (const auto& p : cands) {
-                chunks.push_back(batch_chunks(hs, ms, order, p, nfreq, mixed, oz, budget, groups));
+                chunks.push_back(batch_chunks(hs, ms, order, p, nfreq, mixed, oz, budget, cap, groups));
                 batch_need(chunks.back(), mixed, oz, need);
             }
-            if (need.total() <= (size_t)(0.9 * (double)avail) || attempt >= 12) break;
+            if (need.total() * (size_t)lanes <= (size_t)(0.9 * (double)avail) || attempt >= 12) break;
             budget = (size_t)(0.7 * (double)budget);
         }
-        size_buffer(w, w->a, need.a);
-        size_buffer(w, w->linv, need.linv);
-        size_buffer(w, w->qacc, need.qacc);
-        if (need.panel) size_buffer(w, w->panel32, need.panel);
+        for (int l = 0; l < lanes; ++l) {
+            BatchLane& ln = w->lanes[l];
+            size_buffer(w, ln.a, need.a);
+            size_buffer(w, ln.linv, need.linv);
+            size_buffer(w, ln.qacc, need.qacc);
+            if (need.panel) size_buffer(w, ln.panel, need.panel);
+            ln.sched.ensure(sizeof(unsigned long long));
+            if (l > 0 && !ln.stream) {
+                GWB_CUDA(cudaStreamCreateWithFlags(&ln.stream, cudaStreamNonBlocking));
+                GWB_CUDA(cudaEventCreateWithFlags(&ln.done, cudaEventDisableTiming));
+            }
+        }
+        if (!w->batch_fork) GWB_CUDA(cudaEventCreateWithFlags(&w->batch_fork, cudaEventDisableTiming));
         w->batch_desc.ensure(sizeof(BatchGroup) * groups.size());
+        std::vector<std::vector<std::vector<size_t>>> assign;
+        for (const auto& ch : chunks) assign.push_back(batch_assign(ch, lanes, batch_step_us(mixed), batch_tflops(mixed)));
         // FP64: the update kernel of each chunk geometry (timed before anything is built: the
         // autotuner overwrites the workspace)
         std::vector<std::vector<int>> variants(cands.size());
         for (size_t c = 0; c < cands.size(); ++c)
             for (const BatchChunk& ch : chunks[c])
                 variants[c].push_back(mixed ? -1
-                                            : tune_update_variant(ch.g, ch.nmat, w->a.as<double>(), s,
-                                                                  oz ? w->panel32.p : nullptr,
-                                                                  w->tc_sched.as<unsigned long long>(),
+                                            : tune_update_variant(ch.g, ch.nmat, w->lanes[0].a.as<double>(), s,
+                                                                  oz ? w->lanes[0].panel.p : nullptr,
+                                                                  w->lanes[0].sched.as<unsigned long long>(),
                                                                   w->err.as<unsigned long long>(), w->mem_limit <= 0));
 
         // uploads through the lead handle's pinned staging buffer: grid, state lists, group tables
@@ -1067,30 +1141,55 @@ int gwb200_run_g0w0_batch(gwb200_handle* const* systems, int64_t nsys, int64_t n
         std::memcpy(sp + 2 * nb_om + nb_states, groups.data(), nb_groups);
         GWB_CUDA(cudaMemcpyAsync(w->batch_desc.p, sp + 2 * nb_om + nb_states, nb_groups, cudaMemcpyHostToDevice, s));
         GWB_CUDA(cudaMemsetAsync(w->err.p, 0xFF, sizeof(unsigned long long), s));
+        // the lanes fork off the lead stream and join back onto it around each phase
+        auto lane_stream = [&](int l) { return l == 0 ? s : w->lanes[l].stream; };
+        auto fork = [&]() {
+            GWB_CUDA(cudaEventRecord(w->batch_fork, s));
+            for (int l = 1; l < lanes; ++l) GWB_CUDA(cudaStreamWaitEvent(w->lanes[l].stream, w->batch_fork, 0));
+        };
+        auto join = [&]() {
+            for (int l = 1; l < lanes; ++l) {
+                GWB_CUDA(cudaEventRecord(w->lanes[l].done, w->lanes[l].stream));
+                GWB_CUDA(cudaStreamWaitEvent(s, w->lanes[l].done, 0));
+            }
+        };
         GWB_CUDA(cudaEventRecord(w->ev[0], s));
         int64_t launches = 0;
         size_t off = 2 * nb_om;
+        fork();  // members' uploads, panel gathers and scale vectors, round robin over the lanes
         for (int64_t i = 0; i < nsys; ++i) {
             gwb200_handle* h = hs[(size_t)i];
+            cudaStream_t ls = lane_stream((int)(i % lanes));
             const size_t nb_st = sizeof(int64_t) * nstates[i];
             std::memcpy(sp + off, states[i], nb_st);
-            GWB_CUDA(cudaMemcpyAsync(h->omega.p, sp, nb_om, cudaMemcpyHostToDevice, s));
-            GWB_CUDA(cudaMemcpyAsync(h->weight.p, sp + nb_om, nb_om, cudaMemcpyHostToDevice, s));
-            GWB_CUDA(cudaMemcpyAsync(h->states.p, sp + off, nb_st, cudaMemcpyHostToDevice, s));
+            GWB_CUDA(cudaMemcpyAsync(h->omega.p, sp, nb_om, cudaMemcpyHostToDevice, ls));
+            GWB_CUDA(cudaMemcpyAsync(h->weight.p, sp + nb_om, nb_om, cudaMemcpyHostToDevice, ls));
+            GWB_CUDA(cudaMemcpyAsync(h->states.p, sp + off, nb_st, cudaMemcpyHostToDevice, ls));
             off += nb_st;
             launches += launch_gather_panel(h->pqo.as<double>(), h->nmo, h->nocc, h->states.as<int64_t>(), nstates[i],
-                                            h->xt.as<double>(), s);
+                                            h->xt.as<double>(), ls);
             launches += launch_scale_vectors(h->delta.as<double>(), h->n, make_geometry(h->n, ms[(size_t)i]).n_pad,
-                                             h->omega.as<double>(), nfreq, h->dvec.as<double>(), s);
+                                             h->omega.as<double>(), nfreq, h->dvec.as<double>(), ls);
         }
+        join();
         GWB_CUDA(cudaEventRecord(w->ev[1], s));
         const BatchGroup* dgroups = w->batch_desc.as<BatchGroup>();
+        // one plan: each lane runs its chunks
+        auto run_plan = [&](size_t c) {
+            int64_t n_launch = 0;
+            fork();
+            for (int l = 0; l < lanes; ++l)
+                n_launch += batch_screen(w, w->lanes[l], lane_stream(l), lane_ctas, chunks[c], assign[c][(size_t)l],
+                                         dgroups, variants[c], mixed, mixed_tc, oz);
+            join();
+            return n_launch;
+        };
         size_t pick = 0;
         if (cands.size() > 1) {  // time each candidate plan once, keep the fastest for this signature
             float best = std::numeric_limits<float>::infinity();
             for (size_t c = 0; c < cands.size(); ++c) {
                 GWB_CUDA(cudaEventRecord(w->ev[4], s));
-                batch_screen(w, chunks[c], dgroups, variants[c], mixed, mixed_tc, oz);
+                run_plan(c);
                 GWB_CUDA(cudaEventRecord(w->ev[5], s));
                 GWB_CUDA(cudaEventSynchronize(w->ev[5]));
                 const float t = elapsed(w->ev[4], w->ev[5]);
@@ -1103,14 +1202,17 @@ int gwb200_run_g0w0_batch(gwb200_handle* const* systems, int64_t nsys, int64_t n
             g_batch_plans[key] = cands[pick];
         }
         GWB_CUDA(cudaEventRecord(w->ev[4], s));
-        launches += batch_screen(w, chunks[pick], dgroups, variants[pick], mixed, mixed_tc, oz);
+        launches += run_plan(pick);
         GWB_CUDA(cudaEventRecord(w->ev[2], s));
         st->kernel_launches = launches;
+        fork();  // members' contractions and QP updates, round robin over the lanes
         for (int64_t i = 0; i < nsys; ++i) {
+            hs[(size_t)i]->stream = lane_stream((int)(i % lanes));
             contract_on_device(hs[(size_t)i], nfreq, nstates[i], st);
             qp_on_device(hs[(size_t)i], nfreq, npade, nstates[i]);
             st->kernel_launches += 2;
         }
+        join();
         GWB_CUDA(cudaEventRecord(w->ev[3], s));
         // results and the pivot word back in one synchronisation
         size_t nb_out = sizeof(unsigned long long);

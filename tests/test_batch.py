@@ -119,7 +119,7 @@ def test_batch_matches_each_molecule_alone(precision, monkeypatch):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("plan", ["each", "single", "model"])
+@pytest.mark.parametrize("plan", ["each", "single", "model", "model-3-streams", "each-4-streams-unshared"])
 def test_every_bucket_plan_gives_the_same_bits(plan, monkeypatch):
     from minigw_b200 import B200Backend, run_g0w0_batch
 
@@ -132,7 +132,10 @@ def test_every_bucket_plan_gives_the_same_bits(plan, monkeypatch):
         monkeypatch.setenv("GWB200_BATCH_PLAN", "each")
         ref = run_g0w0_batch(bes, 16, 8, states)
         assert ref["buckets"] == len(inputs)
-        monkeypatch.setenv("GWB200_BATCH_PLAN", plan)
+        if "streams" in plan:  # buckets on concurrent streams with their own workspaces
+            monkeypatch.setenv("GWB200_BATCH_STREAMS", plan.split("-")[1])
+            monkeypatch.setenv("GWB200_BATCH_SHARE_SMS", "0" if plan.endswith("unshared") else "1")
+        monkeypatch.setenv("GWB200_BATCH_PLAN", plan.split("-")[0])
         got = run_g0w0_batch(bes, 16, 8, states)
         if plan == "single":
             assert got["buckets"] == 1
@@ -149,14 +152,16 @@ def test_batch_multi_chunk_and_states(monkeypatch):
     from minigw_b200 import B200Backend, run_g0w0_batch
 
     inputs = _systems([(16, 3), (22, 4), (26, 4)], seed0=500)
-    states = [list(range(inp.nmo)), [1, 4, 5], [3]]
+    states = [list(range(inputs[0].nmo)), [1, 4, 5], [3]]
     bes = [B200Backend(0) for _ in inputs]
     try:
         for be, inp in zip(bes, inputs):
             be.load_system(inp)
         alone = [be.run_g0w0(20, 10, st, precision="mixed") for be, st in zip(bes, states)]
         monkeypatch.setenv("GWB200_BATCH_PLAN", "single")
+        monkeypatch.setenv("GWB200_MAX_FREQ_CHUNK", "7")  # 60 matrices in 9 launch sequences
         got = run_g0w0_batch(bes, 20, 10, states)
+        assert got["stats"]["frequency_chunks"] == 9
         for a, s in zip(alone, got["sigma"]):
             np.testing.assert_array_equal(s, a["sigma"])
     finally:
