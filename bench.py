@@ -254,7 +254,7 @@ def run_b200(args, wl):
     stream = torch.cuda.Stream(device=local)
     be.set_stream(stream.cuda_stream)
     peak_fp64 = be.fp64_peak_tflops()
-    be.load_system(inp)
+    be.load_system(inp, states)  # V_ph and the requested states' panel rows only
 
     reduce_sum = torch_allreduce_sum(f"cuda:{local}") if split else None
 
@@ -311,19 +311,20 @@ def run_b200(args, wl):
     total_ms = max_over_ranks(total_ms)
     ms_per_step = total_ms / args.steps
 
-    # ---- e2e: ERI uploaded from pinned host memory every step ----
-    # bytes the library moves per e2e step: the (pq|o.) ERI block and exchange diagonal, mo energies
-    # and vxc diagonal (load_system); grid, weights and states (run_g0w0); Sigma_c, Sigma_x diagonal,
-    # QP energies and the pivot flag read back
+    # ---- e2e: the system uploaded from pinned host memory every step ----
+    # bytes the library moves per e2e step: V_ph = (ia|jb), the states' (pk|ia) panel rows, the
+    # exchange diagonal, mo energies and vxc diagonal (load_system with the state list); grid,
+    # weights and states (run_g0w0); Sigma_c, Sigma_x diagonal, QP energies and the pivot flag back
     nmo, nocc, nf, ns = wl.nmo, wl.nocc, wl.nfreq, len(states)
-    h2d = 8 * (nmo * nmo * nocc * nmo + nmo * nocc + 2 * nmo) + (16 * nf + 8 * ns)
+    nph = nocc * (nmo - nocc)
+    h2d = 8 * (nph * nph + ns * nmo * nph + nmo * nocc + 2 * nmo) + (16 * nf + 8 * ns)
     d2h = 16 * nmo * nf + 8 * nmo + 8 * nmo + 8
     ee0, ee1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     barrier()
     torch.cuda.synchronize()
     ee0.record(stream)
     for _ in range(args.steps):
-        be.load_system(inp)
+        be.load_system(inp, states)
         step()
     ee1.record(stream)
     torch.cuda.synchronize()
@@ -338,13 +339,13 @@ def run_b200(args, wl):
         be2 = B200Backend(local)
         stream2 = torch.cuda.Stream(device=local)
         be2.set_stream(stream2.cuda_stream)
-        be2.load_system(inp)
+        be2.load_system(inp, states)
         be2.run_g0w0(wl.nfreq, wl.npade, states, precision=args.precision)  # buffers sized, tuner cached
         pair = [be, be2]
 
         def upload(h, box):
             try:
-                h.load_system(inp)
+                h.load_system(inp, states)
             except Exception as exc:  # re-raised on the main thread
                 box.append(exc)
 
@@ -352,7 +353,7 @@ def run_b200(args, wl):
         torch.cuda.synchronize()
         ep0, ep1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         ep0.record(stream)
-        pair[0].load_system(inp)
+        pair[0].load_system(inp, states)
         for k in range(args.steps):
             nxt, errs = None, []
             if k + 1 < args.steps:
@@ -591,7 +592,7 @@ def run_batch(args):
         inp = make_input_on_device(nmo, nocc, seed=args.seed + 2000 + i, device=0, pin=False)
         be = B200Backend(0)
         be.set_stream(stream.cuda_stream)
-        be.load_system(inp)
+        be.load_system(inp, [nocc - 1, nocc])
         del inp
         bes.append(be)
         states.append([nocc - 1, nocc])

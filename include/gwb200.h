@@ -104,6 +104,18 @@ int gwb200_set_memory_limit(gwb200_handle* h, int64_t bytes);
 int gwb200_load_system(gwb200_handle* h, int64_t nmo, int64_t nocc, const double* mo_energy,
                        const double* eri, const double* vxc, double fermi_energy);
 
+/* gwb200_load_system for a known state list: only V_ph = (ia|jb) (n^2 doubles), the panel rows
+ * (p k|i a) of the given states (nstates * nmo * n doubles) and the exchange diagonal are copied
+ * from eri (3D copies of contiguous runs of nvir doubles), instead of the (pq|o.) block
+ * (nmo^3 * nocc doubles): 0.29 GB instead of 1.92 GB at nmo = 200, nocc = 30, 10 states.  Later
+ * calls on the handle must pass this same state list (same order); results are bit-identical
+ * to gwb200_load_system's.  Replaces the same reference code as gwb200_load_system, with the
+ * (p k|ov) slices of gw::workspace::DevicePqPhPanelView::fill_panel
+ * (src/workspace/device_pq_ph_panel.cu:141-166) taken once per state. */
+int gwb200_load_system_states(gwb200_handle* h, int64_t nmo, int64_t nocc, const double* mo_energy,
+                              const double* eri, const double* vxc, double fermi_energy,
+                              const int64_t* states, int64_t nstates);
+
 /* Correlation self-energy Sigma_c(i w_n) on the imaginary grid for the requested states.
  * sigma_out is nmo x nfreq complex, row-major (gw::MatrixComplex); rows of states not
  * requested are set to zero.  eta == 0: real SPD Cholesky of eps = I + D^1/2 V D^1/2;

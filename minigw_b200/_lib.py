@@ -35,7 +35,7 @@ EXPORTS = (
     "gwb200_last_error", "gwb200_version", "gwb200_create", "gwb200_destroy", "gwb200_set_stream",
     "gwb200_set_memory_limit", "gwb200_server_create", "gwb200_server_submit", "gwb200_server_wait",
     "gwb200_server_destroy",
-    "gwb200_load_system", "gwb200_run_g0w0", "gwb200_sigma_c_shard",
+    "gwb200_load_system", "gwb200_load_system_states", "gwb200_run_g0w0", "gwb200_sigma_c_shard",
     "gwb200_sigma_c", "gwb200_screened_forms", "gwb200_screened_forms_complex", "gwb200_sigma_x_diag", "gwb200_qp", "gwb200_pade_sweep",
     "gwb200_grid", "gwb200_read_input_h5", "gwb200_screened_forms_noalloc", "gwb200_fp64_peak_tflops",
     "gwb200_update_kernel", "gwb200_run_g0w0_batch", "gwb200_plan_buckets",
@@ -105,6 +105,7 @@ def _load() -> C.CDLL:
     lib.gwb200_server_wait.argtypes = [_vp, C.c_int64, C.POINTER(C.c_int), _dp, _dp, _dp]
     lib.gwb200_server_destroy.argtypes = [_vp]
     lib.gwb200_load_system.argtypes = [_vp, C.c_int64, C.c_int64, _dp, _dp, _dp, C.c_double]
+    lib.gwb200_load_system_states.argtypes = [_vp, C.c_int64, C.c_int64, _dp, _dp, _dp, C.c_double, _ip, C.c_int64]
     lib.gwb200_sigma_c.argtypes = [_vp, _dp, _dp, C.c_int64, _ip, C.c_int64, C.c_double, C.c_int, _dp,
                                    C.POINTER(Stats)]
     lib.gwb200_sigma_c_shard.argtypes = [_vp, _dp, _dp, C.c_int64, C.c_int64, C.c_int64, _ip, C.c_int64, C.c_double,

@@ -223,15 +223,16 @@ int main(int argc, char** argv) {
         std::cout << "Frequency parallel mode: device-batched (all frequencies per launch)\n";
         std::cout << "Precision: " << cli.precision << '\n';
         if (cli.print_memory_footprint) {
-            const double eri_gib = static_cast<double>(nmo) * nmo * nmo * nmo * 8.0 / (1024.0 * 1024.0 * 1024.0);
-            const double eps_gib = (static_cast<double>(n_ph) * n_ph + static_cast<double>(n_ph) * states.size() * nmo) *
+            const double res_gib = (static_cast<double>(n_ph) * n_ph + static_cast<double>(n_ph) * states.size() * nmo) *
                                    8.0 / (1024.0 * 1024.0 * 1024.0);
-            std::cout << "Device memory estimate: ERI " << eri_gib << " GiB resident, eps(iw)+panel " << eps_gib
-                      << " GiB per frequency (frequencies are chunked to fit)\n";
+            std::cout << "Device memory estimate: V_ph + panel " << res_gib << " GiB resident, eps(iw)+panel "
+                      << res_gib << " GiB per frequency (frequencies are chunked to fit)\n";
         }
         const auto t_total = std::chrono::steady_clock::now();
         auto t = std::chrono::steady_clock::now();
-        check(gwb200_load_system(h, nmo, nocc, mo.data(), eri.data(), vxc.data(), fermi), "gwb200_load_system");
+        check(gwb200_load_system_states(h, nmo, nocc, mo.data(), eri.data(), vxc.data(), fermi, states.data(),
+                                        static_cast<int64_t>(states.size())),
+              "gwb200_load_system_states");
         const double setup_seconds = seconds_since(t);
         std::vector<double> omega(cli.freq_points), weight(cli.freq_points);
         check(gwb200_grid(static_cast<int64_t>(cli.freq_points), omega.data(), weight.data()), "generate grid");

@@ -141,6 +141,9 @@ struct gwb200_handle {
     cudaMemPool_t pool = nullptr;   // pool for exact-size buffers (set by a server), else the default
     int64_t chunk_fc = 0;
     int64_t last_update_kernel = -1;  // gwb200_update_kernel
+    // gwb200_load_system_states: the state list whose panel rows are resident in xt (empty: the
+    // (pq|o.) block is resident in pqo and the panel is gathered per call)
+    std::vector<int64_t> bound_states;
     int persistent_ctas = 0;          // > 0: cap of the persistent kernels' grids (GPU shared by slots)
 };
 
@@ -224,7 +227,10 @@ void compute_forms(gwb200_handle* h, const double* omega, int64_t nfreq, const i
 
     h->omega.ensure(sizeof(double) * nfreq);
     h->states.ensure(sizeof(int64_t) * nstates);
-    size_buffer(h, h->xt, sizeof(double) * (size_t)m * h->n);
+    const bool bound = !h->bound_states.empty();
+    if (bound && !std::equal(states, states + nstates, h->bound_states.begin(), h->bound_states.end()))
+        fail(GWB200_BAD_ARGUMENT, "the state list must be the one given to gwb200_load_system_states");
+    if (!bound) size_buffer(h, h->xt, sizeof(double) * (size_t)m * h->n);
     size_buffer(h, h->qall, sizeof(double) * planes * (size_t)nfreq * g.m_pad);
     h->err.ensure(sizeof(unsigned long long));
     {  // grid, states and (optionally) weights through the pinned staging buffer, all up front
@@ -294,8 +300,9 @@ void compute_forms(gwb200_handle* h, const double* omega, int64_t nfreq, const i
     }
 
     GWB_CUDA(cudaEventRecord(h->ev[0], s));
-    launches += launch_gather_panel(h->pqo.as<double>(), h->nmo, h->nocc, h->states.as<int64_t>(), nstates,
-                                    h->xt.as<double>(), s);
+    if (!bound)
+        launches += launch_gather_panel(h->pqo.as<double>(), h->nmo, h->nocc, h->states.as<int64_t>(), nstates,
+                                        h->xt.as<double>(), s);
     GWB_CUDA(cudaEventRecord(h->ev[1], s));
     const char* prof_env = std::getenv("GWB200_PROFILE");
     UpdateProfiler prof(prof_env && prof_env[0] == '1', s);
@@ -633,54 +640,109 @@ int gwb200_set_stream(gwb200_handle* h, void* stream) {
     });
 }
 
-int gwb200_load_system(gwb200_handle* h, int64_t nmo, int64_t nocc, const double* mo_energy, const double* eri,
-                       const double* vxc, double fermi_energy) {
-    return guarded([&] {
-        check_handle(h);
-        if (!mo_energy || !eri || !vxc) fail(GWB200_BAD_ARGUMENT, "null input array");
-        if (nmo <= 0) fail(GWB200_BAD_SHAPE, "OrbitalSpace: empty MO energy vector");
-        if (nocc <= 0 || nocc >= nmo) fail(GWB200_BAD_SHAPE, "OrbitalSpace: invalid number of occupied orbitals");
-        if (nmo > 1024) fail(GWB200_BAD_SHAPE, "nmo > 1024 is not supported");
-        cudaStream_t s = h->stream;
-        h->loaded = false;
-        const size_t nmo2 = (size_t)nmo * nmo;
-        const int64_t n = nocc * (nmo - nocc);
+namespace {
+// Shared body of gwb200_load_system (states == NULL: the (pq|o.) block stays resident and panels
+// are gathered per call) and gwb200_load_system_states (V_ph and the panel rows of `states` copied
+// from the host straight into their device layouts; nothing else of the ERI is uploaded).
+void load_system_impl(gwb200_handle* h, int64_t nmo, int64_t nocc, const double* mo_energy, const double* eri,
+                      const double* vxc, double fermi_energy, const int64_t* states, int64_t nstates) {
+    check_handle(h);
+    if (!mo_energy || !eri || !vxc) fail(GWB200_BAD_ARGUMENT, "null input array");
+    if (nmo <= 0) fail(GWB200_BAD_SHAPE, "OrbitalSpace: empty MO energy vector");
+    if (nocc <= 0 || nocc >= nmo) fail(GWB200_BAD_SHAPE, "OrbitalSpace: invalid number of occupied orbitals");
+    if (nmo > 1024) fail(GWB200_BAD_SHAPE, "nmo > 1024 is not supported");
+    const bool bound = states != nullptr;
+    if (bound) {
+        if (nstates <= 0) fail(GWB200_BAD_SHAPE, "at least one state is required");
+        std::vector<int64_t> seen(states, states + nstates);
+        for (int64_t st : seen)
+            if (st < 0 || st >= nmo) fail(GWB200_BAD_SHAPE, "Selected state is out of range");
+        std::sort(seen.begin(), seen.end());
+        if (std::adjacent_find(seen.begin(), seen.end()) != seen.end())
+            fail(GWB200_BAD_SHAPE, "duplicate state in the state list");
+    }
+    cudaStream_t s = h->stream;
+    h->loaded = false;
+    h->bound_states.clear();
+    const size_t nmo2 = (size_t)nmo * nmo;
+    const int64_t nvir = nmo - nocc, n = nocc * nvir;
+    if (h->mem_limit > 0)  // drop the previous request's workspaces before sizing this system
+        for (DevBuf* b : {&h->xt, &h->dvec, &h->a, &h->linv, &h->qacc, &h->qall, &h->panel32}) b->release();
+    if (bound) {
+        h->pqo.release();
+        size_buffer(h, h->xt, sizeof(double) * (size_t)nstates * nmo * n);
+    } else {
+        size_buffer(h, h->pqo, sizeof(double) * nmo2 * nocc * nmo);
+    }
+    size_buffer(h, h->xdiag, sizeof(double) * nmo * nocc);
+    h->mo.ensure(sizeof(double) * nmo);
+    h->vxc_diag.ensure(sizeof(double) * nmo);
+    h->sigx.ensure(sizeof(double) * nmo);
+    h->delta.ensure(sizeof(double) * n);
+    size_buffer(h, h->v, sizeof(double) * (size_t)n * n);
+    h->flag.ensure(sizeof(int));
+    std::vector<double> vd((size_t)nmo);
+    for (int64_t p = 0; p < nmo; ++p) vd[(size_t)p] = vxc[p * nmo + p];
+    if (bound) {
+        // One 3D copy per source block eri[p, ., ., .] (an nmo x nmo x nmo array of rows of nmo
+        // doubles): x = the virtual index s (nvir doubles from nocc), y = the occupied index
+        // r < nocc, z = q.  The destination rows are the n = nocc * nvir columns (i, a) of
+        //   V[j nvir + b, i nvir + a] = eri[j, nocc + b, i, nocc + a]   (p = j < nocc, z = b)
+        //   Xt[t nmo + k, i nvir + a]  = eri[states[t], k, i, nocc + a]   (p = states[t], z = k),
+        // the layouts k_gather_vph / k_gather_panel produce from the (pq|o.) block.
+        auto copy_block = [&](int64_t p, int64_t q0, int64_t depth, double* dst) {
+            cudaMemcpy3DParms c{};
+            c.srcPtr = make_cudaPitchedPtr(const_cast<double*>(eri + (size_t)p * nmo2 * nmo), sizeof(double) * nmo,
+                                           sizeof(double) * nmo, (size_t)nmo);
+            c.srcPos = make_cudaPos(sizeof(double) * nocc, 0, (size_t)q0);
+            c.dstPtr = make_cudaPitchedPtr(dst, sizeof(double) * nvir, sizeof(double) * nvir, (size_t)nocc);
+            c.dstPos = make_cudaPos(0, 0, 0);
+            c.extent = make_cudaExtent(sizeof(double) * nvir, (size_t)nocc, (size_t)depth);
+            c.kind = cudaMemcpyHostToDevice;
+            GWB_CUDA(cudaMemcpy3DAsync(&c, s));
+        };
+        for (int64_t j = 0; j < nocc; ++j) copy_block(j, nocc, nvir, h->v.as<double>() + (size_t)j * nvir * n);
+        for (int64_t t = 0; t < nstates; ++t) copy_block(states[t], 0, nmo, h->xt.as<double>() + (size_t)t * nmo * n);
+    } else {
         // Only the (pq|o.) block is uploaded: every V_ph / panel element has an occupied third
         // index.  One 2D copy: nmo^2 rows of nocc*nmo contiguous doubles, source pitch nmo^2.
-        if (h->mem_limit > 0)  // drop the previous request's workspaces before sizing this system
-            for (DevBuf* b : {&h->xt, &h->dvec, &h->a, &h->linv, &h->qacc, &h->qall, &h->panel32}) b->release();
-        size_buffer(h, h->pqo, sizeof(double) * nmo2 * nocc * nmo);
-        size_buffer(h, h->xdiag, sizeof(double) * nmo * nocc);
-        h->mo.ensure(sizeof(double) * nmo);
-        h->vxc_diag.ensure(sizeof(double) * nmo);
-        h->sigx.ensure(sizeof(double) * nmo);
-        h->delta.ensure(sizeof(double) * n);
-        size_buffer(h, h->v, sizeof(double) * (size_t)n * n);
-        h->flag.ensure(sizeof(int));
-        std::vector<double> vd((size_t)nmo);
-        for (int64_t p = 0; p < nmo; ++p) vd[(size_t)p] = vxc[p * nmo + p];
         GWB_CUDA(cudaMemcpy2DAsync(h->pqo.p, sizeof(double) * nocc * nmo, eri, sizeof(double) * nmo2,
                                    sizeof(double) * nocc * nmo, nmo2, cudaMemcpyHostToDevice, s));
-        // exchange diagonal eri[p,i,p,i]: for each p, nocc elements with stride nmo^2 + 1
-        for (int64_t p = 0; p < nmo; ++p)
-            GWB_CUDA(cudaMemcpy2DAsync(h->xdiag.as<double>() + p * nocc, sizeof(double),
-                                       eri + ((size_t)p * nmo * nmo + p) * nmo, sizeof(double) * (nmo2 + 1),
-                                       sizeof(double), nocc, cudaMemcpyHostToDevice, s));
-        GWB_CUDA(cudaMemcpyAsync(h->mo.p, mo_energy, sizeof(double) * nmo, cudaMemcpyHostToDevice, s));
-        GWB_CUDA(cudaMemcpyAsync(h->vxc_diag.p, vd.data(), sizeof(double) * nmo, cudaMemcpyHostToDevice, s));
-        GWB_CUDA(cudaMemsetAsync(h->flag.p, 0, sizeof(int), s));
-        launch_delta(h->mo.as<double>(), nmo, nocc, h->delta.as<double>(), h->flag.as<int>(), s);
-        launch_gather_vph(h->pqo.as<double>(), nmo, nocc, h->v.as<double>(), s);
-        launch_sigma_x_diag(h->xdiag.as<double>(), nmo, nocc, h->sigx.as<double>(), s);
-        int bad = 0;
-        GWB_CUDA(cudaMemcpyAsync(&bad, h->flag.p, sizeof(int), cudaMemcpyDeviceToHost, s));
-        GWB_CUDA(cudaStreamSynchronize(s));
-        h->nmo = nmo;
-        h->nocc = nocc;
-        h->n = n;
-        h->fermi = fermi_energy;
-        h->bad_gap = bad != 0;
-        h->loaded = true;
+    }
+    // exchange diagonal eri[p,i,p,i]: for each p, nocc elements with stride nmo^2 + 1
+    for (int64_t p = 0; p < nmo; ++p)
+        GWB_CUDA(cudaMemcpy2DAsync(h->xdiag.as<double>() + p * nocc, sizeof(double),
+                                   eri + ((size_t)p * nmo * nmo + p) * nmo, sizeof(double) * (nmo2 + 1),
+                                   sizeof(double), nocc, cudaMemcpyHostToDevice, s));
+    GWB_CUDA(cudaMemcpyAsync(h->mo.p, mo_energy, sizeof(double) * nmo, cudaMemcpyHostToDevice, s));
+    GWB_CUDA(cudaMemcpyAsync(h->vxc_diag.p, vd.data(), sizeof(double) * nmo, cudaMemcpyHostToDevice, s));
+    GWB_CUDA(cudaMemsetAsync(h->flag.p, 0, sizeof(int), s));
+    launch_delta(h->mo.as<double>(), nmo, nocc, h->delta.as<double>(), h->flag.as<int>(), s);
+    if (!bound) launch_gather_vph(h->pqo.as<double>(), nmo, nocc, h->v.as<double>(), s);
+    launch_sigma_x_diag(h->xdiag.as<double>(), nmo, nocc, h->sigx.as<double>(), s);
+    int bad = 0;
+    GWB_CUDA(cudaMemcpyAsync(&bad, h->flag.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+    GWB_CUDA(cudaStreamSynchronize(s));
+    h->nmo = nmo;
+    h->nocc = nocc;
+    h->n = n;
+    h->fermi = fermi_energy;
+    h->bad_gap = bad != 0;
+    if (bound) h->bound_states.assign(states, states + nstates);
+    h->loaded = true;
+}
+} // namespace
+
+int gwb200_load_system(gwb200_handle* h, int64_t nmo, int64_t nocc, const double* mo_energy, const double* eri,
+                       const double* vxc, double fermi_energy) {
+    return guarded([&] { load_system_impl(h, nmo, nocc, mo_energy, eri, vxc, fermi_energy, nullptr, 0); });
+}
+
+int gwb200_load_system_states(gwb200_handle* h, int64_t nmo, int64_t nocc, const double* mo_energy, const double* eri,
+                              const double* vxc, double fermi_energy, const int64_t* states, int64_t nstates) {
+    return guarded([&] {
+        if (!states) fail(GWB200_BAD_ARGUMENT, "null state list");
+        load_system_impl(h, nmo, nocc, mo_energy, eri, vxc, fermi_energy, states, nstates);
     });
 }
 
@@ -981,6 +1043,9 @@ int gwb200_run_g0w0_batch(gwb200_handle* const* systems, int64_t nsys, int64_t n
             if (!h->loaded) fail(GWB200_NO_SYSTEM, "no system loaded: call gwb200_load_system first");
             if (h->device != w->device) fail(GWB200_BAD_ARGUMENT, "the systems of a batch must share one device");
             check_states(h, states[i], nstates[i]);
+            if (!h->bound_states.empty() &&
+                !std::equal(states[i], states[i] + nstates[i], h->bound_states.begin(), h->bound_states.end()))
+                fail(GWB200_BAD_ARGUMENT, "the state list must be the one given to gwb200_load_system_states");
             if (h->bad_gap)
                 fail(GWB200_NONPOSITIVE_GAP, "some e_a - e_i <= 0: chi0(iw) is not negative definite, eps(iw) is not SPD");
             ns[(size_t)i] = h->n;
@@ -1009,7 +1074,7 @@ int gwb200_run_g0w0_batch(gwb200_handle* const* systems, int64_t nsys, int64_t n
             h->omega.ensure(nb_om);
             h->weight.ensure(nb_om);
             h->states.ensure(sizeof(int64_t) * nstates[i]);
-            size_buffer(h, h->xt, sizeof(double) * (size_t)ms[(size_t)i] * h->n);
+            if (h->bound_states.empty()) size_buffer(h, h->xt, sizeof(double) * (size_t)ms[(size_t)i] * h->n);
             size_buffer(h, h->dvec, sizeof(double) * (size_t)nfreq * gi.n_pad);
             size_buffer(h, h->qall, sizeof(double) * (size_t)nfreq * gi.m_pad);
             h->complex_forms = false;
@@ -1166,8 +1231,9 @@ int gwb200_run_g0w0_batch(gwb200_handle* const* systems, int64_t nsys, int64_t n
             GWB_CUDA(cudaMemcpyAsync(h->weight.p, sp + nb_om, nb_om, cudaMemcpyHostToDevice, ls));
             GWB_CUDA(cudaMemcpyAsync(h->states.p, sp + off, nb_st, cudaMemcpyHostToDevice, ls));
             off += nb_st;
-            launches += launch_gather_panel(h->pqo.as<double>(), h->nmo, h->nocc, h->states.as<int64_t>(), nstates[i],
-                                            h->xt.as<double>(), ls);
+            if (h->bound_states.empty())
+                launches += launch_gather_panel(h->pqo.as<double>(), h->nmo, h->nocc, h->states.as<int64_t>(),
+                                                nstates[i], h->xt.as<double>(), ls);
             launches += launch_scale_vectors(h->delta.as<double>(), h->n, make_geometry(h->n, ms[(size_t)i]).n_pad,
                                              h->omega.as<double>(), nfreq, h->dvec.as<double>(), ls);
         }

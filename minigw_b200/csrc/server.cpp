@@ -3,7 +3,7 @@
 // A server owns `slots` worker threads on one device; each worker owns one gwb200_handle (its own
 // CUDA stream and resident buffers) with a device-memory limit of hbm_budget / slots.  Requests
 // (one G0W0 solve each: system + grid size + states) wait in a FIFO and are admitted as soon as a
-// worker is free; a request whose smallest footprint (ERI block + V_ph + panels + one frequency
+// worker is free; a request whose smallest footprint (V_ph + its states' panel rows + one frequency
 // of the tall matrices) exceeds a slot's budget is rejected with GWB200_OOM.  Requests in
 // different slots run concurrently on different streams, so their kernels overlap on the GPU.
 // Every kernel is deterministic and a request's arithmetic does not depend on its chunking, so
@@ -64,12 +64,14 @@ struct gwb200_server {
 
 namespace {
 
+// Resident V_ph and panel rows of the request's states (gwb200_load_system_states) plus one
+// frequency of the tall matrices.
 size_t min_footprint(const gwb200_request& r) {
     const size_t nmo = (size_t)r.nmo, nocc = (size_t)r.nocc, n = nocc * (nmo - nocc);
     const size_t m = (size_t)r.nstates * nmo;
     const size_t n64 = (n + 63) / 64 * 64, m64 = (m + 63) / 64 * 64;
     const size_t per = (r.eta != 0.0 ? 2 : 1) * (n64 + m64) * n64 * sizeof(double);
-    return nmo * nmo * nocc * nmo * sizeof(double) + n * n * sizeof(double) + m * n * sizeof(double) + per;
+    return n * n * sizeof(double) + m * n * sizeof(double) + nmo * nocc * sizeof(double) + per;
 }
 
 void worker_main(gwb200_server* s) {
@@ -103,7 +105,8 @@ void worker_main(gwb200_server* s) {
         Result res;
         res.queue_ms = std::chrono::duration<double, std::milli>(start - job.submitted).count();
         const gwb200_request& r = job.req;
-        int st = gwb200_load_system(h, r.nmo, r.nocc, r.mo_energy, r.eri, r.vxc, r.fermi_energy);
+        int st = gwb200_load_system_states(h, r.nmo, r.nocc, r.mo_energy, r.eri, r.vxc, r.fermi_energy,
+                                           job.states.data(), (int64_t)job.states.size());
         gwb200_stats stats{};
         if (st == GWB200_OK)
             st = gwb200_run_g0w0(h, r.nfreq, r.npade, job.states.data(), (int64_t)job.states.size(), r.eta, r.precision,

@@ -162,15 +162,22 @@ class B200Backend:
         """Issue all work on a caller's CUDA stream (e.g. torch.cuda.Stream().cuda_stream)."""
         check(lib.gwb200_set_stream(self._h, C.c_void_p(stream_ptr) if stream_ptr else None))
 
-    def load_system(self, inp: GwInput) -> None:
+    def load_system(self, inp: GwInput, states=None) -> None:
+        """Upload a system.  With `states`, only V_ph and those states' panel rows are uploaded
+        (gwb200_load_system_states) and later calls must use the same state list."""
         eri = np.ascontiguousarray(inp.eri_mo, dtype=np.float64)
         mo = np.ascontiguousarray(inp.mo_energy, dtype=np.float64)
         vxc = np.ascontiguousarray(inp.vxc_mo, dtype=np.float64)
         nmo = mo.shape[0]
         if eri.size != nmo ** 4 or vxc.size != nmo ** 2:
             raise GwB200Error(1, "MolecularIntegrals: ERI tensor must have shape [nmo,nmo,nmo,nmo]")
-        check(lib.gwb200_load_system(self._h, nmo, int(inp.nocc), dptr(mo), dptr(eri), dptr(vxc),
-                                     float(inp.fermi_energy)))
+        if states is None:
+            check(lib.gwb200_load_system(self._h, nmo, int(inp.nocc), dptr(mo), dptr(eri), dptr(vxc),
+                                         float(inp.fermi_energy)))
+        else:
+            st = np.ascontiguousarray(states, dtype=np.int64)
+            check(lib.gwb200_load_system_states(self._h, nmo, int(inp.nocc), dptr(mo), dptr(eri), dptr(vxc),
+                                                float(inp.fermi_energy), iptr(st), st.shape[0]))
         self.nmo, self.nocc, self.fermi = nmo, int(inp.nocc), float(inp.fermi_energy)
 
     def sigma_c(self, omegas, weights, states, eta: float = 0.0, precision="fp64"):

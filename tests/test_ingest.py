@@ -1,0 +1,83 @@
+"""gwb200_load_system_states (V_ph and the states' panel rows copied straight from the host ERI)
+against gwb200_load_system (the (pq|o.) block resident, gathered on the device): identical bits."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+CASES = [(14, 3, [2, 3]), (24, 5, [4]), (30, 4, list(range(30))), (40, 7, [5, 6, 7, 8])]
+
+
+@pytest.mark.parametrize("nmo,nocc,states", CASES)
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_state_bound_load_is_bit_identical(nmo, nocc, states, precision):
+    from minigw_b200 import B200Backend
+    from minigw_b200.synthetic import make_input
+
+    inp = make_input(nmo, nocc, seed=700 + nmo)
+    with B200Backend(0) as full, B200Backend(0) as bound:
+        full.load_system(inp)
+        bound.load_system(inp, states)
+        a = full.run_g0w0(24, 12, states, precision=precision)
+        b = bound.run_g0w0(24, 12, states, precision=precision)
+        np.testing.assert_array_equal(a["sigma"], b["sigma"])
+        np.testing.assert_array_equal(a["sigma_x_diag"], b["sigma_x_diag"])
+        np.testing.assert_array_equal(a["qp"][states], b["qp"][states])
+
+
+def test_state_bound_load_complex_forms_and_shards():
+    from minigw_b200 import B200Backend, generate_transformed_legendre_grid
+    from minigw_b200.synthetic import make_input
+
+    inp = make_input(22, 4, seed=11)
+    states = [3, 4, 9]
+    om, w = generate_transformed_legendre_grid(16)
+    with B200Backend(0) as full, B200Backend(0) as bound:
+        full.load_system(inp)
+        bound.load_system(inp, states)
+        qa, _ = full.screened_forms_complex(om, states, eta=1e-3)
+        qb, _ = bound.screened_forms_complex(om, states, eta=1e-3)
+        np.testing.assert_array_equal(qa, qb)
+        pa, _ = full.sigma_c_shard(om, w, 3, 11, states)
+        pb, _ = bound.sigma_c_shard(om, w, 3, 11, states)
+        np.testing.assert_array_equal(pa, pb)
+
+
+def test_state_bound_load_rejects_another_state_list():
+    from minigw_b200 import B200Backend, GwB200Error
+    from minigw_b200.synthetic import make_input
+
+    inp = make_input(16, 3, seed=5)
+    with B200Backend(0) as be:
+        be.load_system(inp, [2, 3])
+        with pytest.raises(GwB200Error) as e:
+            be.run_g0w0(8, 4, [3, 2])
+        assert e.value.status == "GWB200_BAD_ARGUMENT"
+        with pytest.raises(GwB200Error) as e:
+            be.load_system(inp, [2, 2])
+        assert e.value.status == "GWB200_BAD_SHAPE"
+        be.load_system(inp)  # the full block again: any state list
+        r = be.run_g0w0(8, 4, [3, 2])
+        assert np.isfinite(r["sigma"][2]).all()
+
+
+def test_batch_of_state_bound_members():
+    from minigw_b200 import B200Backend, run_g0w0_batch
+    from minigw_b200.synthetic import make_input
+
+    specs = [(12, 2), (26, 4), (20, 3)]
+    inputs = [make_input(nmo, nocc, seed=800 + i) for i, (nmo, nocc) in enumerate(specs)]
+    states = [[inp.nocc - 1, inp.nocc] for inp in inputs]
+    bes = [B200Backend(0) for _ in inputs]
+    try:
+        for be, inp, st in zip(bes, inputs, states):
+            be.load_system(inp, st)
+        alone = [be.run_g0w0(16, 8, st, precision="mixed") for be, st in zip(bes, states)]
+        got = run_g0w0_batch(bes, 16, 8, states)
+        for a, s in zip(alone, got["sigma"]):
+            np.testing.assert_array_equal(s, a["sigma"])
+    finally:
+        for be in bes:
+            be.close()

@@ -43,7 +43,7 @@ def test_server_matches_backend_and_rejects_oversize():
     with B200Server(0, slots=2, hbm_budget_bytes=2 << 30) as srv:
         r = srv.wait(srv.submit(inp, 32, 12, [3, 4]))
         np.testing.assert_array_equal(r["sigma"], ref["sigma"])
-        big = make_input(60, 10, seed=4)  # (pq|o.) alone is 173 MB > the 1 MB slot below
+        big = make_input(60, 10, seed=4)  # V_ph alone is 2 MB > the 1 MB slot below
         with B200Server(0, slots=1, hbm_budget_bytes=1 << 20) as tiny:
             with pytest.raises(GwB200Error) as e:
                 tiny.submit(big, 16, 8, [9])
