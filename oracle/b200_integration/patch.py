@@ -25,11 +25,12 @@ DRIVER_BRANCH = '''#ifdef GW_HAS_B200_BACKEND
         std::unique_ptr<gwb200_handle, int (*)(gwb200_handle*)> guard(h, gwb200_destroy);
         const auto& eri = integrals.eri_tensor().data();
         const auto& vxc = integrals.vxc_matrix().data();
-        chk(gwb200_load_system(h, static_cast<int64_t>(orbitals.nmo()), static_cast<int64_t>(orbitals.nocc()),
-                               orbitals.energies().data(), eri.data(), vxc.data(), orbitals.fermi_energy()));
+        std::vector<int64_t> st(states.begin(), states.end());
+        chk(gwb200_load_system_states(h, static_cast<int64_t>(orbitals.nmo()), static_cast<int64_t>(orbitals.nocc()),
+                                      orbitals.energies().data(), eri.data(), vxc.data(), orbitals.fermi_energy(),
+                                      st.data(), static_cast<int64_t>(st.size())));
         std::vector<double> omega(omega_im.size());
         for (std::size_t f = 0; f < omega.size(); ++f) omega[f] = omega_im[f].imag();
-        std::vector<int64_t> st(states.begin(), states.end());
         gwb200_stats stats{};
         chk(gwb200_sigma_c(h, omega.data(), weights.data(), static_cast<int64_t>(omega.size()), st.data(),
                            static_cast<int64_t>(st.size()), settings.eta, GWB200_FP64,
