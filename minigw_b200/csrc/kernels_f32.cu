@@ -105,12 +105,14 @@ __global__ void k_build_tall32(int64_t n, int64_t m, int64_t n_pad, int64_t ld, 
 }
 
 // Diagonal block in FP64 (from the FP32 tall matrix), written back as FP32 L and FP32 L^{-1}.
+// One 64 x 65 FP64 tile: L in the lower triangle, Y = L^{-1} (lower too) transposed into the
+// upper triangle (Y[l][c] at T[c][l], l > c) with its diagonal in Yd, so 6 CTAs fit an SM.
 __global__ void __launch_bounds__(256) k_potrf_diag32(float* __restrict__ a, int64_t ld, int64_t stride, int64_t k,
                                                       float* __restrict__ linv, unsigned long long* err_pivot) {
     extern __shared__ double smem[];
     constexpr int L = kNb + 1;
     double* T = smem;
-    double* Y = smem + kNb * L;
+    double* Yd = smem + kNb * L;
     float* A = a + (size_t)blockIdx.x * stride + k * ld + k;
     const int tid = threadIdx.x;
     for (int idx = tid; idx < kNb * kNb; idx += blockDim.x) {
@@ -147,22 +149,22 @@ __global__ void __launch_bounds__(256) k_potrf_diag32(float* __restrict__ a, int
         for (int i = 0; i < kNb; ++i) {
             double sum = 0.0;
             if (i > col)
-                for (int l = col + part; l < i; l += 4) sum = fma(T[i * L + l], Y[l * L + col], sum);
+                for (int l = col + part; l < i; l += 4) sum = fma(T[i * L + l], l == col ? Yd[col] : T[col * L + l], sum);
             sum += __shfl_xor_sync(0xffffffffu, sum, 1);
             sum += __shfl_xor_sync(0xffffffffu, sum, 2);
             if (part == 0) {
-                double y;
-                if (i < col) y = 0.0;
-                else if (i == col) y = 1.0 / T[i * L + i];
-                else y = -sum / T[i * L + i];
-                Y[i * L + col] = y;
+                if (i == col) Yd[col] = 1.0 / T[i * L + i];
+                else if (i > col) T[col * L + i] = -sum / T[i * L + i];
             }
             __syncwarp();
         }
     }
     __syncthreads();
     float* out = linv + (size_t)blockIdx.x * kNb * kNb;
-    for (int idx = tid; idx < kNb * kNb; idx += blockDim.x) out[idx] = (float)Y[(idx / kNb) * L + idx % kNb];
+    for (int idx = tid; idx < kNb * kNb; idx += blockDim.x) {
+        const int r = idx / kNb, c = idx % kNb;
+        out[idx] = r > c ? (float)T[c * L + r] : (r == c ? (float)Yd[r] : 0.0f);
+    }
 }
 
 // Panel solve P <- P Linv^T on the tensor cores (3xTF32); RHS rows add their squared norms (FP64).
@@ -293,7 +295,7 @@ int launch_factor_chunk32(const TallGeometry& g, int64_t nf, float* a, float* li
                           unsigned long long* sched, int max_ctas) {
     const size_t smem_tile = 2 * 64 * kLdf * sizeof(float);
     const size_t smem_update = 4 * 64 * kLdkf * sizeof(float);
-    const size_t smem_potrf = 2 * kNb * (kNb + 1) * sizeof(double);
+    const size_t smem_potrf = (kNb * (kNb + 1) + kNb) * sizeof(double);
     GWB_CUDA(cudaFuncSetAttribute(k_trsm_panel32, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_tile));
     GWB_CUDA(cudaFuncSetAttribute(k_update32, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_update));
     GWB_CUDA(cudaFuncSetAttribute(k_potrf_diag32, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_potrf));
