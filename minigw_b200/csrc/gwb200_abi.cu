@@ -134,6 +134,10 @@ struct gwb200_handle {
     DevBuf batch_desc;  // BatchGroup tables of gwb200_run_g0w0_batch (when this handle leads a batch)
     BatchLane lanes[kMaxBatchLanes];  // streams + workspaces of the batches this handle leads
     cudaEvent_t batch_fork = nullptr;
+    cudaGraphExec_t batch_exec = nullptr;   // the last batch sequence captured as a CUDA graph
+    std::vector<int64_t> batch_graph_key;   // what it was captured for (sizes, plan, every pointer)
+    std::vector<int64_t> batch_graph_failed;  // a signature whose capture failed (issued eagerly)
+    int64_t batch_graph_launches = 0;
     PinnedBuf stage_in, stage_out;
     // cached frequency-chunk size for a repeated geometry (avoids cudaMemGetInfo per call)
     int64_t chunk_key[5] = {-1, -1, -1, -1, -1};
@@ -617,6 +621,7 @@ int gwb200_destroy(gwb200_handle* h) {
         if (l.stream) cudaStreamDestroy(l.stream);
     }
     if (h->batch_fork) cudaEventDestroy(h->batch_fork);
+    if (h->batch_exec) cudaGraphExecDestroy(h->batch_exec);
     for (auto& e : h->ev)
         if (e) cudaEventDestroy(e);
     if (h->own_stream) cudaStreamDestroy(h->own_stream);
@@ -1195,7 +1200,8 @@ int gwb200_run_g0w0_batch(gwb200_handle* const* systems, int64_t nsys, int64_t n
                                                                   w->lanes[0].sched.as<unsigned long long>(),
                                                                   w->err.as<unsigned long long>(), w->mem_limit <= 0));
 
-        // uploads through the lead handle's pinned staging buffer: grid, state lists, group tables
+        // the lead handle's pinned staging buffer, filled on the host before anything is issued:
+        // grid, every member's state list, group tables
         std::vector<double> omega((size_t)nfreq), weight((size_t)nfreq);
         transformed_legendre_grid(nfreq, omega.data(), weight.data());
         const size_t nb_groups = sizeof(BatchGroup) * groups.size();
@@ -1203,9 +1209,22 @@ int gwb200_run_g0w0_batch(gwb200_handle* const* systems, int64_t nsys, int64_t n
         char* sp = w->stage_in.as<char>();
         std::memcpy(sp, omega.data(), nb_om);
         std::memcpy(sp + nb_om, weight.data(), nb_om);
+        std::vector<size_t> st_off((size_t)nsys);
+        {
+            size_t off = 2 * nb_om;
+            for (int64_t i = 0; i < nsys; ++i) {
+                st_off[(size_t)i] = off;
+                std::memcpy(sp + off, states[i], sizeof(int64_t) * nstates[i]);
+                off += sizeof(int64_t) * nstates[i];
+            }
+        }
         std::memcpy(sp + 2 * nb_om + nb_states, groups.data(), nb_groups);
-        GWB_CUDA(cudaMemcpyAsync(w->batch_desc.p, sp + 2 * nb_om + nb_states, nb_groups, cudaMemcpyHostToDevice, s));
-        GWB_CUDA(cudaMemsetAsync(w->err.p, 0xFF, sizeof(unsigned long long), s));
+        for (int64_t i = 0; i < nsys; ++i) {  // every buffer the device sequence touches, sized now
+            gwb200_handle* h = hs[(size_t)i];
+            h->sigma.ensure(sizeof(double) * 2 * (size_t)h->nmo * nfreq);
+            h->qp.ensure(sizeof(double) * h->nmo);
+            h->qp_scratch.ensure(qp_scratch_bytes(nfreq, nstates[i]));
+        }
         // the lanes fork off the lead stream and join back onto it around each phase
         auto lane_stream = [&](int l) { return l == 0 ? s : w->lanes[l].stream; };
         auto fork = [&]() {
@@ -1218,29 +1237,30 @@ int gwb200_run_g0w0_batch(gwb200_handle* const* systems, int64_t nsys, int64_t n
                 GWB_CUDA(cudaStreamWaitEvent(s, w->lanes[l].done, 0));
             }
         };
-        GWB_CUDA(cudaEventRecord(w->ev[0], s));
-        int64_t launches = 0;
-        size_t off = 2 * nb_om;
-        fork();  // members' uploads, panel gathers and scale vectors, round robin over the lanes
-        for (int64_t i = 0; i < nsys; ++i) {
-            gwb200_handle* h = hs[(size_t)i];
-            cudaStream_t ls = lane_stream((int)(i % lanes));
-            const size_t nb_st = sizeof(int64_t) * nstates[i];
-            std::memcpy(sp + off, states[i], nb_st);
-            GWB_CUDA(cudaMemcpyAsync(h->omega.p, sp, nb_om, cudaMemcpyHostToDevice, ls));
-            GWB_CUDA(cudaMemcpyAsync(h->weight.p, sp + nb_om, nb_om, cudaMemcpyHostToDevice, ls));
-            GWB_CUDA(cudaMemcpyAsync(h->states.p, sp + off, nb_st, cudaMemcpyHostToDevice, ls));
-            off += nb_st;
-            if (h->bound_states.empty())
-                launches += launch_gather_panel(h->pqo.as<double>(), h->nmo, h->nocc, h->states.as<int64_t>(),
-                                                nstates[i], h->xt.as<double>(), ls);
-            launches += launch_scale_vectors(h->delta.as<double>(), h->n, make_geometry(h->n, ms[(size_t)i]).n_pad,
-                                             h->omega.as<double>(), nfreq, h->dvec.as<double>(), ls);
-        }
-        join();
-        GWB_CUDA(cudaEventRecord(w->ev[1], s));
         const BatchGroup* dgroups = w->batch_desc.as<BatchGroup>();
-        // one plan: each lane runs its chunks
+        // the device sequence in three phases: uploads and member preparation; the screening of a
+        // plan (each lane runs its chunks); members' contractions and QP updates
+        auto prefix = [&]() {
+            int64_t n_launch = 0;
+            GWB_CUDA(cudaMemcpyAsync(w->batch_desc.p, sp + 2 * nb_om + nb_states, nb_groups, cudaMemcpyHostToDevice, s));
+            GWB_CUDA(cudaMemsetAsync(w->err.p, 0xFF, sizeof(unsigned long long), s));
+            fork();
+            for (int64_t i = 0; i < nsys; ++i) {
+                gwb200_handle* h = hs[(size_t)i];
+                cudaStream_t ls = lane_stream((int)(i % lanes));
+                GWB_CUDA(cudaMemcpyAsync(h->omega.p, sp, nb_om, cudaMemcpyHostToDevice, ls));
+                GWB_CUDA(cudaMemcpyAsync(h->weight.p, sp + nb_om, nb_om, cudaMemcpyHostToDevice, ls));
+                GWB_CUDA(cudaMemcpyAsync(h->states.p, sp + st_off[(size_t)i], sizeof(int64_t) * nstates[i],
+                                         cudaMemcpyHostToDevice, ls));
+                if (h->bound_states.empty())
+                    n_launch += launch_gather_panel(h->pqo.as<double>(), h->nmo, h->nocc, h->states.as<int64_t>(),
+                                                    nstates[i], h->xt.as<double>(), ls);
+                n_launch += launch_scale_vectors(h->delta.as<double>(), h->n, make_geometry(h->n, ms[(size_t)i]).n_pad,
+                                                 h->omega.as<double>(), nfreq, h->dvec.as<double>(), ls);
+            }
+            join();
+            return n_launch;
+        };
         auto run_plan = [&](size_t c) {
             int64_t n_launch = 0;
             fork();
@@ -1250,36 +1270,124 @@ int gwb200_run_g0w0_batch(gwb200_handle* const* systems, int64_t nsys, int64_t n
             join();
             return n_launch;
         };
+        auto suffix = [&]() {
+            gwb200_stats scratch{};
+            fork();
+            for (int64_t i = 0; i < nsys; ++i) {
+                hs[(size_t)i]->stream = lane_stream((int)(i % lanes));
+                contract_on_device(hs[(size_t)i], nfreq, nstates[i], &scratch);
+                qp_on_device(hs[(size_t)i], nfreq, npade, nstates[i]);
+            }
+            join();
+            return scratch.kernel_launches + 2 * nsys;
+        };
+
+        // CUDA graph of the whole sequence for a repeated batch (one plan, nothing to time):
+        // captured on the first such call, replayed while every pointer it holds is unchanged.
+        // GWB200_BATCH_GRAPH=0 issues the launches one by one.
+        const char* graph_env = std::getenv("GWB200_BATCH_GRAPH");
+        const bool want_graph = cands.size() == 1 && !(graph_env && std::strcmp(graph_env, "0") == 0);
+        std::vector<int64_t> gkey;
+        if (want_graph) {
+            auto put = [&](const void* ptr) { gkey.push_back((int64_t)reinterpret_cast<intptr_t>(ptr)); };
+            gkey = key;
+            gkey.insert(gkey.end(), cands[0].begin(), cands[0].end());
+            gkey.push_back(npade);
+            gkey.push_back(lanes);
+            gkey.push_back(lane_ctas);
+            gkey.insert(gkey.end(), variants[0].begin(), variants[0].end());
+            for (int64_t i = 0; i < nsys; ++i) {
+                const gwb200_handle* h = hs[(size_t)i];
+                put(h);
+                gkey.push_back(nstates[i]);
+                gkey.insert(gkey.end(), states[i], states[i] + nstates[i]);
+                gkey.push_back(h->bound_states.empty() ? 0 : 1);
+                for (const DevBuf* b : {&h->pqo, &h->v, &h->xt, &h->dvec, &h->qall, &h->sigma, &h->qp, &h->qp_scratch,
+                                        &h->omega, &h->weight, &h->states, &h->delta, &h->mo, &h->sigx, &h->vxc_diag})
+                    put(b->p);
+            }
+            put(w->batch_desc.p);
+            put(w->err.p);
+            put(w->stage_in.p);
+            put(w->batch_fork);
+            for (int l = 0; l < lanes; ++l) {
+                const BatchLane& ln = w->lanes[l];
+                for (const DevBuf* b : {&ln.a, &ln.linv, &ln.qacc, &ln.panel, &ln.sched}) put(b->p);
+                put(ln.stream);
+                put(ln.done);
+            }
+        }
+        int64_t launches = 0;
         size_t pick = 0;
-        if (cands.size() > 1) {  // time each candidate plan once, keep the fastest for this signature
-            float best = std::numeric_limits<float>::infinity();
-            for (size_t c = 0; c < cands.size(); ++c) {
-                GWB_CUDA(cudaEventRecord(w->ev[4], s));
-                run_plan(c);
-                GWB_CUDA(cudaEventRecord(w->ev[5], s));
-                GWB_CUDA(cudaEventSynchronize(w->ev[5]));
-                const float t = elapsed(w->ev[4], w->ev[5]);
-                if (t < best) {
-                    best = t;
-                    pick = c;
+        bool graphed = false;
+        if (want_graph && gkey != w->batch_graph_failed) {
+            if (!w->batch_exec || gkey != w->batch_graph_key) {
+                if (w->batch_exec) cudaGraphExecDestroy(w->batch_exec);
+                w->batch_exec = nullptr;
+                w->batch_graph_key.clear();
+                cudaGraph_t graph = nullptr;
+                bool capturing = false;
+                try {
+                    GWB_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeRelaxed));
+                    capturing = true;
+                    int64_t n = prefix();
+                    n += run_plan(0);
+                    n += suffix();
+                    capturing = false;
+                    GWB_CUDA(cudaStreamEndCapture(s, &graph));
+                    GWB_CUDA(cudaGraphInstantiate(&w->batch_exec, graph, 0));
+                    cudaGraphDestroy(graph);
+                    w->batch_graph_key = gkey;
+                    w->batch_graph_launches = n;
+                } catch (...) {
+                    // not capturable here: remember, and issue this signature's launches one by one
+                    if (capturing) {
+                        cudaGraph_t g2 = nullptr;
+                        cudaStreamEndCapture(s, &g2);
+                        if (g2) cudaGraphDestroy(g2);
+                    }
+                    if (graph) cudaGraphDestroy(graph);
+                    if (w->batch_exec) cudaGraphExecDestroy(w->batch_exec);
+                    w->batch_exec = nullptr;
+                    cudaGetLastError();
+                    w->batch_graph_failed = gkey;
                 }
             }
-            std::lock_guard<std::mutex> lk(g_batch_mu);
-            g_batch_plans[key] = cands[pick];
+            if (w->batch_exec) {
+                GWB_CUDA(cudaEventRecord(w->ev[0], s));
+                GWB_CUDA(cudaGraphLaunch(w->batch_exec, s));
+                GWB_CUDA(cudaEventRecord(w->ev[3], s));
+                launches = w->batch_graph_launches;
+                graphed = true;
+            }
         }
-        GWB_CUDA(cudaEventRecord(w->ev[4], s));
-        launches += run_plan(pick);
-        GWB_CUDA(cudaEventRecord(w->ev[2], s));
+        if (!graphed) {
+            GWB_CUDA(cudaEventRecord(w->ev[0], s));
+            launches += prefix();
+            GWB_CUDA(cudaEventRecord(w->ev[1], s));
+            if (cands.size() > 1) {  // time each candidate plan once, keep the fastest for this signature
+                float best = std::numeric_limits<float>::infinity();
+                for (size_t c = 0; c < cands.size(); ++c) {
+                    GWB_CUDA(cudaEventRecord(w->ev[4], s));
+                    run_plan(c);
+                    GWB_CUDA(cudaEventRecord(w->ev[5], s));
+                    GWB_CUDA(cudaEventSynchronize(w->ev[5]));
+                    const float t = elapsed(w->ev[4], w->ev[5]);
+                    if (t < best) {
+                        best = t;
+                        pick = c;
+                    }
+                }
+                std::lock_guard<std::mutex> lk(g_batch_mu);
+                g_batch_plans[key] = cands[pick];
+            }
+            GWB_CUDA(cudaEventRecord(w->ev[4], s));
+            launches += run_plan(pick);
+            GWB_CUDA(cudaEventRecord(w->ev[2], s));
+            launches += suffix();
+            GWB_CUDA(cudaEventRecord(w->ev[3], s));
+        }
         st->kernel_launches = launches;
-        fork();  // members' contractions and QP updates, round robin over the lanes
-        for (int64_t i = 0; i < nsys; ++i) {
-            hs[(size_t)i]->stream = lane_stream((int)(i % lanes));
-            contract_on_device(hs[(size_t)i], nfreq, nstates[i], st);
-            qp_on_device(hs[(size_t)i], nfreq, npade, nstates[i]);
-            st->kernel_launches += 2;
-        }
-        join();
-        GWB_CUDA(cudaEventRecord(w->ev[3], s));
         // results and the pivot word back in one synchronisation
         size_t nb_out = sizeof(unsigned long long);
         for (gwb200_handle* h : hs) nb_out += sizeof(double) * (2 * (size_t)h->nmo * nfreq + h->nmo);
@@ -1322,10 +1430,14 @@ int gwb200_run_g0w0_batch(gwb200_handle* const* systems, int64_t nsys, int64_t n
         st->frequency_chunks = (int64_t)chunks[pick].size();
         st->nph = nmax;
         st->ncols = mmax;
-        st->device_ms_gather = elapsed(w->ev[0], w->ev[1]);
-        st->device_ms_screening = elapsed(w->ev[4], w->ev[2]);
-        st->device_ms_contract = elapsed(w->ev[2], w->ev[3]);
         st->device_ms_total = elapsed(w->ev[0], w->ev[3]);
+        if (graphed) {  // one graph launch: no phase split, the whole sequence counts as screening
+            st->device_ms_screening = st->device_ms_total;
+        } else {
+            st->device_ms_gather = elapsed(w->ev[0], w->ev[1]);
+            st->device_ms_screening = elapsed(w->ev[4], w->ev[2]);
+            st->device_ms_contract = elapsed(w->ev[2], w->ev[3]);
+        }
         if (nbuckets_out) *nbuckets_out = (int64_t)cands[pick].size();
     });
 }
