@@ -1283,7 +1283,8 @@ int gwb200_run_g0w0_batch(gwb200_handle* const* systems, int64_t nsys, int64_t n
         };
 
         // CUDA graph of the whole sequence for a repeated batch (one plan, nothing to time):
-        // captured on the first such call, replayed while every pointer it holds is unchanged.
+        // captured on the first such call, replayed while every pointer it holds and every scalar
+        // it passes by value is unchanged.
         // GWB200_BATCH_GRAPH=0 issues the launches one by one.
         const char* graph_env = std::getenv("GWB200_BATCH_GRAPH");
         const bool want_graph = cands.size() == 1 && !(graph_env && std::strcmp(graph_env, "0") == 0);
@@ -1299,6 +1300,10 @@ int gwb200_run_g0w0_batch(gwb200_handle* const* systems, int64_t nsys, int64_t n
             for (int64_t i = 0; i < nsys; ++i) {
                 const gwb200_handle* h = hs[(size_t)i];
                 put(h);
+                // scalars the kernels take by value (E_F for the contraction and the QP update)
+                int64_t fermi_bits = 0;
+                std::memcpy(&fermi_bits, &h->fermi, sizeof(fermi_bits));
+                gkey.insert(gkey.end(), {fermi_bits, h->n, h->nmo, h->nocc});
                 gkey.push_back(nstates[i]);
                 gkey.insert(gkey.end(), states[i], states[i] + nstates[i]);
                 gkey.push_back(h->bound_states.empty() ? 0 : 1);
