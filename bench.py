@@ -662,8 +662,50 @@ def run_batch(args):
         result["mixed_vs_fp64"] = {"sigma_c_max_rel_err": rel, "qp_max_abs_err_meV": dqp * 27.211386245988e3}
     for be in bes:
         be.close()
+    if not args.no_cpu_baseline:
+        cb = batch_cpu_baseline(args, nmos, nfreq, npade)
+        if cb:
+            result["cpu_baseline"] = cb
     print(json.dumps(result))
     return 0
+
+
+def batch_cpu_baseline(args, nmos, nfreq, npade, sample=8):
+    """The reference's own CPU path on the batch: one (f_n, f') pair (one W_c build plus the
+    HOMO/LUMO panel contractions) timed on `sample` molecules spread over the size range (the
+    smallest and the largest included), the pair time of every molecule interpolated in log-log
+    between them, and solve time = nfreq^2 x pair time summed over all molecules (extrapolated, as
+    for the single-molecule workloads)."""
+    import numpy as np
+
+    import oracle
+    from minigw_b200 import generate_transformed_legendre_grid
+    from minigw_b200.synthetic import Workload, make_input_on_device
+
+    if not oracle.Ref.available:
+        return None
+    threads = os.cpu_count() or 1
+    om, w = generate_transformed_legendre_grid(nfreq)
+    occ = [max(1, int(round(nmo / 6))) for nmo in nmos]
+    nph = [o * (nmo - o) for nmo, o in zip(nmos, occ)]
+    order = sorted(range(len(nmos)), key=lambda i: nph[i])
+    picks = sorted({order[int(round(k * (len(order) - 1) / max(1, sample - 1)))] for k in range(sample)})
+    xs, ys, t0 = [], [], time.perf_counter()
+    for i in picks:
+        inp = make_input_on_device(nmos[i], occ[i], seed=args.seed + 2000 + i, device=0, pin=False)
+        wl = Workload(f"cfg4-{i}", nmos[i], occ[i], nfreq, npade, (occ[i] - 1, occ[i]))
+        cb = cpu_reference_sample(inp, wl, om, w, 1, threads)
+        xs.append(np.log(nph[i]))
+        ys.append(np.log(cb["seconds_per_pair"]))
+        del inp
+    # the sample spans the smallest and the largest molecule: interpolate log time in log nph
+    total_s = sum(nfreq ** 2 * float(np.exp(np.interp(np.log(n), xs, ys))) for n in nph)
+    return {"value": len(nmos) / total_s, "unit": "GW solves/s", "cores": threads, "kind": "reference",
+            "sample": f"one (f_n, f') pair of each of {len(picks)} molecules spread over nph "
+                      f"{min(nph)}..{max(nph)} through the reference's own code (oracle/_ref, blas-lapack backend, "
+                      f"{threads} OpenBLAS threads; {time.perf_counter() - t0:.0f} s of sampling); pair time of "
+                      f"the others interpolated in log-log; solve time = nfreq^2 x pair time, summed over the "
+                      f"{len(nmos)} molecules (extrapolated)"}
 
 
 def main() -> int:
