@@ -3,8 +3,10 @@ OUT_DIR (a temporary build directory; nothing is written into the repository or 
 
     python oracle/b200_integration/patch.py REF_ROOT OUT_DIR
 
-The insertions are the maintainer-side binding shown in INTEGRATION.md; they are placed at
-anchors found in the reference files and the script fails if an anchor is missing.
+The insertions are the maintainer-side binding: the `b200` case of make_local_linalg_backend
+and, in compute_sigma_c_with_backend, a branch that loads the system with the state list and
+fills Sigma_c(iw) with one gwb200_sigma_c call.  They are placed at anchors found in the reference
+files, and the script fails if an anchor is missing.
 """
 import sys
 from pathlib import Path

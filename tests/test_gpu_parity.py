@@ -273,7 +273,7 @@ REF_B200 = ROOT / "oracle" / "_ref" / "gw_ref_b200"
 @pytest.mark.skipif(not REF_B200.exists(), reason="the reference executable with the b200 backend was not built")
 def test_reference_executable_with_b200_backend(tmp_path):
     """The reference's own `gw` (its main, CLI, backend factory, run_g0w0 and writers) with the
-    b200 backend registered as INTEGRATION.md describes: `--linalg-backend b200` on the H2O input
+    b200 backend registered (factory case + driver branch): `--linalg-backend b200` on the H2O input
     reproduces the reference's committed regression outputs."""
     out = tmp_path / "out"
     r = subprocess.run([str(REF_B200), "--linalg-backend", "b200", "--input-dir", str(GOLDEN / "h2o"), "--output-dir",
