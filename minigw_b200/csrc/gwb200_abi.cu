@@ -1027,6 +1027,7 @@ int gwb200_run_g0w0_batch(gwb200_handle* const* systems, int64_t nsys, int64_t n
                           double* const* qp_out, int64_t* nbuckets_out, gwb200_stats* stats) {
     return guarded([&] {
         if (!systems || nsys <= 0) fail(GWB200_BAD_ARGUMENT, "empty batch");
+        if (nsys > 65535) fail(GWB200_BAD_SHAPE, "at most 65535 systems per batch");  // one grid row per member run
         if (!states || !nstates) fail(GWB200_BAD_ARGUMENT, "null state lists");
         if (nfreq <= 0) fail(GWB200_BAD_SHAPE, "--freq-points must be positive");
         if (npade <= 0) fail(GWB200_BAD_SHAPE, "--pade-params must be positive");
@@ -1116,7 +1117,15 @@ int gwb200_run_g0w0_batch(gwb200_handle* const* systems, int64_t nsys, int64_t n
         GWB_CUDA(cudaMemGetInfo(&free_b, &total_b));
         size_t held = 0;
         for (const BatchLane& l : w->lanes) held += l.bytes();
-        const size_t avail = free_b + held;
+        size_t avail = free_b + held;
+        if (w->mem_limit > 0) {  // a capped lead handle: its cap minus what it already holds besides the lanes
+            size_t resident = (size_t)1 << 20;
+            for (const DevBuf* b : {&w->pqo, &w->xdiag, &w->v, &w->xt, &w->dvec, &w->qall, &w->sigma, &w->qp_scratch,
+                                    &w->a, &w->linv, &w->qacc, &w->panel32})
+                resident += b->bytes;
+            const size_t lim = (size_t)w->mem_limit;
+            avail = std::min(avail, lim > resident ? lim - resident : (size_t)0);
+        }
         const char* mode_env = std::getenv("GWB200_BATCH_PLAN");
         const std::string mode = mode_env ? mode_env : "tuned";
         std::vector<int64_t> key = {(int64_t)w->device, (int64_t)precision, (int64_t)oz, (int64_t)mixed_tc, nfreq,
