@@ -994,6 +994,114 @@ std::vector<int> batch_order(const std::vector<int64_t>& ns, const std::vector<i
     });
     return order;
 }
+
+// Lanes of a batch: GWB200_BATCH_STREAMS concurrent streams (default 4, at most one per
+// molecule), each with its own workspaces; GWB200_BATCH_SHARE_SMS=1 caps each lane's persistent
+// update kernels at SMs / lanes CTAs (default: every lane's grid covers the GPU; those kernels take
+// their work units from a counter and never wait on one another, so they need not be co-resident).
+// Measured on the 64-molecule config-4 batch (mixed): 1 lane 261-274 ms, 2 lanes 233-244, 4 lanes
+// 221-224.  Returns the lane count; *ctas the persistent-grid cap (0: none).
+int batch_lanes(const gwb200_handle* w, int64_t nsys, int* ctas) {
+    int lanes = kMaxBatchLanes;
+    if (const char* e = std::getenv("GWB200_BATCH_STREAMS")) lanes = std::atoi(e);
+    lanes = std::max(1, std::min<int>({kMaxBatchLanes, lanes, (int)nsys}));
+    const char* share_env = std::getenv("GWB200_BATCH_SHARE_SMS");
+    *ctas = w->persistent_ctas;
+    if (lanes > 1 && share_env && std::strcmp(share_env, "1") == 0) {
+        int sms = 148;
+        GWB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, w->device));
+        *ctas = std::max(1, (w->persistent_ctas > 0 ? w->persistent_ctas : sms) / lanes);
+    }
+    return lanes;
+}
+
+// Device bytes the batch's lane workspaces may take: free memory plus what the lanes hold, and,
+// for a capped lead handle, its cap minus what it holds besides the lanes.
+size_t batch_avail(const gwb200_handle* w) {
+    size_t free_b = 0, total_b = 0;
+    GWB_CUDA(cudaMemGetInfo(&free_b, &total_b));
+    size_t held = 0;
+    for (const BatchLane& l : w->lanes) held += l.bytes();
+    size_t avail = free_b + held;
+    if (w->mem_limit > 0) {
+        size_t resident = (size_t)1 << 20;
+        for (const DevBuf* b : {&w->pqo, &w->xdiag, &w->v, &w->xt, &w->dvec, &w->qall, &w->sigma, &w->qp_scratch, &w->a,
+                                &w->linv, &w->qacc, &w->panel32})
+            resident += b->bytes;
+        const size_t lim = (size_t)w->mem_limit;
+        avail = std::min(avail, lim > resident ? lim - resident : (size_t)0);
+    }
+    return avail;
+}
+
+// Bucket plans to run: GWB200_BATCH_PLAN=tuned (default: the plan cached for this signature, else
+// the cost model's plans for three latency weights plus one bucket per molecule, to be timed),
+// =model (the cost model alone), =each (one bucket per molecule), =single (one bucket).
+std::vector<std::vector<int64_t>> batch_candidates(const std::vector<int64_t>& key, const std::vector<int64_t>& n_sorted,
+                                                   const std::vector<int64_t>& m_sorted, int64_t nfreq, bool mixed,
+                                                   size_t lane_budget) {
+    const int64_t nsys = (int64_t)n_sorted.size();
+    const char* mode_env = std::getenv("GWB200_BATCH_PLAN");
+    const std::string mode = mode_env ? mode_env : "tuned";
+    if (mode == "each") return {std::vector<int64_t>((size_t)nsys, 1)};
+    if (mode == "single") return {{nsys}};
+    if (mode == "tuned") {
+        std::lock_guard<std::mutex> lk(g_batch_mu);
+        auto it = g_batch_plans.find(key);
+        if (it != g_batch_plans.end()) return {it->second};
+    }
+    std::vector<std::vector<int64_t>> cands;
+    const double tau = batch_step_us(mixed), rate = batch_tflops(mixed);
+    for (double mult : (mode == "tuned" ? std::vector<double>{1.0, 0.25, 4.0} : std::vector<double>{1.0})) {
+        std::vector<int64_t> p = plan_buckets(n_sorted, m_sorted, nfreq, mixed, lane_budget, tau * mult, rate);
+        if (std::find(cands.begin(), cands.end(), p) == cands.end()) cands.push_back(p);
+    }
+    if (mode == "tuned") {
+        std::vector<int64_t> each((size_t)nsys, 1);
+        if (std::find(cands.begin(), cands.end(), each) == cands.end()) cands.push_back(each);
+    }
+    return cands;
+}
+
+// What a captured batch graph depends on: the plan signature and plan, the scalars its kernels take
+// by value (E_F, sizes, Pade order, lanes, update variants) and every device pointer and stream it
+// uses.  A replay is valid exactly while this is unchanged.
+std::vector<int64_t> batch_graph_key(const gwb200_handle* w, const std::vector<gwb200_handle*>& hs,
+                                     const std::vector<int64_t>& key, const std::vector<int64_t>& plan, int64_t npade,
+                                     int lanes, int lane_ctas, const std::vector<int>& variants,
+                                     const int64_t* const* states, const int64_t* nstates) {
+    std::vector<int64_t> gkey = key;
+    auto put = [&](const void* ptr) { gkey.push_back((int64_t)reinterpret_cast<intptr_t>(ptr)); };
+    gkey.insert(gkey.end(), plan.begin(), plan.end());
+    gkey.push_back(npade);
+    gkey.push_back(lanes);
+    gkey.push_back(lane_ctas);
+    gkey.insert(gkey.end(), variants.begin(), variants.end());
+    for (size_t i = 0; i < hs.size(); ++i) {
+        const gwb200_handle* h = hs[i];
+        put(h);
+        int64_t fermi_bits = 0;
+        std::memcpy(&fermi_bits, &h->fermi, sizeof(fermi_bits));
+        gkey.insert(gkey.end(), {fermi_bits, h->n, h->nmo, h->nocc});
+        gkey.push_back(nstates[i]);
+        gkey.insert(gkey.end(), states[i], states[i] + nstates[i]);
+        gkey.push_back(h->bound_states.empty() ? 0 : 1);
+        for (const DevBuf* b : {&h->pqo, &h->v, &h->xt, &h->dvec, &h->qall, &h->sigma, &h->qp, &h->qp_scratch, &h->omega,
+                                &h->weight, &h->states, &h->delta, &h->mo, &h->sigx, &h->vxc_diag})
+            put(b->p);
+    }
+    put(w->batch_desc.p);
+    put(w->err.p);
+    put(w->stage_in.p);
+    put(w->batch_fork);
+    for (int l = 0; l < lanes; ++l) {
+        const BatchLane& ln = w->lanes[l];
+        for (const DevBuf* b : {&ln.a, &ln.linv, &ln.qacc, &ln.panel, &ln.sched}) put(b->p);
+        put(ln.stream);
+        put(ln.done);
+    }
+    return gkey;
+}
 } // namespace
 
 int gwb200_plan_buckets(int64_t nsys, const int64_t* nph, const int64_t* ncols, int64_t nfreq, int precision,
@@ -1087,79 +1195,23 @@ int gwb200_run_g0w0_batch(gwb200_handle* const* systems, int64_t nsys, int64_t n
             nb_states += sizeof(int64_t) * nstates[i];
         }
         w->err.ensure(sizeof(unsigned long long));
-        // lanes: GWB200_BATCH_STREAMS concurrent streams (default 4, at most one per molecule), each
-        // with its own workspaces; GWB200_BATCH_SHARE_SMS=1 caps each lane's persistent update
-        // kernels at SMs / lanes CTAs (default: every lane's grid covers the GPU; those kernels take
-        // their work units from a counter and never wait on one another, so they need not be
-        // co-resident).  Measured on the 64-molecule config-4 batch (mixed): 1 lane 261-274 ms,
-        // 2 lanes 233-244, 4 lanes 221-224.
-        int lanes = kMaxBatchLanes;
-        if (const char* e = std::getenv("GWB200_BATCH_STREAMS")) lanes = std::atoi(e);
-        lanes = std::max(1, std::min<int>({kMaxBatchLanes, lanes, (int)nsys}));
-        const char* share_env = std::getenv("GWB200_BATCH_SHARE_SMS");
-        const bool share = share_env && std::strcmp(share_env, "1") == 0;
-        int lane_ctas = w->persistent_ctas;
-        if (lanes > 1 && share) {
-            int sms = 148;
-            GWB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, w->device));
-            lane_ctas = std::max(1, (w->persistent_ctas > 0 ? w->persistent_ctas : sms) / lanes);
-        }
+        int lane_ctas = 0;
+        const int lanes = batch_lanes(w, nsys, &lane_ctas);
 
-        // plans: cached per batch signature, else timed candidates (GWB200_BATCH_PLAN=tuned, the
-        // default), the cost model alone (=model), one bucket per molecule (=each), one bucket (=single)
+        // plans over the molecules sorted by size (batch_candidates)
         const std::vector<int> order = batch_order(ns, ms);
         std::vector<int64_t> n_sorted, m_sorted;
         for (int i : order) {
             n_sorted.push_back(ns[(size_t)i]);
             m_sorted.push_back(ms[(size_t)i]);
         }
-        size_t free_b = 0, total_b = 0;
-        GWB_CUDA(cudaMemGetInfo(&free_b, &total_b));
-        size_t held = 0;
-        for (const BatchLane& l : w->lanes) held += l.bytes();
-        size_t avail = free_b + held;
-        if (w->mem_limit > 0) {  // a capped lead handle: its cap minus what it already holds besides the lanes
-            size_t resident = (size_t)1 << 20;
-            for (const DevBuf* b : {&w->pqo, &w->xdiag, &w->v, &w->xt, &w->dvec, &w->qall, &w->sigma, &w->qp_scratch,
-                                    &w->a, &w->linv, &w->qacc, &w->panel32})
-                resident += b->bytes;
-            const size_t lim = (size_t)w->mem_limit;
-            avail = std::min(avail, lim > resident ? lim - resident : (size_t)0);
-        }
-        const char* mode_env = std::getenv("GWB200_BATCH_PLAN");
-        const std::string mode = mode_env ? mode_env : "tuned";
+        const size_t avail = batch_avail(w);
         std::vector<int64_t> key = {(int64_t)w->device, (int64_t)precision, (int64_t)oz, (int64_t)mixed_tc, nfreq,
                                     (int64_t)lanes, (int64_t)lane_ctas};
         key.insert(key.end(), n_sorted.begin(), n_sorted.end());
         key.insert(key.end(), m_sorted.begin(), m_sorted.end());
-        std::vector<std::vector<int64_t>> cands;
-        bool cached = false;
-        if (mode == "each") {
-            cands.push_back(std::vector<int64_t>((size_t)nsys, 1));
-        } else if (mode == "single") {
-            cands.push_back({nsys});
-        } else {
-            if (mode == "tuned") {
-                std::lock_guard<std::mutex> lk(g_batch_mu);
-                auto it = g_batch_plans.find(key);
-                if (it != g_batch_plans.end()) {
-                    cands.push_back(it->second);
-                    cached = true;
-                }
-            }
-            if (!cached) {
-                const double tau = batch_step_us(mixed), rate = batch_tflops(mixed);
-                const size_t b0 = (size_t)(0.85 * (double)avail / lanes);
-                for (double mult : (mode == "tuned" ? std::vector<double>{1.0, 0.25, 4.0} : std::vector<double>{1.0})) {
-                    std::vector<int64_t> p = plan_buckets(n_sorted, m_sorted, nfreq, mixed, b0, tau * mult, rate);
-                    if (std::find(cands.begin(), cands.end(), p) == cands.end()) cands.push_back(p);
-                }
-                if (mode == "tuned") {
-                    std::vector<int64_t> each((size_t)nsys, 1);
-                    if (std::find(cands.begin(), cands.end(), each) == cands.end()) cands.push_back(each);
-                }
-            }
-        }
+        const std::vector<std::vector<int64_t>> cands =
+            batch_candidates(key, n_sorted, m_sorted, nfreq, mixed, (size_t)(0.85 * (double)avail / lanes));
         // chunks of every candidate inside one budget (all candidates share the workspaces)
         const TallGeometry gmax = make_geometry(n_sorted.back(), *std::max_element(m_sorted.begin(), m_sorted.end()));
         if (batch_bytes_per_matrix(gmax, mixed, oz) > avail)
@@ -1297,40 +1349,9 @@ int gwb200_run_g0w0_batch(gwb200_handle* const* systems, int64_t nsys, int64_t n
         // GWB200_BATCH_GRAPH=0 issues the launches one by one.
         const char* graph_env = std::getenv("GWB200_BATCH_GRAPH");
         const bool want_graph = cands.size() == 1 && !(graph_env && std::strcmp(graph_env, "0") == 0);
-        std::vector<int64_t> gkey;
-        if (want_graph) {
-            auto put = [&](const void* ptr) { gkey.push_back((int64_t)reinterpret_cast<intptr_t>(ptr)); };
-            gkey = key;
-            gkey.insert(gkey.end(), cands[0].begin(), cands[0].end());
-            gkey.push_back(npade);
-            gkey.push_back(lanes);
-            gkey.push_back(lane_ctas);
-            gkey.insert(gkey.end(), variants[0].begin(), variants[0].end());
-            for (int64_t i = 0; i < nsys; ++i) {
-                const gwb200_handle* h = hs[(size_t)i];
-                put(h);
-                // scalars the kernels take by value (E_F for the contraction and the QP update)
-                int64_t fermi_bits = 0;
-                std::memcpy(&fermi_bits, &h->fermi, sizeof(fermi_bits));
-                gkey.insert(gkey.end(), {fermi_bits, h->n, h->nmo, h->nocc});
-                gkey.push_back(nstates[i]);
-                gkey.insert(gkey.end(), states[i], states[i] + nstates[i]);
-                gkey.push_back(h->bound_states.empty() ? 0 : 1);
-                for (const DevBuf* b : {&h->pqo, &h->v, &h->xt, &h->dvec, &h->qall, &h->sigma, &h->qp, &h->qp_scratch,
-                                        &h->omega, &h->weight, &h->states, &h->delta, &h->mo, &h->sigx, &h->vxc_diag})
-                    put(b->p);
-            }
-            put(w->batch_desc.p);
-            put(w->err.p);
-            put(w->stage_in.p);
-            put(w->batch_fork);
-            for (int l = 0; l < lanes; ++l) {
-                const BatchLane& ln = w->lanes[l];
-                for (const DevBuf* b : {&ln.a, &ln.linv, &ln.qacc, &ln.panel, &ln.sched}) put(b->p);
-                put(ln.stream);
-                put(ln.done);
-            }
-        }
+        const std::vector<int64_t> gkey = want_graph ? batch_graph_key(w, hs, key, cands[0], npade, lanes, lane_ctas,
+                                                                        variants[0], states, nstates)
+                                                     : std::vector<int64_t>{};
         int64_t launches = 0;
         size_t pick = 0;
         bool graphed = false;
