@@ -56,7 +56,7 @@ void print_usage(const char* exe) {
               << "  --state N                    1-based orbital index to calculate [default: 5]\n"
               << "  --states A,B,...             1-based orbital indices to calculate (b200 extension)\n"
               << "  --all-states                 Calculate all diagonal states\n"
-              << "  --eta VALUE                  Infinitesimal broadening [default: 0.0; b200 requires 0]\n"
+              << "  --eta VALUE                  Infinitesimal broadening [default: 0.0; nonzero: complex symmetric path, fp64 only]\n"
               << "  --linalg-backend NAME        b200 [default: b200]\n"
               << "  --precision MODE             fp64 or mixed [default: fp64]\n"
               << "  --frequency-parallel MODE    auto or serial (the device batches all frequencies)\n"
