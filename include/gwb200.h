@@ -257,21 +257,25 @@ int gwb200_server_destroy(gwb200_server* s);
 
 /* ---- Batched solves: many molecules of uneven size in shared launches (no reference counterpart;
  * the reference runs one molecule per process, src/main.cpp:68-103) ----
- * systems[i] holds molecule i (gwb200_load_system), all on one device, no handle twice.  Every
- * molecule is solved as gwb200_run_g0w0(systems[i], nfreq, npade, states[i], nstates[i], 0, precision,
- * ...) would solve it, eta = 0.  The molecules are sorted by size and grouped into buckets; a
- * bucket's matrices (every member x every frequency) take the bucket's largest geometry (identity /
- * zero padding, exact) and are factored by one launch sequence.  Bucket boundaries: a cost model
- * (block-step latency against padded work) gives candidate plans, timed on the first call of a batch
- * signature (sorted sizes, nfreq, precision); the fastest is kept for later calls in the process
- * (GWB200_BATCH_PLAN=model|each|single skips the timing).  All work runs on systems[0]'s stream
- * with systems[0]'s workspaces.  Outputs (either array, or any entry, may be NULL): sigma_out[i]
- * nmo_i x nfreq complex row-major, qp_out[i] nmo_i (NaN where not requested).  *nbuckets_out: the
- * buckets used.  stats: totals of the call (flops at the true sizes, device times, launches). */
-int gwb200_run_g0w0_batch(gwb200_handle* const* systems, int64_t nsys, int64_t nfreq, int64_t npade,
-                          const int64_t* const* states, const int64_t* nstates, int precision,
-                          double* const* sigma_out, double* const* qp_out, int64_t* nbuckets_out,
-                          gwb200_stats* stats);
+ * systems[i] holds molecule i (gwb200_load_system or gwb200_load_system_states), all on one device,
+ * no handle twice, at most 65535.  Molecule i is solved as gwb200_run_g0w0(systems[i], nfreq[i],
+ * npade[i], states[i], nstates[i], 0, precision, ...) would solve it (eta = 0; frequency and Pade
+ * counts may differ between molecules).  The molecules are sorted by size and grouped into
+ * buckets; a bucket's matrices (every member x every one of its frequencies) take the bucket's
+ * largest geometry (identity / zero padding, exact) and are factored by shared launches on up to 4
+ * streams.  Bucket boundaries: a cost model (block-step latency against padded work) gives
+ * candidate plans, timed on the first call of a batch signature (sorted sizes and frequency
+ * counts, precision); the fastest is kept for later calls in the process
+ * (GWB200_BATCH_PLAN=model|each|single skips the timing).  A repeated call with one plan replays
+ * a CUDA graph of the whole sequence while no buffer has moved.  All work runs on systems[0]'s
+ * stream with systems[0]'s workspaces.  Outputs (either array, or any entry, may be NULL):
+ * sigma_out[i] nmo_i x nfreq[i] complex row-major, qp_out[i] nmo_i (NaN where not requested).
+ * *nbuckets_out: the buckets used.  stats: totals of the call (flops at the true sizes, device
+ * times, launches).  Each result is bit-identical to the molecule's own gwb200_run_g0w0. */
+int gwb200_run_g0w0_batch(gwb200_handle* const* systems, int64_t nsys, const int64_t* nfreq,
+                          const int64_t* npade, const int64_t* const* states, const int64_t* nstates,
+                          int precision, double* const* sigma_out, double* const* qp_out,
+                          int64_t* nbuckets_out, gwb200_stats* stats);
 
 /* The cost model's bucket plan alone (host only, no device): bucket_of[i] in 0..*nbuckets-1 for
  * molecules of nph[i] x ncols[i] (buckets in ascending size), budget_bytes of device memory for the

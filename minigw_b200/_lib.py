@@ -125,7 +125,7 @@ def _load() -> C.CDLL:
     lib.gwb200_screened_forms_noalloc.argtypes = [C.c_int64, C.c_int64, _vp, _vp, _vp, _vp, C.c_int64, _vp, _vp]
     lib.gwb200_fp64_peak_tflops.argtypes = [_vp, _dp]
     lib.gwb200_update_kernel.argtypes = [_vp, _ip]
-    lib.gwb200_run_g0w0_batch.argtypes = [C.POINTER(_vp), C.c_int64, C.c_int64, C.c_int64, C.POINTER(_ip), _ip,
+    lib.gwb200_run_g0w0_batch.argtypes = [C.POINTER(_vp), C.c_int64, _ip, _ip, C.POINTER(_ip), _ip,
                                           C.c_int, C.POINTER(_dp), C.POINTER(_dp), _ip, C.POINTER(Stats)]
     lib.gwb200_plan_buckets.argtypes = [C.c_int64, _ip, _ip, C.c_int64, C.c_int, C.c_int64, C.c_double, C.c_double,
                                         _ip, _ip]

@@ -443,8 +443,9 @@ struct BatchChunk {
 // `budget` bytes (and, if cap > 0, cap matrices) at once; appends the groups (device pointers of
 // each member).
 std::vector<BatchChunk> batch_chunks(const std::vector<gwb200_handle*>& hs, const std::vector<int64_t>& ms,
-                                     const std::vector<int>& order, const std::vector<int64_t>& sizes, int64_t nfreq,
-                                     bool mixed, bool oz, size_t budget, int64_t cap, std::vector<BatchGroup>& groups) {
+                                     const std::vector<int64_t>& fs, const std::vector<int>& order,
+                                     const std::vector<int64_t>& sizes, bool mixed, bool oz, size_t budget, int64_t cap,
+                                     std::vector<BatchGroup>& groups) {
     std::vector<BatchChunk> chunks;
     size_t pos = 0;
     for (int64_t bsz : sizes) {
@@ -462,6 +463,7 @@ std::vector<BatchChunk> batch_chunks(const std::vector<gwb200_handle*>& hs, cons
             const int i = order[pos + (size_t)t];
             gwb200_handle* h = hs[(size_t)i];
             const TallGeometry gi = make_geometry(h->n, ms[(size_t)i]);
+            const int64_t nfreq = fs[(size_t)i];
             for (int64_t f0 = 0; f0 < nfreq;) {
                 if (cur.nmat == fit) {
                     chunks.push_back(cur);
@@ -1038,7 +1040,8 @@ size_t batch_avail(const gwb200_handle* w) {
 // the cost model's plans for three latency weights plus one bucket per molecule, to be timed),
 // =model (the cost model alone), =each (one bucket per molecule), =single (one bucket).
 std::vector<std::vector<int64_t>> batch_candidates(const std::vector<int64_t>& key, const std::vector<int64_t>& n_sorted,
-                                                   const std::vector<int64_t>& m_sorted, int64_t nfreq, bool mixed,
+                                                   const std::vector<int64_t>& m_sorted,
+                                                   const std::vector<int64_t>& f_sorted, bool mixed,
                                                    size_t lane_budget) {
     const int64_t nsys = (int64_t)n_sorted.size();
     const char* mode_env = std::getenv("GWB200_BATCH_PLAN");
@@ -1053,7 +1056,7 @@ std::vector<std::vector<int64_t>> batch_candidates(const std::vector<int64_t>& k
     std::vector<std::vector<int64_t>> cands;
     const double tau = batch_step_us(mixed), rate = batch_tflops(mixed);
     for (double mult : (mode == "tuned" ? std::vector<double>{1.0, 0.25, 4.0} : std::vector<double>{1.0})) {
-        std::vector<int64_t> p = plan_buckets(n_sorted, m_sorted, nfreq, mixed, lane_budget, tau * mult, rate);
+        std::vector<int64_t> p = plan_buckets(n_sorted, m_sorted, f_sorted, mixed, lane_budget, tau * mult, rate);
         if (std::find(cands.begin(), cands.end(), p) == cands.end()) cands.push_back(p);
     }
     if (mode == "tuned") {
@@ -1067,13 +1070,15 @@ std::vector<std::vector<int64_t>> batch_candidates(const std::vector<int64_t>& k
 // by value (E_F, sizes, Pade order, lanes, update variants) and every device pointer and stream it
 // uses.  A replay is valid exactly while this is unchanged.
 std::vector<int64_t> batch_graph_key(const gwb200_handle* w, const std::vector<gwb200_handle*>& hs,
-                                     const std::vector<int64_t>& key, const std::vector<int64_t>& plan, int64_t npade,
-                                     int lanes, int lane_ctas, const std::vector<int>& variants,
-                                     const int64_t* const* states, const int64_t* nstates) {
+                                     const std::vector<int64_t>& key, const std::vector<int64_t>& plan,
+                                     const std::vector<int64_t>& fs, const std::vector<int64_t>& ps, int lanes,
+                                     int lane_ctas, const std::vector<int>& variants, const int64_t* const* states,
+                                     const int64_t* nstates) {
     std::vector<int64_t> gkey = key;
     auto put = [&](const void* ptr) { gkey.push_back((int64_t)reinterpret_cast<intptr_t>(ptr)); };
     gkey.insert(gkey.end(), plan.begin(), plan.end());
-    gkey.push_back(npade);
+    gkey.insert(gkey.end(), fs.begin(), fs.end());
+    gkey.insert(gkey.end(), ps.begin(), ps.end());
     gkey.push_back(lanes);
     gkey.push_back(lane_ctas);
     gkey.insert(gkey.end(), variants.begin(), variants.end());
@@ -1121,7 +1126,8 @@ int gwb200_plan_buckets(int64_t nsys, const int64_t* nph, const int64_t* ncols, 
             m_sorted.push_back(ms[(size_t)i]);
         }
         const std::vector<int64_t> sizes =
-            plan_buckets(n_sorted, m_sorted, nfreq, mixed, (size_t)budget_bytes, step_us > 0 ? step_us : batch_step_us(mixed),
+            plan_buckets(n_sorted, m_sorted, std::vector<int64_t>(n_sorted.size(), nfreq), mixed, (size_t)budget_bytes,
+                         step_us > 0 ? step_us : batch_step_us(mixed),
                          tflops > 0 ? tflops : batch_tflops(mixed));
         size_t pos = 0;
         for (size_t b = 0; b < sizes.size(); ++b)
@@ -1130,15 +1136,19 @@ int gwb200_plan_buckets(int64_t nsys, const int64_t* nph, const int64_t* ncols, 
     });
 }
 
-int gwb200_run_g0w0_batch(gwb200_handle* const* systems, int64_t nsys, int64_t nfreq, int64_t npade,
+int gwb200_run_g0w0_batch(gwb200_handle* const* systems, int64_t nsys, const int64_t* nfreq, const int64_t* npade,
                           const int64_t* const* states, const int64_t* nstates, int precision, double* const* sigma_out,
                           double* const* qp_out, int64_t* nbuckets_out, gwb200_stats* stats) {
     return guarded([&] {
         if (!systems || nsys <= 0) fail(GWB200_BAD_ARGUMENT, "empty batch");
         if (nsys > 65535) fail(GWB200_BAD_SHAPE, "at most 65535 systems per batch");  // one grid row per member run
         if (!states || !nstates) fail(GWB200_BAD_ARGUMENT, "null state lists");
-        if (nfreq <= 0) fail(GWB200_BAD_SHAPE, "--freq-points must be positive");
-        if (npade <= 0) fail(GWB200_BAD_SHAPE, "--pade-params must be positive");
+        if (!nfreq || !npade) fail(GWB200_BAD_ARGUMENT, "null frequency or Pade counts");
+        const std::vector<int64_t> fs(nfreq, nfreq + nsys), ps(npade, npade + nsys);
+        for (int64_t i = 0; i < nsys; ++i) {
+            if (fs[(size_t)i] <= 0) fail(GWB200_BAD_SHAPE, "--freq-points must be positive");
+            if (ps[(size_t)i] <= 0) fail(GWB200_BAD_SHAPE, "--pade-params must be positive");
+        }
         if (precision != GWB200_FP64 && precision != GWB200_MIXED) fail(GWB200_BAD_ARGUMENT, "unknown precision");
         std::vector<gwb200_handle*> hs(systems, systems + nsys);
         for (gwb200_handle* h : hs)
@@ -1180,13 +1190,13 @@ int gwb200_run_g0w0_batch(gwb200_handle* const* systems, int64_t nsys, int64_t n
         cudaStream_t s = w->stream;
 
         // members' own buffers first (they are not part of the batched-matrix budget)
-        const size_t nb_om = sizeof(double) * nfreq;
         size_t nb_states = 0;
         for (int64_t i = 0; i < nsys; ++i) {
             gwb200_handle* h = hs[(size_t)i];
             const TallGeometry gi = make_geometry(h->n, ms[(size_t)i]);
-            h->omega.ensure(nb_om);
-            h->weight.ensure(nb_om);
+            const int64_t nfreq = fs[(size_t)i];
+            h->omega.ensure(sizeof(double) * nfreq);
+            h->weight.ensure(sizeof(double) * nfreq);
             h->states.ensure(sizeof(int64_t) * nstates[i]);
             if (h->bound_states.empty()) size_buffer(h, h->xt, sizeof(double) * (size_t)ms[(size_t)i] * h->n);
             size_buffer(h, h->dvec, sizeof(double) * (size_t)nfreq * gi.n_pad);
@@ -1200,18 +1210,20 @@ int gwb200_run_g0w0_batch(gwb200_handle* const* systems, int64_t nsys, int64_t n
 
         // plans over the molecules sorted by size (batch_candidates)
         const std::vector<int> order = batch_order(ns, ms);
-        std::vector<int64_t> n_sorted, m_sorted;
+        std::vector<int64_t> n_sorted, m_sorted, f_sorted;
         for (int i : order) {
             n_sorted.push_back(ns[(size_t)i]);
             m_sorted.push_back(ms[(size_t)i]);
+            f_sorted.push_back(fs[(size_t)i]);
         }
         const size_t avail = batch_avail(w);
-        std::vector<int64_t> key = {(int64_t)w->device, (int64_t)precision, (int64_t)oz, (int64_t)mixed_tc, nfreq,
+        std::vector<int64_t> key = {(int64_t)w->device, (int64_t)precision, (int64_t)oz, (int64_t)mixed_tc,
                                     (int64_t)lanes, (int64_t)lane_ctas};
         key.insert(key.end(), n_sorted.begin(), n_sorted.end());
         key.insert(key.end(), m_sorted.begin(), m_sorted.end());
+        key.insert(key.end(), f_sorted.begin(), f_sorted.end());
         const std::vector<std::vector<int64_t>> cands =
-            batch_candidates(key, n_sorted, m_sorted, nfreq, mixed, (size_t)(0.85 * (double)avail / lanes));
+            batch_candidates(key, n_sorted, m_sorted, f_sorted, mixed, (size_t)(0.85 * (double)avail / lanes));
         // chunks of every candidate inside one budget (all candidates share the workspaces)
         const TallGeometry gmax = make_geometry(n_sorted.back(), *std::max_element(m_sorted.begin(), m_sorted.end()));
         if (batch_bytes_per_matrix(gmax, mixed, oz) > avail)
@@ -1228,7 +1240,7 @@ int gwb200_run_g0w0_batch(gwb200_handle* const* systems, int64_t nsys, int64_t n
             groups.clear();
             need = BatchNeed{};
             for (const auto& p : cands) {
-                chunks.push_back(batch_chunks(hs, ms, order, p, nfreq, mixed, oz, budget, cap, groups));
+                chunks.push_back(batch_chunks(hs, ms, fs, order, p, mixed, oz, budget, cap, groups));
                 batch_need(chunks.back(), mixed, oz, need);
             }
             if (need.total() * (size_t)lanes <= (size_t)(0.9 * (double)avail) || attempt >= 12) break;
@@ -1263,28 +1275,34 @@ int gwb200_run_g0w0_batch(gwb200_handle* const* systems, int64_t nsys, int64_t n
 
         // the lead handle's pinned staging buffer, filled on the host before anything is issued:
         // grid, every member's state list, group tables
-        std::vector<double> omega((size_t)nfreq), weight((size_t)nfreq);
-        transformed_legendre_grid(nfreq, omega.data(), weight.data());
+        // one grid (omega, weights) per distinct frequency count, then the state lists, then the
+        // group tables
+        std::map<int64_t, size_t> grid_off;
+        size_t nb_grids = 0;
+        for (int64_t f : fs)
+            if (grid_off.emplace(f, nb_grids).second) nb_grids += 2 * sizeof(double) * (size_t)f;
         const size_t nb_groups = sizeof(BatchGroup) * groups.size();
-        w->stage_in.ensure(2 * nb_om + nb_states + nb_groups);
+        w->stage_in.ensure(nb_grids + nb_states + nb_groups);
         char* sp = w->stage_in.as<char>();
-        std::memcpy(sp, omega.data(), nb_om);
-        std::memcpy(sp + nb_om, weight.data(), nb_om);
+        for (const auto& [f, off] : grid_off)
+            transformed_legendre_grid(f, reinterpret_cast<double*>(sp + off),
+                                      reinterpret_cast<double*>(sp + off) + f);
         std::vector<size_t> st_off((size_t)nsys);
         {
-            size_t off = 2 * nb_om;
+            size_t off = nb_grids;
             for (int64_t i = 0; i < nsys; ++i) {
                 st_off[(size_t)i] = off;
                 std::memcpy(sp + off, states[i], sizeof(int64_t) * nstates[i]);
                 off += sizeof(int64_t) * nstates[i];
             }
         }
-        std::memcpy(sp + 2 * nb_om + nb_states, groups.data(), nb_groups);
+        const size_t groups_off = nb_grids + nb_states;
+        std::memcpy(sp + groups_off, groups.data(), nb_groups);
         for (int64_t i = 0; i < nsys; ++i) {  // every buffer the device sequence touches, sized now
             gwb200_handle* h = hs[(size_t)i];
-            h->sigma.ensure(sizeof(double) * 2 * (size_t)h->nmo * nfreq);
+            h->sigma.ensure(sizeof(double) * 2 * (size_t)h->nmo * fs[(size_t)i]);
             h->qp.ensure(sizeof(double) * h->nmo);
-            h->qp_scratch.ensure(qp_scratch_bytes(nfreq, nstates[i]));
+            h->qp_scratch.ensure(qp_scratch_bytes(fs[(size_t)i], nstates[i]));
         }
         // the lanes fork off the lead stream and join back onto it around each phase
         auto lane_stream = [&](int l) { return l == 0 ? s : w->lanes[l].stream; };
@@ -1303,14 +1321,16 @@ int gwb200_run_g0w0_batch(gwb200_handle* const* systems, int64_t nsys, int64_t n
         // plan (each lane runs its chunks); members' contractions and QP updates
         auto prefix = [&]() {
             int64_t n_launch = 0;
-            GWB_CUDA(cudaMemcpyAsync(w->batch_desc.p, sp + 2 * nb_om + nb_states, nb_groups, cudaMemcpyHostToDevice, s));
+            GWB_CUDA(cudaMemcpyAsync(w->batch_desc.p, sp + groups_off, nb_groups, cudaMemcpyHostToDevice, s));
             GWB_CUDA(cudaMemsetAsync(w->err.p, 0xFF, sizeof(unsigned long long), s));
             fork();
             for (int64_t i = 0; i < nsys; ++i) {
                 gwb200_handle* h = hs[(size_t)i];
                 cudaStream_t ls = lane_stream((int)(i % lanes));
-                GWB_CUDA(cudaMemcpyAsync(h->omega.p, sp, nb_om, cudaMemcpyHostToDevice, ls));
-                GWB_CUDA(cudaMemcpyAsync(h->weight.p, sp + nb_om, nb_om, cudaMemcpyHostToDevice, ls));
+                const int64_t nfreq = fs[(size_t)i];
+                const size_t nb_om = sizeof(double) * nfreq, goff = grid_off.at(nfreq);
+                GWB_CUDA(cudaMemcpyAsync(h->omega.p, sp + goff, nb_om, cudaMemcpyHostToDevice, ls));
+                GWB_CUDA(cudaMemcpyAsync(h->weight.p, sp + goff + nb_om, nb_om, cudaMemcpyHostToDevice, ls));
                 GWB_CUDA(cudaMemcpyAsync(h->states.p, sp + st_off[(size_t)i], sizeof(int64_t) * nstates[i],
                                          cudaMemcpyHostToDevice, ls));
                 if (h->bound_states.empty())
@@ -1336,8 +1356,8 @@ int gwb200_run_g0w0_batch(gwb200_handle* const* systems, int64_t nsys, int64_t n
             fork();
             for (int64_t i = 0; i < nsys; ++i) {
                 hs[(size_t)i]->stream = lane_stream((int)(i % lanes));
-                contract_on_device(hs[(size_t)i], nfreq, nstates[i], &scratch);
-                qp_on_device(hs[(size_t)i], nfreq, npade, nstates[i]);
+                contract_on_device(hs[(size_t)i], fs[(size_t)i], nstates[i], &scratch);
+                qp_on_device(hs[(size_t)i], fs[(size_t)i], ps[(size_t)i], nstates[i]);
             }
             join();
             return scratch.kernel_launches + 2 * nsys;
@@ -1349,7 +1369,7 @@ int gwb200_run_g0w0_batch(gwb200_handle* const* systems, int64_t nsys, int64_t n
         // GWB200_BATCH_GRAPH=0 issues the launches one by one.
         const char* graph_env = std::getenv("GWB200_BATCH_GRAPH");
         const bool want_graph = cands.size() == 1 && !(graph_env && std::strcmp(graph_env, "0") == 0);
-        const std::vector<int64_t> gkey = want_graph ? batch_graph_key(w, hs, key, cands[0], npade, lanes, lane_ctas,
+        const std::vector<int64_t> gkey = want_graph ? batch_graph_key(w, hs, key, cands[0], fs, ps, lanes, lane_ctas,
                                                                         variants[0], states, nstates)
                                                      : std::vector<int64_t>{};
         int64_t launches = 0;
@@ -1425,13 +1445,15 @@ int gwb200_run_g0w0_batch(gwb200_handle* const* systems, int64_t nsys, int64_t n
         st->kernel_launches = launches;
         // results and the pivot word back in one synchronisation
         size_t nb_out = sizeof(unsigned long long);
-        for (gwb200_handle* h : hs) nb_out += sizeof(double) * (2 * (size_t)h->nmo * nfreq + h->nmo);
+        for (int64_t i = 0; i < nsys; ++i)
+            nb_out += sizeof(double) * (2 * (size_t)hs[(size_t)i]->nmo * fs[(size_t)i] + hs[(size_t)i]->nmo);
         w->stage_out.ensure(nb_out);
         char* op = w->stage_out.as<char>();
         GWB_CUDA(cudaMemcpyAsync(op, w->err.p, sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
         size_t o = sizeof(unsigned long long);
-        for (gwb200_handle* h : hs) {
-            const size_t nb_sig = sizeof(double) * 2 * (size_t)h->nmo * nfreq, nb_qp = sizeof(double) * h->nmo;
+        for (int64_t i = 0; i < nsys; ++i) {
+            const gwb200_handle* h = hs[(size_t)i];
+            const size_t nb_sig = sizeof(double) * 2 * (size_t)h->nmo * fs[(size_t)i], nb_qp = sizeof(double) * h->nmo;
             GWB_CUDA(cudaMemcpyAsync(op + o, h->sigma.p, nb_sig, cudaMemcpyDeviceToHost, s));
             GWB_CUDA(cudaMemcpyAsync(op + o + nb_sig, h->qp.p, nb_qp, cudaMemcpyDeviceToHost, s));
             o += nb_sig + nb_qp;
@@ -1448,7 +1470,7 @@ int gwb200_run_g0w0_batch(gwb200_handle* const* systems, int64_t nsys, int64_t n
         o = sizeof(unsigned long long);
         for (int64_t i = 0; i < nsys; ++i) {
             const gwb200_handle* h = hs[(size_t)i];
-            const size_t nb_sig = sizeof(double) * 2 * (size_t)h->nmo * nfreq, nb_qp = sizeof(double) * h->nmo;
+            const size_t nb_sig = sizeof(double) * 2 * (size_t)h->nmo * fs[(size_t)i], nb_qp = sizeof(double) * h->nmo;
             if (sigma_out && sigma_out[i]) std::memcpy(sigma_out[i], op + o, nb_sig);
             if (qp_out && qp_out[i]) std::memcpy(qp_out[i], op + o + nb_sig, nb_qp);
             o += nb_sig + nb_qp;
@@ -1457,7 +1479,7 @@ int gwb200_run_g0w0_batch(gwb200_handle* const* systems, int64_t nsys, int64_t n
         int64_t nmax = 0, mmax = 0;
         for (int64_t i = 0; i < nsys; ++i) {
             const double nd = (double)ns[(size_t)i], md = (double)ms[(size_t)i];
-            flops += (double)nfreq * (nd * nd * nd / 3.0 + nd * nd * md + 3.0 * nd * md);
+            flops += (double)fs[(size_t)i] * (nd * nd * nd / 3.0 + nd * nd * md + 3.0 * nd * md);
             nmax = std::max(nmax, ns[(size_t)i]);
             mmax = std::max(mmax, ms[(size_t)i]);
         }

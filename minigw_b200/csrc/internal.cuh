@@ -212,7 +212,8 @@ int launch_forms_scatter(const BatchGroup* groups, int64_t ngroups, const double
 size_t batch_bytes_per_matrix(const TallGeometry& g, bool mixed, bool fp64_oz);
 // bucket sizes over the molecules sorted by (n, m): minimises block-step latency + padded work
 std::vector<int64_t> plan_buckets(const std::vector<int64_t>& n_sorted, const std::vector<int64_t>& m_sorted,
-                                  int64_t nfreq, bool mixed, size_t budget, double step_us, double tflops);
+                                  const std::vector<int64_t>& f_sorted, bool mixed, size_t budget, double step_us,
+                                  double tflops);
 
 // noalloc.cu
 size_t noalloc_scratch_bytes();

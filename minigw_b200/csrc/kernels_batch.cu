@@ -101,14 +101,18 @@ size_t batch_bytes_per_matrix(const TallGeometry& g, bool mixed, bool fp64_oz) {
 
 // Contiguous groups of the molecules sorted by (n, m) that minimise
 //   sum over buckets of  chunks * (n_pad / 64) * step_us  +  padded flops / rate,
-// chunks = the bucket's matrices over what fits `budget` bytes at once, padded flops =
-// matrices * (N^3/3 + N^2 M) at the bucket's padded N, M.  Dynamic programming over the end of
+// chunks = the bucket's matrices (its molecules' frequency counts f_sorted, summed) over what
+// fits `budget` bytes at once, padded flops = matrices * (N^3/3 + N^2 M) at the bucket's padded
+// N, M.  Dynamic programming over the end of
 // the last bucket, O(nsys^2).  Returns the bucket sizes in sorted order.
 std::vector<int64_t> plan_buckets(const std::vector<int64_t>& n_sorted, const std::vector<int64_t>& m_sorted,
-                                  int64_t nfreq, bool mixed, size_t budget, double step_us, double tflops) {
+                                  const std::vector<int64_t>& f_sorted, bool mixed, size_t budget, double step_us,
+                                  double tflops) {
     const int64_t ns = (int64_t)n_sorted.size();
     std::vector<double> best((size_t)ns + 1, std::numeric_limits<double>::infinity());
     std::vector<int64_t> from((size_t)ns + 1, 0);
+    std::vector<double> fsum((size_t)ns + 1, 0.0);  // prefix sums of the frequency counts
+    for (int64_t i = 0; i < ns; ++i) fsum[(size_t)i + 1] = fsum[(size_t)i] + (double)f_sorted[(size_t)i];
     best[0] = 0.0;
     const double rate = std::max(tflops, 1e-3) * 1e12;
     for (int64_t k = 1; k <= ns; ++k) {
@@ -116,7 +120,7 @@ std::vector<int64_t> plan_buckets(const std::vector<int64_t>& n_sorted, const st
         for (int64_t j = k; j >= 1; --j) {  // bucket = sorted molecules j-1 .. k-1
             mmax = std::max(mmax, m_sorted[(size_t)j - 1]);
             const TallGeometry g = make_geometry(n_sorted[(size_t)k - 1], mmax);
-            const double nmat = (double)(k - j + 1) * (double)nfreq;
+            const double nmat = fsum[(size_t)k] - fsum[(size_t)j - 1];
             const double per = (double)batch_bytes_per_matrix(g, mixed, false);
             const double fit = std::max(1.0, std::floor((double)budget / per));
             const double chunks = std::ceil(nmat / fit);

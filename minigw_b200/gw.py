@@ -266,25 +266,28 @@ class B200Backend:
         return v.value
 
 
-def run_g0w0_batch(backends: list[B200Backend], nfreq: int, npade: int, states: list, precision="mixed"):
+def run_g0w0_batch(backends: list[B200Backend], nfreq, npade, states: list, precision="mixed"):
     """Solve every loaded backend's molecule (eta = 0) through shared launches (gwb200_run_g0w0_batch).
 
-    Work runs on backends[0]'s stream and workspaces.  Returns per-molecule Sigma_c(iw) and QP
-    energies, the number of buckets the molecules were grouped into, and the call's stats."""
+    `nfreq` and `npade` are one count for all molecules or one per molecule.  Work runs on
+    backends[0]'s stream and workspaces.  Returns per-molecule Sigma_c(iw) and QP energies, the
+    number of buckets the molecules were grouped into, and the call's stats."""
     n = len(backends)
+    nf = np.ascontiguousarray(np.broadcast_to(np.asarray(nfreq, dtype=np.int64), (n,)))
+    npd = np.ascontiguousarray(np.broadcast_to(np.asarray(npade, dtype=np.int64), (n,)))
     hs = (C.c_void_p * n)(*[b._h for b in backends])
     st_arrays = [np.ascontiguousarray(s, dtype=np.int64) for s in states]
     if len(st_arrays) != n:
         raise GwB200Error(7, "one state list per molecule is required")
     st_ptrs = (_ip * n)(*[iptr(a) for a in st_arrays])
     nst = np.array([a.shape[0] for a in st_arrays], dtype=np.int64)
-    sig = [np.zeros((b.nmo, nfreq), dtype=np.complex128) for b in backends]
+    sig = [np.zeros((b.nmo, int(f)), dtype=np.complex128) for b, f in zip(backends, nf)]
     qp = [np.zeros(b.nmo) for b in backends]
     sig_ptrs = (_dp * n)(*[dptr(a) for a in sig])
     qp_ptrs = (_dp * n)(*[dptr(a) for a in qp])
     nb = C.c_int64()
     stats = Stats()
-    check(lib.gwb200_run_g0w0_batch(hs, n, int(nfreq), int(npade), st_ptrs, iptr(nst), _precision_code(precision),
+    check(lib.gwb200_run_g0w0_batch(hs, n, iptr(nf), iptr(npd), st_ptrs, iptr(nst), _precision_code(precision),
                                     sig_ptrs, qp_ptrs, C.byref(nb), C.byref(stats)))
     return {"sigma": sig, "qp": qp, "buckets": nb.value, "stats": stats.as_dict()}
 

@@ -228,3 +228,26 @@ def test_graph_replay_matches_eager_and_follows_reloads(monkeypatch):
     finally:
         for be in bes:
             be.close()
+
+
+@pytest.mark.gpu
+def test_batch_with_per_molecule_frequency_and_pade_counts():
+    from minigw_b200 import B200Backend, run_g0w0_batch
+
+    inputs = _systems([(16, 3), (28, 5), (22, 4)], seed0=950)
+    states = [_states(inp) for inp in inputs]
+    nfreq, npade = [16, 24, 20], [8, 12, 10]
+    bes = [B200Backend(0) for _ in inputs]
+    try:
+        for be, inp in zip(bes, inputs):
+            be.load_system(inp)
+        alone = [be.run_g0w0(nf, npd, st, precision="mixed") for be, nf, npd, st in zip(bes, nfreq, npade, states)]
+        for _ in range(2):  # eager (plan timed), then the graph
+            got = run_g0w0_batch(bes, nfreq, npade, states)
+            for a, s, q, st, nf in zip(alone, got["sigma"], got["qp"], states, nfreq):
+                assert s.shape[1] == nf
+                np.testing.assert_array_equal(s, a["sigma"])
+                np.testing.assert_array_equal(q[st], a["qp"][st])
+    finally:
+        for be in bes:
+            be.close()
