@@ -152,7 +152,64 @@ def cpu_reference_sample(inp, wl, omegas, weights, pairs: int, threads: int):
                               backend="blas-lapack", threads=1)
     per_pair = sec / len(fsel)
     return {"seconds_per_pair": per_pair, "pairs": len(fsel), "threads": threads,
-            "solves_per_s": 1.0 / (wl.nfreq ** 2 * per_pair)}
+            "solves_per_s": 1.0 / (wl.nfreq ** 2 * per_pair), "mode": "threaded BLAS"}
+
+
+def cpu_reference_sample_openmp(inp, wl, omegas, weights, pairs: int, threads: int):
+    """The reference's OpenMP frequency mode (src/gw/sigma_c_driver.cpp:403-447): `pairs`
+    (f_n, f') pairs spread over `threads` OpenMP threads, one OpenBLAS thread each (the mode's
+    OPENBLAS_NUM_THREADS=1).  Pairs are rounded up to a multiple of `threads` so every thread
+    works for the whole region."""
+    import oracle
+
+    if not oracle.Ref.available:
+        return None
+    pairs = max(threads, (pairs + threads - 1) // threads * threads)
+    ref = oracle.Ref(blas_threads=1)
+    fsel = [int(i * (wl.nfreq - 1) / max(1, pairs - 1)) for i in range(pairs)]
+    sec, _ = ref.pair_seconds(inp, omegas[fsel], weights[fsel], float(omegas[0]), list(wl.states),
+                              backend="blas-lapack", threads=threads)
+    per_pair = sec / len(fsel)
+    return {"seconds_per_pair": per_pair, "pairs": len(fsel), "threads": threads,
+            "solves_per_s": 1.0 / (wl.nfreq ** 2 * per_pair), "mode": "OpenMP frequency"}
+
+
+def openmp_mode_fits(wl, threads: int) -> bool:
+    """Host memory for the OpenMP mode: per thread the reference holds eps, its LU copy and the
+    identity right-hand sides (three n x n complex matrices), besides two copies of the ERI."""
+    try:
+        avail = os.sysconf("SC_AVPHYS_PAGES") * os.sysconf("SC_PAGE_SIZE")
+    except (ValueError, OSError):
+        return False
+    need = threads * 3 * 16 * wl.nph ** 2 + 2 * 8 * wl.nmo ** 4
+    return need < 0.8 * avail
+
+
+def cpu_model() -> str:
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def workload_config(args, wl, world: int) -> dict:
+    """The `config` both arms print for the same command line (identical dicts)."""
+    from minigw_b200.sharding import shard_bounds  # no library load
+
+    split = getattr(args, "split_frequencies", False)
+    return {"workload": f"{wl.name}: {WORKLOAD_TEXT[wl.name]}", "nmo": wl.nmo, "nocc": wl.nocc,
+            "nph": wl.nph, "ncols": wl.ncols, "nfreq": wl.nfreq, "npade": wl.npade, "states": list(wl.states),
+            "precision": args.precision,
+            "parallelism": (f"integration frequencies split over {world} ranks "
+                            f"(rank 0: {shard_bounds(wl.nfreq, world, 0)}), NCCL all-reduce of Sigma_c")
+            if split else f"{world} independent replica(s)",
+            "l2": ("inputs larger than L2 (eps(iw) is a "
+                   f"{(wl.nph + wl.ncols) * wl.nph * 8 / 1e6:.0f} MB matrix per frequency)")
+            if (wl.nph + wl.ncols) * wl.nph * 8 * wl.nfreq > 126e6 else
+            "inputs smaller than L2 (a parity-size workload, not flushed between steps)"}
 
 
 def traffic_oz(workload: str):
@@ -173,11 +230,47 @@ def hbm_peak_gbs() -> float:
 
 
 def auto_pairs(wl) -> int:
-    return {"cfg1": 400, "cfg2": 6, "cfg3": 2}[wl.name]
+    """(f_n, f') pairs per threaded-BLAS sample: a few seconds of CPU work per sample."""
+    return {"cfg1": 400, "cfg2": 2, "cfg3": 1}[wl.name]
+
+
+def reference_cpu_baseline(inp, wl, omegas, weights, threads: int, blas_pairs: int, omp_pairs: int) -> dict | None:
+    """The reference's CPU path in both modes (BASELINE plan: OpenMP frequency parallelism with one
+    BLAS thread per OpenMP thread, or threaded BLAS in serial mode), the faster one reported."""
+    blas = cpu_reference_sample(inp, wl, omegas, weights, blas_pairs, threads)
+    if blas is None:
+        return None
+    omp = cpu_reference_sample_openmp(inp, wl, omegas, weights, omp_pairs, threads) \
+        if threads > 1 and openmp_mode_fits(wl, threads) else None
+    best = min([m for m in (blas, omp) if m], key=lambda m: m["seconds_per_pair"])
+    modes = {"threaded_blas": blas, "openmp_frequency": omp or "not run (one core, or too little host memory)"}
+    return {"best": best, "modes": modes}
+
+
+def cpu_baseline_record(cb: dict, wl, threads: int) -> dict:
+    best = cb["best"]
+    other = [f"{m['mode']}: {m['seconds_per_pair']:.4g} s per pair over {m['pairs']} pairs"
+             for m in cb["modes"].values() if isinstance(m, dict)]
+    return {"value": best["solves_per_s"], "unit": "GW solves/s", "cores": threads, "kind": "reference",
+            "cpu_model": cpu_model(), "mode": best["mode"],
+            "sample": f"(f_n, f') pairs of the {wl.name} solve (one W_c build by zgetrf+zgetrs on nph={wl.nph} plus "
+                      f"{len(wl.states)}x{wl.nmo} panel contractions each) through the reference's own code "
+                      f"(oracle/_ref, blas-lapack backend) on {threads} threads; "
+                      + "; ".join(other) + f"; faster: {best['mode']}; solve time = nfreq^2 x seconds per pair "
+                      "(extrapolated)",
+            "modes": {k: ({kk: vv for kk, vv in v.items()} if isinstance(v, dict) else v)
+                      for k, v in cb["modes"].items()}}
 
 
 def run_reference(args, wl):
-    """--impl reference: the reference's own CPU implementation of the path on the host cores."""
+    """--impl reference: the reference's own CPU implementation of the path on the host cores.
+
+    Nothing of this repository's library runs here: the input comes from the numpy generator
+    (which does not load libgwb200.so), the frequency grid from the reference's own
+    generate_transformed_legendre_grid, the work from oracle/_ref (the reference's sources
+    compiled unmodified).  Warm-up: `warmup` single pairs.  Timed: `steps` samples of
+    auto_pairs() pairs with threaded BLAS, and the same number of pairs in the OpenMP frequency
+    mode (one region); the faster mode is the value."""
     world, rank, _ = dist_setup()
     if rank != 0:
         return 0
@@ -189,30 +282,32 @@ def run_reference(args, wl):
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libgwref.so was not built (the reference "
                           "tree was absent when the repository was built)"}))
         return 0
-    from minigw_b200 import generate_transformed_legendre_grid
-
     inp = make_input(wl.nmo, wl.nocc, args.seed)
-    om, w = generate_transformed_legendre_grid(wl.nfreq)
+    om, w = oracle.Ref().grid(wl.nfreq)
     pairs = args.cpu_pairs or auto_pairs(wl)
     for _ in range(args.warmup):
-        cpu_reference_sample(inp, wl, om, w, max(1, pairs // 2), threads)
-    samples = [cpu_reference_sample(inp, wl, om, w, pairs, threads) for _ in range(args.steps)]
-    per_pair = statistics.mean(s["seconds_per_pair"] for s in samples)
+        cpu_reference_sample(inp, wl, om, w, 1, threads)
+    blas = [cpu_reference_sample(inp, wl, om, w, pairs, threads) for _ in range(args.steps)]
+    blas_pp = statistics.mean(s["seconds_per_pair"] for s in blas)
+    blas_rec = dict(blas[0], seconds_per_pair=blas_pp, pairs=pairs * args.steps,
+                    solves_per_s=1.0 / (wl.nfreq ** 2 * blas_pp))
+    omp = cpu_reference_sample_openmp(inp, wl, om, w, pairs * args.steps, threads) \
+        if threads > 1 and openmp_mode_fits(wl, threads) else None
+    cb = {"best": min([m for m in (blas_rec, omp) if m], key=lambda m: m["seconds_per_pair"]),
+          "modes": {"threaded_blas": blas_rec,
+                    "openmp_frequency": omp or "not run (one core, or too little host memory)"}}
+    per_pair = cb["best"]["seconds_per_pair"]
     solve_s = wl.nfreq ** 2 * per_pair
     value = 1.0 / solve_s
-    sample_txt = (f"{pairs} (f_n, f') pairs per step of the {wl.name} solve (one W_c build by zgetrf+zgetrs on "
-                  f"nph={wl.nph} plus {len(wl.states)}x{wl.nmo} panel contractions each), blas-lapack backend, "
-                  f"{threads} OpenBLAS threads; solve time = nfreq^2 x seconds per pair (extrapolated)")
+    rec = cpu_baseline_record(cb, wl, threads)
     out = {
         "impl": "reference", "metric": "gw_solves_per_s", "value": value, "unit": "GW solves/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": per_pair * pairs * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c128",
         "data": f"synthetic (seeded generator, seed {args.seed})",
-        "config": {"workload": f"{wl.name}: {WORKLOAD_TEXT[wl.name]}", "nmo": wl.nmo, "nocc": wl.nocc,
-                   "nph": wl.nph, "nfreq": wl.nfreq, "npade": wl.npade, "states": list(wl.states)},
+        "config": workload_config(args, wl, world),
         "seconds_per_solve_extrapolated": solve_s,
-        "cpu_baseline": {"value": value, "unit": "GW solves/s", "cores": threads, "kind": "reference",
-                         "sample": sample_txt},
+        "cpu_baseline": rec,
         "e2e": {"value": value, "unit": "GW solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(out))
@@ -394,14 +489,7 @@ def run_b200(args, wl):
         "scaling": "strong" if split else "weak",
         "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f32 (3xTF32) + f64",
         "data": f"synthetic (seeded generator, seed {args.seed}+rank; GEMM of the ERI on the GPU)",
-        "config": {"workload": f"{wl.name}: {WORKLOAD_TEXT[wl.name]}", "nmo": wl.nmo, "nocc": wl.nocc,
-                   "nph": wl.nph, "ncols": wl.ncols, "nfreq": wl.nfreq, "npade": wl.npade, "states": states,
-                   "precision": args.precision,
-                   "parallelism": (f"integration frequencies split over {world} ranks "
-                                   f"(rank 0: {shard_bounds(wl.nfreq, world, 0)}), NCCL all-reduce of Sigma_c")
-                   if split else f"{world} independent replica(s)",
-                   "l2": "inputs larger than L2 (eps(iw) is a "
-                         f"{(wl.nph + wl.ncols) * wl.nph * 8 / 1e6:.0f} MB matrix per frequency)"},
+        "config": workload_config(args, wl, world),
         "ms_per_frequency": ms_per_step / wl.nfreq,
         "frequency_points_per_s": solves_per_step * wl.nfreq * 1e3 / ms_per_step,
         "p50_ms": statistics.median(step_ms), "p99_ms": max(step_ms) if len(step_ms) < 100 else
@@ -476,19 +564,14 @@ def run_b200(args, wl):
         pass
 
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        try:
-            host_inp = inp
-            cb = cpu_reference_sample(host_inp, wl, om, w, args.cpu_pairs or auto_pairs(wl), os.cpu_count() or 1)
+        threads = os.cpu_count() or 1
+        try:  # both CPU modes of the reference; a bounded sample of each
+            cb = reference_cpu_baseline(inp, wl, om, w, threads, args.cpu_pairs or max(2, auto_pairs(wl)), threads)
         except Exception as exc:  # the baseline is reported, never fatal
             cb = None
             result["cpu_baseline_error"] = str(exc)
         if cb:
-            result["cpu_baseline"] = {
-                "value": cb["solves_per_s"], "unit": "GW solves/s", "cores": cb["threads"], "kind": "reference",
-                "sample": f"{cb['pairs']} (f_n, f') pairs of the {wl.name} solve through the reference's own code "
-                          f"(oracle/_ref, blas-lapack backend, {cb['threads']} OpenBLAS threads), "
-                          f"{cb['seconds_per_pair']:.3f} s per pair; solve time = nfreq^2 x pair time "
-                          "(extrapolated)"}
+            result["cpu_baseline"] = cpu_baseline_record(cb, wl, threads)
     if dist is not None:
         dist.destroy_process_group()
     if rank == 0:

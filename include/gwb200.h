@@ -150,6 +150,16 @@ int gwb200_run_g0w0(gwb200_handle* h, int64_t nfreq, int64_t npade, const int64_
                     double eta, int precision, double* omega_out, double* weight_out, double* sigma_out,
                     double* sigma_x_out, double* qp_out, gwb200_stats* stats);
 
+/* Copies of the resident screening inputs, for checking the gathers bit for bit.  vph_out (n x n,
+ * row-major): V_ph[jb, ia] = (jb|ia), as gw::calculate_v_ph_matrix builds it (src/gw/sigma.cpp:56-71).
+ * panel_out (nstates*nmo x n, row-major): row s*nmo + k = (p_s k|ia), i.e. the columns of the panels
+ * gw::workspace::PqPhPanelView::fill_panel fills (src/workspace/pq_ph_panel.cpp:25-47) for state p_s.
+ * Either output may be NULL.  After gwb200_load_system the panel rows are gathered from the resident
+ * (pq|o.) block by the kernel the screening calls use; after gwb200_load_system_states `states` must be
+ * the bound list (the rows are the resident ones).  Exported for checking; it replaces nothing. */
+int gwb200_read_resident(gwb200_handle* h, const int64_t* states, int64_t nstates, double* vph_out,
+                         double* panel_out);
+
 /* Screened quadratic forms Q[f, s, k] = x_{p_s k}^T W_c(i w_f) x_{p_s k} (real, <= 0) at eta == 0
  * (GWB200_ETA_NONZERO otherwise), layout [nfreq][nstates][nmo].  The per-frequency quantity the reference computes as
  * quadratic_forms_panel (src/workspace/screening_workspace.cpp:69-102); exported for checking. */
@@ -205,10 +215,13 @@ int gwb200_read_input_h5(const char* path, int64_t* nmo, int64_t* nocc, double* 
  * on `stream` (a cudaStream_t as void*, NULL = the legacy default stream) of the CURRENT device.
  * Every intermediate lives in one file-scope device array of 4 MiB that each GPU loading the
  * library holds until exit; one frequency must fit: (n64 + m64) * n64 + n64 + 4096 + m64 doubles
- * <= 524256 (n64, m64 = n, m rounded up to 64), e.g. n = m = 320, else GWB200_BAD_SHAPE.  The
- * first call on a device looks up that array's device address (cudaGetSymbolAddress); make that
- * first call before any stream capture.  All calls share the array and it keeps the last call's
- * contents: calls that overlap on the GPU race and must be serialised by the caller.
+ * <= 524256 (n64, m64 = n, m rounded up to 64), e.g. n = m = 320, else GWB200_BAD_SHAPE.  Every
+ * buffer must be device (or managed) memory of the current device, else GWB200_BAD_ARGUMENT.  Each
+ * call looks up that array's device address (cudaGetSymbolAddress); on the first call on a device
+ * this loads the library's device code there, so make that first call before any stream capture.
+ * The call reads the factorisation's pivot flag back and synchronises `stream` before it returns.
+ * All calls share the array and it keeps the last call's contents: calls that overlap on the GPU
+ * race and must be serialised by the caller.
  * No counterpart in the reference (an addition of this library). */
 int gwb200_screened_forms_noalloc(int64_t n, int64_t m, const double* d_v, const double* d_xt,
                                   const double* d_delta, const double* d_omega, int64_t nfreq,

@@ -753,6 +753,32 @@ int gwb200_load_system_states(gwb200_handle* h, int64_t nmo, int64_t nocc, const
     });
 }
 
+int gwb200_read_resident(gwb200_handle* h, const int64_t* states, int64_t nstates, double* vph_out,
+                         double* panel_out) {
+    return guarded([&] {
+        check_system(h);
+        cudaStream_t s = h->stream;
+        const int64_t n = h->n;
+        if (vph_out) GWB_CUDA(cudaMemcpyAsync(vph_out, h->v.p, sizeof(double) * (size_t)n * n, cudaMemcpyDeviceToHost, s));
+        if (panel_out) {
+            check_states(h, states, nstates);
+            const size_t nb = sizeof(double) * (size_t)nstates * h->nmo * n;
+            if (!h->bound_states.empty()) {
+                if (!std::equal(states, states + nstates, h->bound_states.begin(), h->bound_states.end()))
+                    fail(GWB200_BAD_ARGUMENT, "the state list must be the one given to gwb200_load_system_states");
+            } else {  // the panel rows a screening call would gather from the resident (pq|o.) block
+                h->states.ensure(sizeof(int64_t) * nstates);
+                size_buffer(h, h->xt, nb);
+                GWB_CUDA(cudaMemcpyAsync(h->states.p, states, sizeof(int64_t) * nstates, cudaMemcpyHostToDevice, s));
+                launch_gather_panel(h->pqo.as<double>(), h->nmo, h->nocc, h->states.as<int64_t>(), nstates,
+                                    h->xt.as<double>(), s);
+            }
+            GWB_CUDA(cudaMemcpyAsync(panel_out, h->xt.p, nb, cudaMemcpyDeviceToHost, s));
+        }
+        GWB_CUDA(cudaStreamSynchronize(s));
+    });
+}
+
 int gwb200_screened_forms(gwb200_handle* h, const double* omega, int64_t nfreq, const int64_t* states,
                           int64_t nstates, double eta, int precision, double* q_out, gwb200_stats* stats) {
     return guarded([&] {
@@ -1066,17 +1092,29 @@ std::vector<std::vector<int64_t>> batch_candidates(const std::vector<int64_t>& k
     return cands;
 }
 
-// What a captured batch graph depends on: the plan signature and plan, the scalars its kernels take
-// by value (E_F, sizes, Pade order, lanes, update variants) and every device pointer and stream it
-// uses.  A replay is valid exactly while this is unchanged.
+// What a captured batch graph depends on: the plan signature and plan, the launch sequences the plan
+// was cut into (each chunk's geometry, matrix count and group range, and the chunks each lane runs:
+// the chunk size follows the free device memory and GWB200_MAX_FREQ_CHUNK, so the same plan can be
+// cut differently from call to call), the scalars its kernels take by value (E_F, sizes, Pade order,
+// lanes, update variants) and every device pointer and stream it uses.  A replay is valid exactly
+// while this is unchanged.
 std::vector<int64_t> batch_graph_key(const gwb200_handle* w, const std::vector<gwb200_handle*>& hs,
                                      const std::vector<int64_t>& key, const std::vector<int64_t>& plan,
+                                     const std::vector<BatchChunk>& chunks,
+                                     const std::vector<std::vector<size_t>>& assign,
                                      const std::vector<int64_t>& fs, const std::vector<int64_t>& ps, int lanes,
                                      int lane_ctas, const std::vector<int>& variants, const int64_t* const* states,
                                      const int64_t* nstates) {
     std::vector<int64_t> gkey = key;
     auto put = [&](const void* ptr) { gkey.push_back((int64_t)reinterpret_cast<intptr_t>(ptr)); };
     gkey.insert(gkey.end(), plan.begin(), plan.end());
+    gkey.push_back((int64_t)chunks.size());
+    for (const BatchChunk& c : chunks)
+        gkey.insert(gkey.end(), {c.g.n, c.g.m, c.g.n_pad, c.g.m_pad, c.nmat, c.group0, c.ngroups});
+    for (const auto& lane : assign) {
+        gkey.push_back(-1 - (int64_t)lane.size());
+        gkey.insert(gkey.end(), lane.begin(), lane.end());
+    }
     gkey.insert(gkey.end(), fs.begin(), fs.end());
     gkey.insert(gkey.end(), ps.begin(), ps.end());
     gkey.push_back(lanes);
@@ -1369,8 +1407,9 @@ int gwb200_run_g0w0_batch(gwb200_handle* const* systems, int64_t nsys, const int
         // GWB200_BATCH_GRAPH=0 issues the launches one by one.
         const char* graph_env = std::getenv("GWB200_BATCH_GRAPH");
         const bool want_graph = cands.size() == 1 && !(graph_env && std::strcmp(graph_env, "0") == 0);
-        const std::vector<int64_t> gkey = want_graph ? batch_graph_key(w, hs, key, cands[0], fs, ps, lanes, lane_ctas,
-                                                                        variants[0], states, nstates)
+        const std::vector<int64_t> gkey = want_graph ? batch_graph_key(w, hs, key, cands[0], chunks[0], assign[0], fs,
+                                                                        ps, lanes, lane_ctas, variants[0], states,
+                                                                        nstates)
                                                      : std::vector<int64_t>{};
         int64_t launches = 0;
         size_t pick = 0;

@@ -15,8 +15,6 @@
 // (two streams, two host threads) race on it and must be serialised by the caller.
 #include "internal.cuh"
 
-#include <mutex>
-
 namespace gwb200 {
 namespace {
 
@@ -26,23 +24,14 @@ constexpr size_t kHeaderDoubles = 32;  // 256 bytes: the failing-pivot flag
 
 __device__ __align__(256) double g_noalloc_scratch[kStaticScratchDoubles];
 
-// Device address of g_noalloc_scratch per device.  In host code the symbol is only a host-side
-// stand-in: the address must come from cudaGetSymbolAddress with the device current.
-constexpr int kMaxDevices = 64;
-std::mutex g_scratch_mu;
-double* g_scratch_addr[kMaxDevices] = {};
-
+// Device address of g_noalloc_scratch on the current device.  In host code the symbol is only a
+// host-side stand-in: the address must come from cudaGetSymbolAddress with the device current.  It
+// is looked up on every call (cheap next to a solve) rather than cached, so it stays right after the
+// primary context of the device has been reset and the module loaded again.
 double* scratch_for_current_device() {
-    int dev = 0;
-    GWB_CUDA(cudaGetDevice(&dev));
-    if (dev < 0 || dev >= kMaxDevices) fail(GWB200_BAD_ARGUMENT, "device index beyond the static scratch table");
-    std::lock_guard<std::mutex> lock(g_scratch_mu);
-    if (!g_scratch_addr[dev]) {
-        void* p = nullptr;
-        GWB_CUDA(cudaGetSymbolAddress(&p, g_noalloc_scratch));
-        g_scratch_addr[dev] = static_cast<double*>(p);
-    }
-    return g_scratch_addr[dev];
+    void* p = nullptr;
+    GWB_CUDA(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+    return static_cast<double*>(p);
 }
 
 void require_device_pointer(const void* p, const char* name) {
@@ -55,6 +44,11 @@ void require_device_pointer(const void* p, const char* name) {
     }
     if (attr.type != cudaMemoryTypeDevice && attr.type != cudaMemoryTypeManaged)
         fail(GWB200_BAD_ARGUMENT, std::string(name) + " must be device memory");
+    int dev = 0;
+    GWB_CUDA(cudaGetDevice(&dev));
+    if (attr.type == cudaMemoryTypeDevice && attr.device != dev)
+        fail(GWB200_BAD_ARGUMENT, std::string(name) + " is memory of device " + std::to_string(attr.device) +
+                                      ", not of the current device " + std::to_string(dev));
 }
 
 } // namespace

@@ -24,22 +24,9 @@ import ctypes as C
 import numpy as np
 
 from ._lib import FP64, MIXED, GwB200Error, Request, Stats, _dp, _ip, check, dptr, iptr, lib
+from .gw_input import GwInput
 
 HARTREE_TO_EV = 27.211386245988  # include/types.hpp:12
-
-
-@dataclass
-class GwInput:
-    """include/gw/gw.hpp:17-23 (eri_mo C-order [nmo]*4, mo_energy, vxc_mo, nocc, fermi_energy)."""
-    eri_mo: np.ndarray
-    mo_energy: np.ndarray
-    vxc_mo: np.ndarray
-    nocc: int
-    fermi_energy: float
-
-    @property
-    def nmo(self) -> int:
-        return int(self.mo_energy.shape[0])
 
 
 @dataclass
@@ -253,6 +240,19 @@ class B200Backend:
         check(lib.gwb200_pade_sweep(self._h, dptr(om), om.shape[0], dptr(row), int(npade), int(npts), float(f),
                                     float(x_start), float(interval), dptr(out)))
         return out
+
+    def read_resident(self, states=None, vph: bool = True):
+        """(V_ph n x n, panel rows nstates*nmo x n) as resident on the device (gwb200_read_resident);
+        either is None when not asked for (vph=False / states=None)."""
+        n = self.nocc * (self.nmo - self.nocc)
+        v = np.zeros((n, n)) if vph else None
+        panel, st = None, None
+        if states is not None:
+            st = np.ascontiguousarray(states, dtype=np.int64)
+            panel = np.zeros((st.shape[0] * self.nmo, n))
+        check(lib.gwb200_read_resident(self._h, iptr(st) if st is not None else None,
+                                       st.shape[0] if st is not None else 0, dptr(v), dptr(panel)))
+        return v, panel
 
     def fp64_peak_tflops(self) -> float:
         v = C.c_double()

@@ -22,7 +22,7 @@ from dataclasses import dataclass
 
 import numpy as np
 
-from .gw import GwInput
+from .gw_input import GwInput
 
 
 @dataclass(frozen=True)

@@ -28,8 +28,11 @@ _ip = C.POINTER(C.c_int64)
 i64 = C.c_int64
 
 
-def build(ref_root: str = "/root/reference") -> None:
-    """make -C oracle (restatement always; _ref when the reference tree exists)."""
+def build(ref_root: str | None = None) -> None:
+    """make -C oracle (restatement always; _ref when the reference tree exists).  The tree is
+    `ref_root`, else the MINIGW_REF_ROOT environment variable; without either only the
+    restatement is built."""
+    ref_root = ref_root or os.environ.get("MINIGW_REF_ROOT", "")
     subprocess.run(["make", "-s", "-C", str(HERE), f"REF_ROOT={ref_root}", "all"], check=True)
 
 
@@ -166,6 +169,7 @@ class Ref:
                                   _dp]
         lib.ref_pair_seconds.argtypes = [i64, i64, C.c_double, _dp, _dp, _dp, i64, _dp, C.c_double, _dp, _ip, i64,
                                          C.c_int, C.c_int, _dp, _dp]
+        lib.ref_resident.argtypes = [i64, i64, C.c_double, _dp, _dp, _dp, _ip, i64, _dp, _dp]
         lib.ref_grid.argtypes = [i64, _dp, _dp]
         lib.ref_pade_coeffs.argtypes = [i64, _dp, _dp, i64, _dp, _dp]
         lib.ref_pade_coeffs.restype = i64
@@ -212,6 +216,17 @@ class Ref:
                                      _d(inp.vxc_mo), om.shape[0], _d(om), _i(states), len(states), eta,
                                      1 if backend == "blas-lapack" else 0, panel, _d(q)))
         return q
+
+    def resident(self, inp, states=None, vph=True):
+        """The reference's V_ph (n x n) and the panel columns of `states` as rows (nstates*nmo x n)."""
+        n = inp.nocc * (inp.nmo - inp.nocc)
+        v = np.zeros((n, n)) if vph else None
+        panel = np.zeros((len(states) * inp.nmo, n)) if states is not None else None
+        st = np.ascontiguousarray(states if states is not None else [0], dtype=np.int64)
+        self._chk(self.lib.ref_resident(inp.nmo, inp.nocc, inp.fermi_energy, _d(inp.mo_energy), _d(inp.eri_mo),
+                                        _d(inp.vxc_mo), st.ctypes.data_as(_ip), len(states) if states is not None
+                                        else 0, _d(v), _d(panel)))
+        return v, panel
 
     def pair_seconds(self, inp, omegas_fp, weights_fp, omega_n, states, backend="blas-lapack", threads=1):
         sec = C.c_double()

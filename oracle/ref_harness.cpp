@@ -15,6 +15,9 @@
 //   ref_run_g0w0    -- gw::run_g0w0 itself (single selected state or all states).
 //   ref_forms       -- q[f,s,k] = x^T W_c(iw_f) x via HostScreeningWorkspace
 //                      (src/workspace/screening_workspace.cpp:21-102).
+//   ref_resident    -- V_ph (calculate_v_ph_matrix) and the panel columns of the
+//                      requested states (PqPhPanelView::make_panel), for bit-exact
+//                      checks of the device gathers.
 //   ref_pair_seconds-- wall time of the body of the reference's per-(f_n, f') loop
 //                      (src/gw/sigma_c_driver.cpp:133-164) over `npairs` pairs,
 //                      run on `threads` OpenMP threads like the reference's OpenMP
@@ -172,6 +175,37 @@ int ref_forms(i64 nmo, i64 nocc, double fermi, const double* mo, const double* e
                     for (std::size_t kk = 0; kk < width; ++kk)
                         q[(static_cast<std::size_t>(f * nstates + s)) * unmo + k0 + kk] = vals[kk];
                 }
+            }
+        }
+        return 0;
+    } catch (const std::exception& e) {
+        g_last_error = e.what();
+        return -1;
+    }
+}
+
+// The reference's V_ph (gw::calculate_v_ph_matrix, src/gw/sigma.cpp:56-71) into vph_out (n x n, may be
+// NULL) and, for each state, the panel columns k = 0..nmo-1 of PqPhPanelView::make_panel
+// (src/workspace/pq_ph_panel.cpp:18-47) transposed into panel_out rows s*nmo + k (may be NULL).
+int ref_resident(i64 nmo, i64 nocc, double fermi, const double* mo, const double* eri, const double* vxc,
+                 const i64* states, i64 nstates, double* vph_out, double* panel_out) {
+    try {
+        gw::GwInput in = make_input(nmo, nocc, fermi, mo, eri, vxc);
+        gw::OrbitalSpace orbitals(in.mo_energy, in.nocc, in.fermi_energy);
+        gw::MolecularIntegrals integrals(std::move(in.eri_mo), std::move(in.vxc_mo));
+        const gw::ParticleHoleBasis ph(orbitals);
+        const std::size_t n = ph.size(), unmo = static_cast<std::size_t>(nmo);
+        if (vph_out) {
+            const gw::MatrixReal v = gw::calculate_v_ph_matrix(integrals, ph);
+            std::memcpy(vph_out, v.data().data(), sizeof(double) * v.size());
+        }
+        if (panel_out) {
+            const gw::workspace::PqPhPanelView view(integrals, ph);
+            for (i64 s = 0; s < nstates; ++s) {
+                const gw::MatrixReal x = view.make_panel(static_cast<std::size_t>(states[s]), 0, unmo);
+                double* dst = panel_out + static_cast<std::size_t>(s) * unmo * n;
+                for (std::size_t r = 0; r < n; ++r)
+                    for (std::size_t k = 0; k < unmo; ++k) dst[k * n + r] = x(r, k);
             }
         }
         return 0;

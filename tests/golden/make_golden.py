@@ -1,7 +1,7 @@
 """Regenerate the committed golden fixtures under tests/golden/ (run in a container that has
 the reference tree; the fixtures then travel with the repository).
 
-    python tests/golden/make_golden.py [--ref-root /root/reference]
+    MINIGW_REF_ROOT=<reference tree> python tests/golden/make_golden.py [--ref-root <reference tree>]
 
 1. h2o/: the reference's own H2O regression vectors, copied verbatim from
    regression_tests/h2o_serial/ -- gw_input.h5 (the input), E_c_before_Pade.out (200 complex
@@ -15,6 +15,7 @@ the reference tree; the fixtures then travel with the repository).
 from __future__ import annotations
 
 import argparse
+import os
 import shutil
 import sys
 from pathlib import Path
@@ -28,8 +29,11 @@ sys.path.insert(0, str(ROOT))
 
 def main() -> None:
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref-root", default="/root/reference")
+    ap.add_argument("--ref-root", default=os.environ.get("MINIGW_REF_ROOT"),
+                    help="the reference tree (default: $MINIGW_REF_ROOT)")
     args = ap.parse_args()
+    if not args.ref_root:
+        ap.error("give --ref-root or set MINIGW_REF_ROOT")
     src = Path(args.ref_root) / "regression_tests" / "h2o_serial"
     dst = HERE / "h2o"
     dst.mkdir(exist_ok=True)

@@ -231,6 +231,33 @@ def test_graph_replay_matches_eager_and_follows_reloads(monkeypatch):
 
 
 @pytest.mark.gpu
+def test_graph_recaptured_when_chunk_boundaries_move(monkeypatch):
+    """The same plan cut into the same number of launch sequences with other boundaries (chunk cap
+    20 -> 25 on 60 matrices: 20/20/20 -> 25/25/10) must not replay the old graph."""
+    from minigw_b200 import B200Backend, run_g0w0_batch
+
+    inputs = _systems([(16, 3), (22, 4), (26, 4)], seed0=1200)
+    states = [_states(inp) for inp in inputs]
+    bes = [B200Backend(0) for _ in inputs]
+    try:
+        for be, inp, st in zip(bes, inputs, states):
+            be.load_system(inp, st)
+        alone = [be.run_g0w0(20, 10, st, precision="mixed") for be, st in zip(bes, states)]
+        monkeypatch.setenv("GWB200_BATCH_PLAN", "single")
+        monkeypatch.setenv("GWB200_BATCH_GRAPH", "1")
+        for cap in ("20", "20", "25", "25", "20"):
+            monkeypatch.setenv("GWB200_MAX_FREQ_CHUNK", cap)
+            got = run_g0w0_batch(bes, 20, 10, states)
+            assert got["stats"]["frequency_chunks"] == 3
+            for a, s, q, st in zip(alone, got["sigma"], got["qp"], states):
+                np.testing.assert_array_equal(s, a["sigma"])
+                np.testing.assert_array_equal(q[st], a["qp"][st])
+    finally:
+        for be in bes:
+            be.close()
+
+
+@pytest.mark.gpu
 def test_batch_with_per_molecule_frequency_and_pade_counts():
     from minigw_b200 import B200Backend, run_g0w0_batch
 

@@ -8,6 +8,35 @@ import numpy as np
 import pytest
 
 
+def test_reference_arm_runs_only_the_reference():
+    """`bench.py --impl reference` maps the reference's compiled code and not libgwb200.so, takes the
+    grid from the reference, and prints the config dict the b200 arm prints for the same command."""
+    import json
+    import subprocess
+    import sys
+
+    import oracle
+    from conftest import ROOT
+
+    if not oracle.Ref.available:
+        pytest.skip("oracle/_ref was not built (reference tree absent)")
+    code = ("import sys; sys.argv=['bench.py','--impl','reference','--workload','cfg1','--steps','1','--warmup','1',"
+            "'--cpu-pairs','4']; import bench; bench.main(); maps=open('/proc/self/maps').read(); "
+            "print('MAPS', 'libgwb200' in maps, 'libgwref' in maps)")
+    r = subprocess.run([sys.executable, "-c", code], cwd=ROOT, capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr
+    lines = r.stdout.strip().splitlines()
+    assert lines[-1] == "MAPS False True"
+    out = json.loads(lines[-2])
+    import bench
+    from minigw_b200.synthetic import WORKLOADS
+
+    args = types.SimpleNamespace(precision="fp64", split_frequencies=False)
+    assert out["impl"] == "reference" and out["config"] == bench.workload_config(args, WORKLOADS["cfg1"], 1)
+    assert out["cpu_baseline"]["kind"] == "reference" and out["cpu_baseline"]["cpu_model"]
+    assert out["e2e"]["h2d_bytes_per_step"] == 0 and out["value"] > 0
+
+
 def test_batch_cpu_baseline_samples_and_interpolates(monkeypatch):
     import bench
     import minigw_b200.synthetic as syn

@@ -1,0 +1,101 @@
+"""Parity of the headline workload (nmo=200, nocc=30, nph=5100, 10 states, 128 frequencies) on the
+path the benchmark runs: the system loaded with gwb200_load_system_states, the screened forms of
+all 128 frequencies in one call with the autotuned trailing update (the int8 tensor-core
+emulation of the FP64 update on a B200), checked against the reference's own code.
+
+  * gathers: V_ph and the states' panel rows as resident on the device, bit for bit against the
+    reference's calculate_v_ph_matrix / PqPhPanelView::make_panel (oracle/_ref) and the oracle's
+    restatement (gwo_vph);
+  * screened forms q at three integration frequencies (lowest, middle, highest omega) against the
+    reference's HostScreeningWorkspace (blas-lapack backend): <= 1e-11 relative to max |q|, for the
+    autotuned path and for the FP64 DMMA path alone (GWB200_FP64_UPDATE=dmma);
+  * Sigma_c: the contribution of each sampled f' (gwb200_sigma_c_shard over [f', f'+1)) against
+    the oracle's contraction of the reference's forms at f' (<= 1e-10 Ha), and the full Sigma_c
+    against the oracle's contraction of the device's own 128-frequency forms (<= 1e-10 Ha).
+
+The input is the benchmark's generator (the ERI product on the GPU, then on the host).
+"""
+from __future__ import annotations
+
+import os
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+SIGMA_ATOL = 1e-10
+FORMS_RTOL = 1e-11
+FSEL = (0, 64, 127)
+
+
+@pytest.fixture(scope="module")
+def cfg3():
+    import oracle
+    from minigw_b200 import B200Backend, generate_transformed_legendre_grid
+    from minigw_b200.synthetic import WORKLOADS, make_input_on_device
+
+    if not oracle.Ref.available:
+        pytest.skip("oracle/_ref was not built (reference tree absent at build time)")
+    wl = WORKLOADS["cfg3"]
+    inp = make_input_on_device(wl.nmo, wl.nocc, seed=0, device=0, pin=False)
+    om, w = generate_transformed_legendre_grid(wl.nfreq)
+    states = list(wl.states)
+    ref = oracle.Ref(blas_threads=os.cpu_count())
+    with B200Backend(0) as be:
+        be.load_system(inp, states)
+        q_all, stats = be.screened_forms(om, states)
+        kernel = be.update_kernel()
+        sig, _ = be.sigma_c(om, w, states)
+        shards = {f: be.sigma_c_shard(om, w, f, f + 1, states)[0] for f in FSEL}
+        vph, panel = be.read_resident(states)
+        os.environ["GWB200_FP64_UPDATE"] = "dmma"
+        try:
+            q_dmma, _ = be.screened_forms(om[list(FSEL)], states)
+            kernel_dmma = be.update_kernel()
+        finally:
+            os.environ.pop("GWB200_FP64_UPDATE", None)
+    rq = ref.forms(inp, om[list(FSEL)], states, backend="blas-lapack")
+    yield {"wl": wl, "inp": inp, "om": om, "w": w, "states": states, "ref": ref, "q_all": q_all, "stats": stats,
+           "kernel": kernel, "sig": sig, "shards": shards, "vph": vph, "panel": panel, "q_dmma": q_dmma,
+           "kernel_dmma": kernel_dmma, "rq": rq}
+
+
+def test_cfg3_gathers_bit_exact(cfg3, oracle_lib):
+    rv, rp = cfg3["ref"].resident(cfg3["inp"], cfg3["states"])
+    np.testing.assert_array_equal(cfg3["vph"], rv)
+    np.testing.assert_array_equal(cfg3["panel"], rp)
+    np.testing.assert_array_equal(cfg3["vph"], oracle_lib.vph(cfg3["inp"]))
+
+
+def test_cfg3_forms_default_path_against_reference(cfg3):
+    assert cfg3["stats"]["nph"] == 5100 and cfg3["stats"]["ncols"] == 2000
+    assert cfg3["kernel"] in (0, 1, 2, 3, 4, 5, 6)  # an FP64 update (6: the int8 emulation)
+    rq = cfg3["rq"]
+    assert np.abs(rq.imag).max() <= 1e-9 * np.abs(rq.real).max()
+    q = cfg3["q_all"][list(FSEL)]
+    err = np.abs(q - rq.real).max() / np.abs(rq.real).max()
+    assert err <= FORMS_RTOL, (err, cfg3["kernel"])
+
+
+def test_cfg3_forms_dmma_path_against_reference(cfg3):
+    assert cfg3["kernel_dmma"] in (0, 1, 2, 3, 4, 5)
+    rq = cfg3["rq"]
+    err = np.abs(cfg3["q_dmma"] - rq.real).max() / np.abs(rq.real).max()
+    assert err <= FORMS_RTOL, err
+
+
+def test_cfg3_sigma_c_against_oracle_contraction(cfg3, oracle_lib):
+    inp, om, w, states = cfg3["inp"], cfg3["om"], cfg3["w"], cfg3["states"]
+    # each sampled f': the device's contribution against the oracle's contraction of the
+    # reference's forms at that f'
+    for j, f in enumerate(FSEL):
+        wf = np.zeros_like(w)
+        wf[f] = w[f]
+        qf = np.zeros((len(om), len(states), inp.nmo), dtype=np.complex128)
+        qf[f] = cfg3["rq"][j]
+        ref_part = oracle_lib.sigma_from_forms(inp, om, wf, states, qf)
+        assert np.abs(cfg3["shards"][f] - ref_part).max() <= SIGMA_ATOL, f
+    # the whole grid: the device's Sigma_c against the oracle's contraction of the device's forms
+    full = oracle_lib.sigma_from_forms(inp, om, w, states, cfg3["q_all"].astype(np.complex128))
+    assert np.abs(cfg3["sig"] - full).max() <= SIGMA_ATOL

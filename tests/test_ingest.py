@@ -27,6 +27,30 @@ def test_state_bound_load_is_bit_identical(nmo, nocc, states, precision):
         np.testing.assert_array_equal(a["qp"][states], b["qp"][states])
 
 
+@pytest.mark.parametrize("nmo,nocc,states", CASES[:2] + [(120, 20, [17, 18, 19, 20, 21, 22])])
+def test_gathers_bit_exact_against_reference(nmo, nocc, states, oracle_lib):
+    """Both ingest paths' resident V_ph and panel rows, bit for bit against the reference's
+    calculate_v_ph_matrix (src/gw/sigma.cpp:56-71) and PqPhPanelView::make_panel
+    (src/workspace/pq_ph_panel.cpp:18-47), and the oracle's gwo_vph."""
+    import oracle
+    from minigw_b200 import B200Backend
+    from minigw_b200.synthetic import make_input
+
+    inp = make_input(nmo, nocc, seed=900 + nmo)
+    with B200Backend(0) as full, B200Backend(0) as bound:
+        full.load_system(inp)  # V_ph and panels gathered on the device from the (pq|o.) block
+        bound.load_system(inp, states)  # copied from the host ERI by 3D copies
+        va, pa = full.read_resident(states)
+        vb, pb = bound.read_resident(states)
+    np.testing.assert_array_equal(va, vb)
+    np.testing.assert_array_equal(pa, pb)
+    np.testing.assert_array_equal(va, oracle_lib.vph(inp))
+    if oracle.Ref.available:
+        rv, rp = oracle.Ref().resident(inp, states)
+        np.testing.assert_array_equal(va, rv)
+        np.testing.assert_array_equal(pa, rp)
+
+
 def test_state_bound_load_complex_forms_and_shards():
     from minigw_b200 import B200Backend, generate_transformed_legendre_grid
     from minigw_b200.synthetic import make_input

@@ -80,3 +80,18 @@ def test_noalloc_rejects_oversize_and_host_pointers():
     p = C.c_void_p(host.ctypes.data)
     rc = lib.gwb200_screened_forms_noalloc(4, 4, p, p, p, p, 2, p, None)
     assert STATUS[rc] == "GWB200_BAD_ARGUMENT"
+
+
+def test_noalloc_rejects_memory_of_another_device():
+    import torch
+
+    from minigw_b200._lib import STATUS, lib
+
+    if torch.cuda.device_count() < 2:
+        pytest.skip("needs a second GPU")
+    other = torch.zeros(64, dtype=torch.float64, device="cuda:1")
+    p = C.c_void_p(other.data_ptr())
+    torch.cuda.set_device(0)
+    rc = lib.gwb200_screened_forms_noalloc(4, 4, p, p, p, p, 2, p, None)
+    assert STATUS[rc] == "GWB200_BAD_ARGUMENT"
+    assert b"not of the current device" in lib.gwb200_last_error()
