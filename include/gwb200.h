@@ -42,9 +42,15 @@ typedef enum gwb200_status {
 
 typedef enum gwb200_precision {
     GWB200_FP64 = 0,             /* plain form: FP64 throughout (the drop-in) */
-    GWB200_MIXED = 1             /* mixed form (eta == 0): FP32 tall matrices, FP64 diagonal blocks, 3xTF32
+    GWB200_MIXED = 1,            /* mixed form (eta == 0): FP32 tall matrices, FP64 diagonal blocks, 3xTF32
                                   * tensor-core panel solves and updates, FP64 norms / contraction / Pade /
-                                  * QP; FP32-level error, no FP64 refinement */
+                                  * QP; FP32-level error (~1e-7 relative), no FP64 refinement */
+    GWB200_MIXED_REFINED = 2     /* the mixed factorisation brought to FP64 accuracy (eta == 0): a backward
+                                  * solve against the FP32 factor gives z ~ eps^{-1} D^1/2 x, and the forms
+                                  * are the energy functional -(2 x^T D^1/2 z - z^T eps z) evaluated in FP64
+                                  * (error quadratic in the FP32 solve error, ~1e-14 relative); y^T V y
+                                  * through a pivoted Cholesky factor of V computed once per loaded system.
+                                  * gwb200_screened_forms / sigma_c / sigma_c_shard / run_g0w0 only */
 } gwb200_precision;
 
 typedef struct gwb200_stats {

@@ -14,7 +14,7 @@ from __future__ import annotations
 
 import importlib
 
-_LIB_NAMES = ("FP64", "MIXED", "STATUS", "GwB200Error", "version")
+_LIB_NAMES = ("FP64", "MIXED", "MIXED_REFINED", "STATUS", "GwB200Error", "version")
 _GW_NAMES = (
     "B200Backend", "B200Server", "GwInput", "GwResult", "GwSettings", "GwTimings",
     "generate_transformed_legendre_grid", "output_final_energy_table", "output_self_energy_after_pade",

@@ -29,6 +29,7 @@ STATUS_CODE = {v: k for k, v in STATUS.items()}
 
 FP64 = 0
 MIXED = 1
+MIXED_REFINED = 2
 
 # Every symbol include/gwb200.h declares.
 EXPORTS = (

@@ -131,6 +131,11 @@ struct gwb200_handle {
     DevBuf panel32;   // operand workspace of the tcgen05 trailing updates (mixed: FP32 hi/lo split;
                       // plain with GWB200_FP64_UPDATE=ozaki: int8 digit slices + exponents)
     DevBuf tc_sched;  // work counter of the tcgen05 update kernel
+    // GWB200_MIXED_REFINED: pivoted Cholesky factor of the resident V_ph (computed on first use after
+    // a load; pchol_rank < 0: not yet) and the per-chunk refinement workspace
+    DevBuf pchol, refine;
+    int64_t pchol_rank = -1;
+    double* pchol_ct = nullptr;
     DevBuf batch_desc;  // BatchGroup tables of gwb200_run_g0w0_batch (when this handle leads a batch)
     BatchLane lanes[kMaxBatchLanes];  // streams + workspaces of the batches this handle leads
     cudaEvent_t batch_fork = nullptr;
@@ -213,8 +218,10 @@ void compute_forms(gwb200_handle* h, const double* omega, int64_t nfreq, const i
     if (nfreq <= 0) fail(GWB200_BAD_SHAPE, "--freq-points must be positive");
     check_states(h, states, nstates);
     if (!std::isfinite(eta)) fail(GWB200_BAD_ARGUMENT, "non-finite eta");
-    if (precision != GWB200_FP64 && precision != GWB200_MIXED) fail(GWB200_BAD_ARGUMENT, "unknown precision");
-    const bool mixed = precision == GWB200_MIXED;
+    if (precision != GWB200_FP64 && precision != GWB200_MIXED && precision != GWB200_MIXED_REFINED)
+        fail(GWB200_BAD_ARGUMENT, "unknown precision");
+    const bool mixed = precision != GWB200_FP64;
+    const bool refine = precision == GWB200_MIXED_REFINED;
     if (mixed && eta != 0.0) fail(GWB200_BAD_ARGUMENT, "the mixed-precision form requires eta == 0");
     const bool cplx = eta != 0.0;  // eta != 0: complex symmetric factorisation
     if (!cplx && h->bad_gap)
@@ -259,8 +266,18 @@ void compute_forms(gwb200_handle* h, const double* omega, int64_t nfreq, const i
     // (its slice workspace is part of the budget) unless GWB200_FP64_UPDATE=dmma; memory-capped
     // handles use it only when it is forced (GWB200_FP64_UPDATE=ozaki)
     const bool fp64_oz = !mixed && !cplx && fp64_update_mode() != 1 && (h->mem_limit <= 0 || fp64_update_mode() == 2);
+    // refined mixed form: V_ph = C C^T once per loaded system (its rank sizes the correction's work)
+    int64_t r_pad = 0;
+    if (refine) {
+        if (h->pchol_rank < 0) {
+            size_buffer(h, h->pchol, pchol_bytes(h->n));
+            h->pchol_rank = launch_pchol(h->v.as<double>(), h->n, h->pchol.p, &h->pchol_ct, s);
+        }
+        r_pad = std::max<int64_t>(kNb, round_up(h->pchol_rank, kNb));
+    }
     const size_t per_freq = mixed ? sizeof(float) * ((size_t)g.stride + kNb * kNb) + sizeof(double) * (g.n_pad + g.m_pad) +
-                                        (mixed_tc ? tc_panel_bytes_per_freq(g) : 0)
+                                        (mixed_tc ? tc_panel_bytes_per_freq(g) : 0) +
+                                        (refine ? refine_bytes_per_freq(g, r_pad) : 0)
                                   : sizeof(double) * planes * ((size_t)g.stride + g.n_pad + kNb * kNb + g.m_pad) +
                                         (fp64_oz ? oz_slice_bytes_per_freq(g) : 0);
     // GWB200_MAX_FREQ_CHUNK caps the chunk (tests use it to exercise the multi-chunk path).
@@ -273,12 +290,13 @@ void compute_forms(gwb200_handle* h, const double* omega, int64_t nfreq, const i
     } else {
         size_t free_b = 0, total_b = 0;
         GWB_CUDA(cudaMemGetInfo(&free_b, &total_b));
-        const size_t have = h->a.bytes + h->dvec.bytes + h->linv.bytes + h->qacc.bytes + h->panel32.bytes;
+        const size_t have =
+            h->a.bytes + h->dvec.bytes + h->linv.bytes + h->qacc.bytes + h->panel32.bytes + h->refine.bytes;
         size_t avail = free_b + have;  // what the chunk buffers may occupy
         size_t budget = (size_t)((double)avail * 0.85);
         if (h->mem_limit > 0) {  // the handle's cap minus what the system and panels already hold
             const size_t resident = h->pqo.bytes + h->xdiag.bytes + h->v.bytes + h->xt.bytes + h->qall.bytes +
-                                    h->sigma.bytes + h->qp_scratch.bytes + ((size_t)1 << 20);
+                                    h->sigma.bytes + h->qp_scratch.bytes + h->pchol.bytes + ((size_t)1 << 20);
             const size_t lim = (size_t)h->mem_limit;
             const size_t room = lim > resident ? lim - resident : 0;
             budget = std::min(budget, room);
@@ -302,6 +320,7 @@ void compute_forms(gwb200_handle* h, const double* omega, int64_t nfreq, const i
         size_buffer(h, h->panel32, oz_slice_bytes_per_freq(g) * (size_t)fc);
         h->tc_sched.ensure(sizeof(unsigned long long));
     }
+    if (refine) size_buffer(h, h->refine, refine_bytes_per_freq(g, r_pad) * (size_t)fc);
 
     GWB_CUDA(cudaEventRecord(h->ev[0], s));
     if (!bound)
@@ -335,6 +354,12 @@ void compute_forms(gwb200_handle* h, const double* omega, int64_t nfreq, const i
                                               h->err.as<unsigned long long>(), s, prof.enabled ? &prof : nullptr,
                                               mixed_tc ? h->panel32.as<float>() : nullptr,
                                               h->tc_sched.as<unsigned long long>(), h->persistent_ctas);
+            if (refine)  // qacc <- 2 x^T y - z^T z - y^T V y (FP64 energy functional at the FP32 solve)
+                launches += launch_refine_chunk(g, nf, h->a.as<float>(), h->linv.as<float>(), h->xt.as<double>(),
+                                                h->dvec.as<double>(), h->pchol_ct, r_pad, h->refine.p,
+                                                h->qacc.as<double>(), h->err.as<unsigned long long>(), s,
+                                                mixed_tc ? h->panel32.as<float>() : nullptr,
+                                                h->tc_sched.as<unsigned long long>(), h->persistent_ctas);
         } else {
             if (upd_variant < 0)
                 upd_variant = tune_update_variant(g, nf, h->a.as<double>(), s, fp64_oz ? h->panel32.p : nullptr,
@@ -612,7 +637,7 @@ int gwb200_destroy(gwb200_handle* h) {
     if (h->stream) cudaStreamSynchronize(h->stream);
     h->stage_in.release();
     h->stage_out.release();
-    for (DevBuf* b : {&h->pqo, &h->xdiag, &h->mo, &h->vxc_diag, &h->delta, &h->v, &h->sigx, &h->flag, &h->xt, &h->dvec, &h->a,
+    for (DevBuf* b : {&h->pchol, &h->refine, &h->pqo, &h->xdiag, &h->mo, &h->vxc_diag, &h->delta, &h->v, &h->sigx, &h->flag, &h->xt, &h->dvec, &h->a,
                       &h->linv, &h->qacc, &h->qall, &h->sigma, &h->omega, &h->weight, &h->states, &h->err, &h->qp,
                       &h->qp_scratch, &h->omega_out, &h->panel32, &h->tc_sched, &h->batch_desc})
         b->release();
@@ -671,10 +696,13 @@ void load_system_impl(gwb200_handle* h, int64_t nmo, int64_t nocc, const double*
     cudaStream_t s = h->stream;
     h->loaded = false;
     h->bound_states.clear();
+    h->pchol_rank = -1;  // the factor of the previous system's V_ph is stale
+    h->pchol_ct = nullptr;
     const size_t nmo2 = (size_t)nmo * nmo;
     const int64_t nvir = nmo - nocc, n = nocc * nvir;
     if (h->mem_limit > 0)  // drop the previous request's workspaces before sizing this system
-        for (DevBuf* b : {&h->xt, &h->dvec, &h->a, &h->linv, &h->qacc, &h->qall, &h->panel32}) b->release();
+        for (DevBuf* b : {&h->xt, &h->dvec, &h->a, &h->linv, &h->qacc, &h->qall, &h->panel32, &h->pchol, &h->refine})
+            b->release();
     if (bound) {
         h->pqo.release();
         size_buffer(h, h->xt, sizeof(double) * (size_t)nstates * nmo * n);

@@ -175,7 +175,19 @@ int launch_build_tall32(const TallGeometry& g, const double* v, const double* xt
 // split-panel workspace (tc_panel_bytes_per_freq(g) bytes per frequency); NULL: mma.sync.
 int launch_factor_chunk32(const TallGeometry& g, int64_t nf, float* a, float* linv, double* qacc,
                           unsigned long long* err_pivot, cudaStream_t s, UpdateProfiler* prof, float* panel,
-                          unsigned long long* sched, int max_ctas = 0);
+                          unsigned long long* sched, int max_ctas = 0, bool solve_only = false);
+// kernels_refine.cu: FP64 energy-functional correction of the mixed form.  launch_pchol factors
+// V = C C^T (pivoted, FP64; `work` of pchol_bytes(n)), returns the rank r and C^T (r_pad x n_pad,
+// r_pad = max(64, r rounded up to 64)) in *ct_out (inside `work`).  launch_refine_chunk runs after
+// launch_factor_chunk32 on the same chunk: the backward solve against the FP32 factor (solve-only
+// pass), then qacc[f][j] = 2 x^T y - z^T z - y^T V y (`work`: refine_bytes_per_freq(g, r_pad) * nf).
+size_t refine_bytes_per_freq(const TallGeometry& g, int64_t r_pad);
+size_t pchol_bytes(int64_t n);
+int64_t launch_pchol(const double* v, int64_t n, void* work, double** ct_out, cudaStream_t s);
+int launch_refine_chunk(const TallGeometry& g, int64_t nf, float* a, float* linv, const double* xt,
+                        const double* dvec, const double* ct, int64_t r_pad, void* work, double* qacc,
+                        unsigned long long* err_pivot, cudaStream_t s, float* panel, unsigned long long* sched,
+                        int max_ctas);
 // kernels_tc.cu: tcgen05 3xTF32 trailing update C -= P P^T of the mixed form (K = kdim columns from
 // kb0, output columns [c_begin, n_pad), rows [c_begin, rows)).  Two launches; `sched` is one
 // device word the kernel's work counter lives in.  A device wait that expires records pivot 0 in
@@ -183,7 +195,7 @@ int launch_factor_chunk32(const TallGeometry& g, int64_t nf, float* a, float* li
 size_t tc_panel_bytes_per_freq(const TallGeometry& g);
 int launch_update32_tc(const TallGeometry& g, int64_t nf, float* a, int64_t kb0, int kdim, int64_t c_begin,
                        float* panel, unsigned long long* sched, unsigned long long* err_pivot, cudaStream_t s,
-                       int max_ctas = 0);
+                       int max_ctas = 0, int64_t row_min = 0);
 // kernels_c64.cu: eta != 0 (complex symmetric M = I - S V S, S = diag(Pi0)^1/2).  Planes a_re/a_im
 // of geometry g; svec 2*n_pad, linv 2*64*64, qacc 2*m_pad doubles per frequency.
 int launch_factor_chunk_c(const TallGeometry& g, int64_t nf, const double* delta, const double* omega, double eta,

@@ -107,8 +107,11 @@ __global__ void k_build_tall32(int64_t n, int64_t m, int64_t n_pad, int64_t ld, 
 // Diagonal block in FP64 (from the FP32 tall matrix), written back as FP32 L and FP32 L^{-1}.
 // One 64 x 65 FP64 tile: L in the lower triangle, Y = L^{-1} (lower too) transposed into the
 // upper triangle (Y[l][c] at T[c][l], l > c) with its diagonal in Yd, so 6 CTAs fit an SM.
+// invert_only: the block already holds a Cholesky factor (the solve-only pass of the mixed form's
+// refinement); only its inverse is formed and the block is left as it is.
 __global__ void __launch_bounds__(256) k_potrf_diag32(float* __restrict__ a, int64_t ld, int64_t stride, int64_t k,
-                                                      float* __restrict__ linv, unsigned long long* err_pivot) {
+                                                      float* __restrict__ linv, unsigned long long* err_pivot,
+                                                      int invert_only) {
     extern __shared__ double smem[];
     constexpr int L = kNb + 1;
     double* T = smem;
@@ -120,7 +123,7 @@ __global__ void __launch_bounds__(256) k_potrf_diag32(float* __restrict__ a, int
         T[i * L + j] = (j <= i) ? (double)A[(size_t)i * ld + j] : 0.0;
     }
     __syncthreads();
-    for (int j = 0; j < kNb; ++j) {
+    for (int j = 0; j < kNb && !invert_only; ++j) {
         if (tid == 0) {
             double piv = T[j * L + j];
             if (!(piv > 0.0)) {
@@ -140,10 +143,11 @@ __global__ void __launch_bounds__(256) k_potrf_diag32(float* __restrict__ a, int
         }
         __syncthreads();
     }
-    for (int idx = tid; idx < kNb * kNb; idx += blockDim.x) {
-        const int i = idx / kNb, j = idx % kNb;
-        if (j <= i) A[(size_t)i * ld + j] = (float)T[i * L + j];
-    }
+    if (!invert_only)
+        for (int idx = tid; idx < kNb * kNb; idx += blockDim.x) {
+            const int i = idx / kNb, j = idx % kNb;
+            if (j <= i) A[(size_t)i * ld + j] = (float)T[i * L + j];
+        }
     {
         const int col = tid >> 2, part = tid & 3;
         for (int i = 0; i < kNb; ++i) {
@@ -167,15 +171,16 @@ __global__ void __launch_bounds__(256) k_potrf_diag32(float* __restrict__ a, int
     }
 }
 
-// Panel solve P <- P Linv^T on the tensor cores (3xTF32); RHS rows add their squared norms (FP64).
+// Panel solve P <- P Linv^T on the tensor cores (3xTF32) for the 64-row blocks from row0 on; RHS
+// rows add their squared norms (FP64) to qacc unless it is null.
 __global__ void __launch_bounds__(256) k_trsm_panel32(float* __restrict__ a, int64_t ld, int64_t stride, int64_t k,
-                                                      int64_t n_pad, const float* __restrict__ linv,
+                                                      int64_t row0, int64_t n_pad, const float* __restrict__ linv,
                                                       double* __restrict__ qacc, int64_t ldq) {
     extern __shared__ float fsm[];
     float* Ps = fsm;
     float* Ls = fsm + 64 * kLdf;
     const int f = blockIdx.y;
-    const int64_t r0 = k + kNb + (int64_t)blockIdx.x * kNb;
+    const int64_t r0 = row0 + (int64_t)blockIdx.x * kNb;
     float* A = a + (size_t)f * stride;
     load_f32_async<64, kLdf>(Ps, A + r0 * ld + k, ld);
     load_f32_async<64, kLdf>(Ls, linv + (size_t)f * kNb * kNb, kNb);
@@ -201,7 +206,7 @@ __global__ void __launch_bounds__(256) k_trsm_panel32(float* __restrict__ a, int
         *reinterpret_cast<float4*>(A + (size_t)(r0 + r) * ld + k + 4 * c4) =
             *reinterpret_cast<const float4*>(Ps + r * kLdf + 4 * c4);
     }
-    if (r0 >= n_pad && threadIdx.x < kNb) {
+    if (qacc && r0 >= n_pad && threadIdx.x < kNb) {
         const int r = threadIdx.x;
         double s = 0.0;
         for (int j = 0; j < kNb; ++j) {
@@ -213,15 +218,16 @@ __global__ void __launch_bounds__(256) k_trsm_panel32(float* __restrict__ a, int
 }
 
 // Trailing / look-left update on FP32 tiles (3xTF32), same tile enumeration and K chunking as the
-// FP64 k_update: output column tiles [tc0, tc0+T), lower square tiles then all RHS tiles.
+// FP64 k_update: output column tiles [tc0, tc0+T), lower square tiles then all RHS tiles
+// (rhs_only: the RHS tiles alone, for the solve-only pass against a finished factor).
 __global__ void __launch_bounds__(256, 3) k_update32(float* __restrict__ a, int64_t ld, int64_t stride, int64_t kb0,
-                                                     int nk, int64_t tc0, int64_t T, int64_t nsq) {
+                                                     int nk, int64_t tc0, int64_t T, int64_t nsq, int rhs_only) {
     extern __shared__ float fsm[];
     auto stage = [&](int st, int which) { return fsm + (2 * st + which) * 64 * kLdkf; };
     const int f = blockIdx.y;
-    const int64_t x = blockIdx.x;
     const int64_t Lr = nsq - tc0;
-    const int64_t n_square = T * Lr - T * (T - 1) / 2;
+    const int64_t n_square = rhs_only ? 0 : T * Lr - T * (T - 1) / 2;
+    const int64_t x = blockIdx.x;
     int64_t c, tr;
     if (x < n_square) {
         const double b = 2.0 * (double)Lr + 1.0;
@@ -292,7 +298,7 @@ int launch_build_tall32(const TallGeometry& g, const double* v, const double* xt
 
 int launch_factor_chunk32(const TallGeometry& g, int64_t nf, float* a, float* linv, double* qacc,
                           unsigned long long* err_pivot, cudaStream_t s, UpdateProfiler* prof, float* panel,
-                          unsigned long long* sched, int max_ctas) {
+                          unsigned long long* sched, int max_ctas, bool solve_only) {
     const size_t smem_tile = 2 * 64 * kLdf * sizeof(float);
     const size_t smem_update = 4 * 64 * kLdkf * sizeof(float);
     const size_t smem_potrf = (kNb * (kNb + 1) + kNb) * sizeof(double);
@@ -307,10 +313,11 @@ int launch_factor_chunk32(const TallGeometry& g, int64_t nf, float* a, float* li
     UpdateProfiler* lprof = panel ? nullptr : prof;
     auto update = [&](int64_t kb0, int nk, int64_t tc0, int64_t T) {
         const int64_t L = nsq - tc0;
-        const int64_t tiles = T * L - T * (T - 1) / 2 + T * (nrt - nsq);
+        const int64_t tiles = (solve_only ? 0 : T * L - T * (T - 1) / 2) + T * (nrt - nsq);
         if (tiles <= 0) return;
         if (lprof) lprof->begin();
-        k_update32<<<dim3((unsigned)tiles, (unsigned)nf), 256, smem_update, s>>>(a, g.ld, g.stride, kb0, nk, tc0, T, nsq);
+        k_update32<<<dim3((unsigned)tiles, (unsigned)nf), 256, smem_update, s>>>(a, g.ld, g.stride, kb0, nk, tc0, T, nsq,
+                                                                                  solve_only ? 1 : 0);
         GWB_LAUNCH("k_update32");
         if (lprof) lprof->end((double)nf * update_flops32(g, kb0, nk, tc0 * kNb, (tc0 + T) * kNb));
         ++launches;
@@ -320,13 +327,17 @@ int launch_factor_chunk32(const TallGeometry& g, int64_t nf, float* a, float* li
         for (int64_t j = 0; j < q; ++j) {
             const int64_t kt = ob + j, k = kt * kNb;
             if (j > 0) update(ob * kNb, (int)j, kt, 1);
-            k_potrf_diag32<<<(unsigned)nf, 256, smem_potrf, s>>>(a, g.ld, g.stride, k, linv, err_pivot);
+            k_potrf_diag32<<<(unsigned)nf, 256, smem_potrf, s>>>(a, g.ld, g.stride, k, linv, err_pivot,
+                                                                 solve_only ? 1 : 0);
             GWB_LAUNCH("k_potrf_diag32");
             ++launches;
-            const int64_t below = g.rows - (k + kNb);
+            // the panel rows below the block: all of them while factoring, the RHS rows alone when
+            // solving against a finished factor
+            const int64_t row0 = solve_only ? g.n_pad : k + kNb;
+            const int64_t below = g.rows - row0;
             if (below > 0) {
                 k_trsm_panel32<<<dim3((unsigned)(below / kNb), (unsigned)nf), 256, smem_tile, s>>>(
-                    a, g.ld, g.stride, k, g.n_pad, linv, qacc, g.m_pad);
+                    a, g.ld, g.stride, k, row0, g.n_pad, linv, solve_only ? nullptr : qacc, g.m_pad);
                 GWB_LAUNCH("k_trsm_panel32");
                 ++launches;
             }
@@ -336,7 +347,7 @@ int launch_factor_chunk32(const TallGeometry& g, int64_t nf, float* a, float* li
             if (panel) {  // outer trailing update on tcgen05
                 if (prof) prof->begin();
                 launches += launch_update32_tc(g, nf, a, ob * kNb, (int)(q * kNb), tc0 * kNb, panel, sched, err_pivot, s,
-                                                max_ctas);
+                                                max_ctas, solve_only ? g.n_pad : 0);
                 if (prof) prof->end((double)nf * update_flops32(g, ob * kNb, (int)q, tc0 * kNb, nsq * kNb));
             } else {
                 update(ob * kNb, (int)q, tc0, nsq - tc0);

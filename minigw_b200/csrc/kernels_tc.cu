@@ -184,7 +184,7 @@ __device__ __forceinline__ bool decode_unit(const UnitSpace& us, int64_t u, int&
 
 __global__ void __launch_bounds__(kTcThreads, 1)
     k_update32_tc(float* __restrict__ a, int64_t ld, int64_t stride, int64_t c_begin, int64_t rows, int64_t n_pad,
-                  int nkc, const float* __restrict__ panel, int64_t rp, UnitSpace us,
+                  int64_t row_min, int nkc, const float* __restrict__ panel, int64_t rp, UnitSpace us,
                   unsigned long long* __restrict__ sched, unsigned long long* err, int withhold_first_stage,
                   const __grid_constant__ CUtensorMap cmap) {
     extern __shared__ __align__(1024) uint8_t tsm[];
@@ -409,7 +409,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                     // lower part at 64-column-block granularity (the diagonal 64x64 blocks in full): a
                     // 32-row box starting at a multiple of 32 is wholly in or wholly out; rows past
                     // `rows` are clipped by the tensor map
-                    const bool box = cj < n_pad && rs < rows && rs >= (cj & ~(int64_t)63);
+                    const bool box = cj < n_pad && rs < rows && rs >= (cj & ~(int64_t)63) && rs >= row_min;
                     float acc[32];
                     tmem_ld32(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(ab * kTcN + half * 64 + b * 32), acc);
                     if (b == 1) {  // both halves read: the accumulator is free
@@ -513,7 +513,8 @@ size_t tc_panel_bytes_per_freq(const TallGeometry& g) {
 }
 
 int launch_update32_tc(const TallGeometry& g, int64_t nf, float* a, int64_t kb0, int kdim, int64_t c_begin,
-                       float* panel, unsigned long long* sched, unsigned long long* err, cudaStream_t s, int max_ctas) {
+                       float* panel, unsigned long long* sched, unsigned long long* err, cudaStream_t s, int max_ctas,
+                       int64_t row_min) {
     if (kdim <= 0 || kdim > 128 || kdim % kTcKc != 0)
         fail(GWB200_BAD_SHAPE, "tcgen05 update: K must be 32, 64, 96 or 128");
     const int64_t T = (g.n_pad - c_begin + kTcN - 1) / kTcN;  // the last column tile may be 64 wide
@@ -553,7 +554,9 @@ int launch_update32_tc(const TallGeometry& g, int64_t nf, float* a, int64_t kb0,
     us.T = T;
     us.NI = NI;
     us.NS = (T + kTcSeg - 1) / kTcSeg;
-    us.per_f = NI * us.NS;
+    // row_min > c_begin (the solve-only pass): only the row tiles that reach row_min have work
+    const int64_t i0 = std::max<int64_t>(0, (row_min - c_begin) / kTcM);
+    us.per_f = (NI - i0) * us.NS;
     us.total = nf * us.per_f;
     GWB_CUDA(cudaMemsetAsync(sched, 0, sizeof(unsigned long long), s));
     const unsigned grid = (unsigned)std::min<int64_t>(us.total, max_ctas > 0 ? std::min(max_ctas, sm_count()) : sm_count());
@@ -561,8 +564,8 @@ int launch_update32_tc(const TallGeometry& g, int64_t nf, float* a, int64_t kb0,
     // device wait expires and the call reports GWB200_DEVICE_TIMEOUT with the context intact.
     const char* expire = std::getenv("GWB200_TEST_EXPIRE_WAIT");
     const int withhold = (expire && expire[0] == '1') ? 1 : 0;
-    k_update32_tc<<<grid, kTcThreads, kTcSmem, s>>>(a, g.ld, g.stride, c_begin, g.rows, g.n_pad, nkc, panel, rp, us,
-                                                     sched, err, withhold, cmap);
+    k_update32_tc<<<grid, kTcThreads, kTcSmem, s>>>(a, g.ld, g.stride, c_begin, g.rows, g.n_pad, row_min, nkc, panel, rp,
+                                                     us, sched, err, withhold, cmap);
     GWB_LAUNCH("k_update32_tc");
     return 2;
 }

@@ -23,7 +23,7 @@ from typing import Optional, Sequence
 import ctypes as C
 import numpy as np
 
-from ._lib import FP64, MIXED, GwB200Error, Request, Stats, _dp, _ip, check, dptr, iptr, lib
+from ._lib import FP64, MIXED, MIXED_REFINED, GwB200Error, Request, Stats, _dp, _ip, check, dptr, iptr, lib
 from .gw_input import GwInput
 
 HARTREE_TO_EV = 27.211386245988  # include/types.hpp:12
@@ -95,6 +95,8 @@ def _precision_code(p: str | int) -> int:
         return FP64
     if p in ("mixed", MIXED):
         return MIXED
+    if p in ("mixed-refined", MIXED_REFINED):
+        return MIXED_REFINED
     raise GwB200Error(7, f"unknown precision {p!r}")
 
 

@@ -9,6 +9,7 @@ emulation of the FP64 update on a B200), checked against the reference's own cod
   * screened forms q at three integration frequencies (lowest, middle, highest omega) against the
     reference's HostScreeningWorkspace (blas-lapack backend): <= 1e-11 relative to max |q|, for the
     autotuned path and for the FP64 DMMA path alone (GWB200_FP64_UPDATE=dmma);
+  * the refined mixed form (GWB200_MIXED_REFINED) at the same frequencies, <= 1e-10 relative;
   * Sigma_c: the contribution of each sampled f' (gwb200_sigma_c_shard over [f', f'+1)) against
     the oracle's contraction of the reference's forms at f' (<= 1e-10 Ha), and the full Sigma_c
     against the oracle's contraction of the device's own 128-frequency forms (<= 1e-10 Ha).
@@ -49,6 +50,7 @@ def cfg3():
         sig, _ = be.sigma_c(om, w, states)
         shards = {f: be.sigma_c_shard(om, w, f, f + 1, states)[0] for f in FSEL}
         vph, panel = be.read_resident(states)
+        q_refined, _ = be.screened_forms(om, states, precision="mixed-refined")
         os.environ["GWB200_FP64_UPDATE"] = "dmma"
         try:
             q_dmma, _ = be.screened_forms(om[list(FSEL)], states)
@@ -58,7 +60,7 @@ def cfg3():
     rq = ref.forms(inp, om[list(FSEL)], states, backend="blas-lapack")
     yield {"wl": wl, "inp": inp, "om": om, "w": w, "states": states, "ref": ref, "q_all": q_all, "stats": stats,
            "kernel": kernel, "sig": sig, "shards": shards, "vph": vph, "panel": panel, "q_dmma": q_dmma,
-           "kernel_dmma": kernel_dmma, "rq": rq}
+           "kernel_dmma": kernel_dmma, "rq": rq, "q_refined": q_refined}
 
 
 def test_cfg3_gathers_bit_exact(cfg3, oracle_lib):
@@ -83,6 +85,17 @@ def test_cfg3_forms_dmma_path_against_reference(cfg3):
     rq = cfg3["rq"]
     err = np.abs(cfg3["q_dmma"] - rq.real).max() / np.abs(rq.real).max()
     assert err <= FORMS_RTOL, err
+
+
+def test_cfg3_refined_mixed_forms_against_reference(cfg3):
+    """The refined mixed form (FP32 factorisation + FP64 energy-functional correction) on all 128
+    frequencies, checked at the sampled ones against the reference."""
+    rq = cfg3["rq"]
+    err = np.abs(cfg3["q_refined"][list(FSEL)] - rq.real).max() / np.abs(rq.real).max()
+    assert err <= 1e-10, err
+    # and against the plain form on every frequency
+    q = cfg3["q_all"]
+    assert np.abs(cfg3["q_refined"] - q).max() <= 1e-10 * np.abs(q).max()
 
 
 def test_cfg3_sigma_c_against_oracle_contraction(cfg3, oracle_lib):
