@@ -613,6 +613,8 @@ def run_b200(args, wl):
     if not split and args.precision == "fp64" and not args.no_mixed:
         result["mixed"] = mixed_subrecord(be, stream, wl, states, inp, om, args, local, world, max_over_ranks,
                                           barrier)
+        for prec in ("mixed-refined", "mixed"):
+            result["mixed"][prec]["ratio_vs_plain"] = result["mixed"][prec]["value"] / value
     if args.precision == "mixed":
         # error of the mixed form against the plain FP64 form on the same system (untimed)
         r32 = be.run_g0w0(wl.nfreq, wl.npade, states, precision="mixed")
