@@ -324,6 +324,36 @@ def run_reference(args, wl):
     return 0
 
 
+def memory_bound_record(kprof_timed: dict, inp, states, om, local: int) -> dict:
+    """Achieved HBM bandwidth of the memory-bound kernels: algorithmic bytes / CUDA-event time
+    (gwb200_kernel_profile).  k_build_tall and k_sigma_contract come from the timed steps.  The
+    gathers do not run on the benchmark's path (the state-bound load copies V_ph and the panel rows
+    from the host), so they are timed once on a second handle loaded with gwb200_load_system (the
+    (pq|o.) block resident): one load (k_gather_vph) and one screening call (k_gather_panel)."""
+    from minigw_b200 import B200Backend
+
+    os.environ["GWB200_PROFILE"] = "1"
+    try:
+        with B200Backend(local) as blk:
+            blk.load_system(inp)
+            blk.screened_forms(om[:1], states)
+            kp = blk.kernel_profile()
+    finally:
+        os.environ.pop("GWB200_PROFILE", None)
+    peak = hbm_peak_gbs()
+    out = {"peak_gbs": peak, "peak_source": hbm_peak_source(),
+           "note": "achieved = algorithmic bytes per launch / CUDA-event time per launch (include/gwb200.h "
+                   "gwb200_kernel_profile gives the byte counts)"}
+    for name, rec in (("k_build_tall", kprof_timed["k_build_tall"]), ("k_sigma_contract", kprof_timed["k_sigma_contract"]),
+                      ("k_gather_vph", kp["k_gather_vph"]), ("k_gather_panel", kp["k_gather_panel"])):
+        if rec["launches"] == 0 or rec["ms"] <= 0:
+            continue
+        gbs = rec["bytes"] / (rec["ms"] * 1e-3) / 1e9
+        out[name] = {"achieved_gbs": gbs, "frac": gbs / peak, "launches": rec["launches"],
+                     "ms_per_launch": rec["ms"] / rec["launches"], "bytes_per_launch": rec["bytes"] / rec["launches"]}
+    return out
+
+
 def mixed_subrecord(be, stream, wl, states, inp, om, args, local, world, max_over_ranks, barrier) -> dict:
     """The mixed forms on the same resident system, timed like the headline (K steps after warm-up,
     CUDA events on the library's stream, max over ranks, clocks sampled during the timed region):
@@ -461,6 +491,7 @@ def run_b200(args, wl):
     step()
     barrier()
     torch.cuda.synchronize()
+    be.kernel_profile()  # reset: the memory-bound kernels of the timed steps alone
     stats = []
     ev[0].record(stream)
     for i in range(args.steps):
@@ -470,6 +501,7 @@ def run_b200(args, wl):
     torch.cuda.synchronize()
     clock_info = clocks.stop()
     barrier()
+    kprof_timed = be.kernel_profile()
     os.environ.pop("GWB200_PROFILE", None)
     step_ms = [ev[i].elapsed_time(ev[i + 1]) for i in range(args.steps)]
     total_ms = ev[0].elapsed_time(ev[-1])
@@ -610,6 +642,8 @@ def run_b200(args, wl):
             "peak_source": hbm_peak_source(),
             "tflops_fp32_equivalent": achieved, "launches": upd_n, "traffic": None,
             "traffic_source": None}
+    if not split:
+        result["memory_bound"] = memory_bound_record(kprof_timed, inp, states, om, local)
     if not split and args.precision == "fp64" and not args.no_mixed:
         result["mixed"] = mixed_subrecord(be, stream, wl, states, inp, om, args, local, world, max_over_ranks,
                                           barrier)

@@ -314,6 +314,17 @@ int gwb200_fp64_peak_tflops(gwb200_handle* h, double* tflops);
  * form's mma.sync update, -1 none (no outer trailing update, eta != 0, or no call yet). */
 int gwb200_update_kernel(gwb200_handle* h, int64_t* kernel);
 
+/* Device time of the memory-bound kernels, for their HBM rooflines (no counterpart in the
+ * reference).  While the environment sets GWB200_PROFILE=1 each launch of these kernels on the
+ * handle is bracketed by CUDA events on its stream; this call synchronises the stream and returns,
+ * summed since the previous call (then reset), per kind k: ms_out[k] the event time, bytes_out[k]
+ * the algorithmic bytes, launches_out[k] the launches.  Kinds: 0 k_gather_vph (V_ph gather, 16 n^2
+ * bytes; gwb200_load_system), 1 k_gather_panel (panel rows, 16 n m; screening calls after
+ * gwb200_load_system), 2 k_build_tall / k_build_tall32 (eps and right-hand sides of a frequency chunk:
+ * 8 (n^2 + n m) read + (n64 (n64 + 1) / 2 + m64 n64) elements of 8 or 4 bytes written per frequency),
+ * 3 k_sigma_contract (8 F m + 16 nmo F).  Launches captured into a CUDA graph are not timed. */
+int gwb200_kernel_profile(gwb200_handle* h, double* ms_out, double* bytes_out, int64_t* launches_out);
+
 #ifdef __cplusplus
 }
 #endif

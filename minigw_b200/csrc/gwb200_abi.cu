@@ -154,9 +154,56 @@ struct gwb200_handle {
     // (pq|o.) block is resident in pqo and the panel is gathered per call)
     std::vector<int64_t> bound_states;
     int persistent_ctas = 0;          // > 0: cap of the persistent kernels' grids (GPU shared by slots)
+    // GWB200_PROFILE=1: the memory-bound kernels (kKprof* kinds) timed with CUDA events on the
+    // handle's stream, resolved and summed when gwb200_kernel_profile reads them
+    struct KprofPending {
+        int kind;
+        double bytes;
+        cudaEvent_t start, stop;
+    };
+    std::vector<KprofPending> kprof_pending;
+    double kprof_ms[4] = {}, kprof_bytes[4] = {};
+    int64_t kprof_launches[4] = {};
 };
 
 void gwb200_attach_pool(gwb200_handle* h, cudaMemPool_t pool) { h->pool = pool; }
+
+namespace {
+// Kinds of gwb200_kernel_profile
+constexpr int kKprofGatherVph = 0, kKprofGatherPanel = 1, kKprofBuildTall = 2, kKprofContract = 3;
+
+bool kernel_profiling() {
+    const char* e = std::getenv("GWB200_PROFILE");
+    return e && e[0] == '1';
+}
+
+// Runs `launch` (kernels on h->stream); with GWB200_PROFILE=1 brackets it with two events whose
+// elapsed time is credited to `kind` with `bytes` of algorithmic traffic when the profile is read
+// (no synchronisation here).
+template <class F>
+int64_t kprof(gwb200_handle* h, int kind, double bytes, F&& launch) {
+    if (!kernel_profiling()) return launch();
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    GWB_CUDA(cudaStreamIsCapturing(h->stream, &cap));
+    if (cap != cudaStreamCaptureStatusNone) return launch();  // a graph being captured: not timed
+    gwb200_handle::KprofPending p{kind, bytes, nullptr, nullptr};
+    GWB_CUDA(cudaEventCreate(&p.start));
+    GWB_CUDA(cudaEventCreate(&p.stop));
+    GWB_CUDA(cudaEventRecord(p.start, h->stream));
+    const int64_t n = launch();
+    GWB_CUDA(cudaEventRecord(p.stop, h->stream));
+    h->kprof_pending.push_back(p);
+    return n;
+}
+
+void kprof_release(gwb200_handle* h) {
+    for (auto& p : h->kprof_pending) {
+        cudaEventDestroy(p.start);
+        cudaEventDestroy(p.stop);
+    }
+    h->kprof_pending.clear();
+}
+} // namespace
 void gwb200_share_sms(gwb200_handle* h, int ways) {
     int dev = 0, sms = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
@@ -324,9 +371,17 @@ void compute_forms(gwb200_handle* h, const double* omega, int64_t nfreq, const i
 
     GWB_CUDA(cudaEventRecord(h->ev[0], s));
     if (!bound)
-        launches += launch_gather_panel(h->pqo.as<double>(), h->nmo, h->nocc, h->states.as<int64_t>(), nstates,
-                                        h->xt.as<double>(), s);
+        launches += kprof(h, kKprofGatherPanel, 16.0 * (double)m * (double)h->n, [&] {
+            return (int64_t)launch_gather_panel(h->pqo.as<double>(), h->nmo, h->nocc, h->states.as<int64_t>(), nstates,
+                                                h->xt.as<double>(), s);
+        });
     GWB_CUDA(cudaEventRecord(h->ev[1], s));
+    // algorithmic bytes of one build launch: V_ph and the panel rows read once, the lower triangle of
+    // eps and the right-hand-side rows of every frequency written (el bytes per element)
+    auto build_bytes = [&](int64_t nf, double el) {
+        const double np = (double)g.n_pad, mp = (double)g.m_pad;
+        return 8.0 * ((double)g.n * (double)g.n + (double)g.n * (double)m) + el * (double)nf * (np * (np + 1.0) / 2.0 + mp * np);
+    };
     const char* prof_env = std::getenv("GWB200_PROFILE");
     UpdateProfiler prof(prof_env && prof_env[0] == '1', s);
     int64_t chunks = 0;
@@ -348,8 +403,10 @@ void compute_forms(gwb200_handle* h, const double* omega, int64_t nfreq, const i
                                          h->dvec.as<double>(), s);
         GWB_CUDA(cudaMemsetAsync(h->qacc.p, 0, sizeof(double) * (size_t)nf * g.m_pad, s));
         if (mixed) {
-            launches += launch_build_tall32(g, h->v.as<double>(), h->xt.as<double>(), h->dvec.as<double>(), nf,
-                                            h->a.as<float>(), s);
+            launches += kprof(h, kKprofBuildTall, build_bytes(nf, 4.0), [&] {
+                return (int64_t)launch_build_tall32(g, h->v.as<double>(), h->xt.as<double>(), h->dvec.as<double>(), nf,
+                                                    h->a.as<float>(), s);
+            });
             launches += launch_factor_chunk32(g, nf, h->a.as<float>(), h->linv.as<float>(), h->qacc.as<double>(),
                                               h->err.as<unsigned long long>(), s, prof.enabled ? &prof : nullptr,
                                               mixed_tc ? h->panel32.as<float>() : nullptr,
@@ -365,8 +422,10 @@ void compute_forms(gwb200_handle* h, const double* omega, int64_t nfreq, const i
                 upd_variant = tune_update_variant(g, nf, h->a.as<double>(), s, fp64_oz ? h->panel32.p : nullptr,
                                                   h->tc_sched.as<unsigned long long>(), h->err.as<unsigned long long>(),
                                                   /*timed=*/h->mem_limit <= 0);
-            launches += launch_build_tall(g, h->v.as<double>(), h->xt.as<double>(), h->dvec.as<double>(), nf,
-                                          h->a.as<double>(), s);
+            launches += kprof(h, kKprofBuildTall, build_bytes(nf, 8.0), [&] {
+                return (int64_t)launch_build_tall(g, h->v.as<double>(), h->xt.as<double>(), h->dvec.as<double>(), nf,
+                                                  h->a.as<double>(), s);
+            });
             launches += launch_factor_chunk(g, nf, h->a.as<double>(), h->linv.as<double>(), h->qacc.as<double>(),
                                             h->err.as<unsigned long long>(), s, prof.enabled ? &prof : nullptr,
                                             upd_variant, fp64_oz ? h->panel32.p : nullptr,
@@ -427,11 +486,13 @@ void contract_on_device(gwb200_handle* h, int64_t nf_int, int64_t nstates, gwb20
                                                        h->states.as<int64_t>(), h->mo.as<double>(), h->fermi,
                                                        h->omega.as<double>(), h->weight.as<double>(), omega_out_dev,
                                                        nf_out, h->sigma.as<double>(), s);
-    else
-        st->kernel_launches += launch_sigma_contract(h->qall.as<double>(), nf_int, nstates, h->nmo, ldq,
-                                                     h->states.as<int64_t>(), h->mo.as<double>(), h->fermi,
-                                                     h->omega.as<double>(), h->weight.as<double>(), omega_out_dev,
-                                                     nf_out, h->sigma.as<double>(), s);
+    else  // algorithmic bytes: the forms read once, Sigma_c written once
+        st->kernel_launches += kprof(h, kKprofContract, 8.0 * (double)nf_int * (double)m + (double)sig_bytes, [&] {
+            return (int64_t)launch_sigma_contract(h->qall.as<double>(), nf_int, nstates, h->nmo, ldq,
+                                                  h->states.as<int64_t>(), h->mo.as<double>(), h->fermi,
+                                                  h->omega.as<double>(), h->weight.as<double>(), omega_out_dev, nf_out,
+                                                  h->sigma.as<double>(), s);
+        });
     GWB_CUDA(cudaEventRecord(h->ev[3], s));
 }
 
@@ -647,6 +708,7 @@ int gwb200_destroy(gwb200_handle* h) {
         if (l.done) cudaEventDestroy(l.done);
         if (l.stream) cudaStreamDestroy(l.stream);
     }
+    kprof_release(h);
     if (h->batch_fork) cudaEventDestroy(h->batch_fork);
     if (h->batch_exec) cudaGraphExecDestroy(h->batch_exec);
     for (auto& e : h->ev)
@@ -753,7 +815,9 @@ void load_system_impl(gwb200_handle* h, int64_t nmo, int64_t nocc, const double*
     GWB_CUDA(cudaMemcpyAsync(h->vxc_diag.p, vd.data(), sizeof(double) * nmo, cudaMemcpyHostToDevice, s));
     GWB_CUDA(cudaMemsetAsync(h->flag.p, 0, sizeof(int), s));
     launch_delta(h->mo.as<double>(), nmo, nocc, h->delta.as<double>(), h->flag.as<int>(), s);
-    if (!bound) launch_gather_vph(h->pqo.as<double>(), nmo, nocc, h->v.as<double>(), s);
+    if (!bound)
+        kprof(h, kKprofGatherVph, 16.0 * (double)n * (double)n,
+              [&] { return (int64_t)launch_gather_vph(h->pqo.as<double>(), nmo, nocc, h->v.as<double>(), s); });
     launch_sigma_x_diag(h->xdiag.as<double>(), nmo, nocc, h->sigx.as<double>(), s);
     int bad = 0;
     GWB_CUDA(cudaMemcpyAsync(&bad, h->flag.p, sizeof(int), cudaMemcpyDeviceToHost, s));
@@ -1563,6 +1627,29 @@ int gwb200_run_g0w0_batch(gwb200_handle* const* systems, int64_t nsys, const int
             st->device_ms_contract = elapsed(w->ev[2], w->ev[3]);
         }
         if (nbuckets_out) *nbuckets_out = (int64_t)cands[pick].size();
+    });
+}
+
+int gwb200_kernel_profile(gwb200_handle* h, double* ms_out, double* bytes_out, int64_t* launches_out) {
+    return guarded([&] {
+        check_handle(h);
+        if (!ms_out || !bytes_out || !launches_out) fail(GWB200_BAD_ARGUMENT, "null output array");
+        GWB_CUDA(cudaStreamSynchronize(h->stream));
+        for (auto& p : h->kprof_pending) {
+            float t = 0.f;
+            GWB_CUDA(cudaEventElapsedTime(&t, p.start, p.stop));
+            h->kprof_ms[p.kind] += t;
+            h->kprof_bytes[p.kind] += p.bytes;
+            h->kprof_launches[p.kind] += 1;
+        }
+        kprof_release(h);
+        for (int k = 0; k < 4; ++k) {
+            ms_out[k] = h->kprof_ms[k];
+            bytes_out[k] = h->kprof_bytes[k];
+            launches_out[k] = h->kprof_launches[k];
+            h->kprof_ms[k] = h->kprof_bytes[k] = 0.0;
+            h->kprof_launches[k] = 0;
+        }
     });
 }
 

@@ -261,6 +261,17 @@ class B200Backend:
         check(lib.gwb200_fp64_peak_tflops(self._h, C.byref(v)))
         return v.value
 
+    KERNEL_PROFILE_KINDS = ("k_gather_vph", "k_gather_panel", "k_build_tall", "k_sigma_contract")
+
+    def kernel_profile(self) -> dict:
+        """Event time, algorithmic bytes and launches of the memory-bound kernels since the last
+        read, recorded while GWB200_PROFILE=1 (gwb200_kernel_profile)."""
+        ms, by = np.zeros(4), np.zeros(4)
+        n = np.zeros(4, dtype=np.int64)
+        check(lib.gwb200_kernel_profile(self._h, dptr(ms), dptr(by), iptr(n)))
+        return {k: {"ms": float(ms[i]), "bytes": float(by[i]), "launches": int(n[i])}
+                for i, k in enumerate(self.KERNEL_PROFILE_KINDS)}
+
     def update_kernel(self) -> int:
         """Trailing-update kernel of the last screening call (gwb200_update_kernel codes)."""
         v = C.c_int64()

@@ -51,6 +51,31 @@ def test_gathers_bit_exact_against_reference(nmo, nocc, states, oracle_lib):
         np.testing.assert_array_equal(pa, rp)
 
 
+def test_kernel_profile_of_memory_bound_kernels(monkeypatch):
+    """gwb200_kernel_profile: with GWB200_PROFILE=1 the gathers, the build and the contraction are
+    timed with events and credited with their algorithmic bytes; reading resets the sums."""
+    from minigw_b200 import B200Backend, generate_transformed_legendre_grid
+    from minigw_b200.synthetic import make_input
+
+    nmo, nocc, states = 30, 6, [5, 6]
+    inp = make_input(nmo, nocc, seed=3)
+    n, m = nocc * (nmo - nocc), len(states) * nmo
+    om, w = generate_transformed_legendre_grid(10)
+    monkeypatch.setenv("GWB200_PROFILE", "1")
+    with B200Backend(0) as be:
+        be.load_system(inp)
+        be.sigma_c(om, w, states)
+        kp = be.kernel_profile()
+        assert kp["k_gather_vph"]["launches"] == 1 and kp["k_gather_vph"]["bytes"] == 16.0 * n * n
+        assert kp["k_gather_panel"]["launches"] == 1 and kp["k_gather_panel"]["bytes"] == 16.0 * n * m
+        n64, m64 = -(-n // 64) * 64, -(-m // 64) * 64
+        assert kp["k_build_tall"]["bytes"] == 8.0 * (n * n + n * m) + 8.0 * 10 * (n64 * (n64 + 1) / 2 + m64 * n64)
+        assert kp["k_sigma_contract"]["launches"] == 1
+        assert all(v["ms"] > 0 for v in kp.values())
+        again = be.kernel_profile()
+        assert all(v["launches"] == 0 and v["ms"] == 0 for v in again.values())
+
+
 def test_state_bound_load_complex_forms_and_shards():
     from minigw_b200 import B200Backend, generate_transformed_legendre_grid
     from minigw_b200.synthetic import make_input
