@@ -58,7 +58,7 @@ void print_usage(const char* exe) {
               << "  --all-states                 Calculate all diagonal states\n"
               << "  --eta VALUE                  Infinitesimal broadening [default: 0.0; nonzero: complex symmetric path, fp64 only]\n"
               << "  --linalg-backend NAME        b200 [default: b200]\n"
-              << "  --precision MODE             fp64 or mixed [default: fp64]\n"
+              << "  --precision MODE             fp64, mixed or mixed-refined [default: fp64]\n"
               << "  --frequency-parallel MODE    auto or serial (the device batches all frequencies)\n"
               << "  --kernel-parallel MODE       auto, serial, or openmp (host loops; no effect on b200)\n"
               << "  --contraction-panel-size N   Accepted for compatibility; b200 solves all (p,k) columns at once\n"
@@ -125,8 +125,8 @@ Cli parse_cli(int argc, char** argv) {
     if (cli.frequency_parallel == "mpi")
         throw std::runtime_error("--frequency-parallel mpi requires a build configured with MPI; the b200 driver runs "
                                  "one GPU per process");
-    if (cli.precision != "fp64" && cli.precision != "mixed")
-        throw std::runtime_error("--precision must be fp64 or mixed");
+    if (cli.precision != "fp64" && cli.precision != "mixed" && cli.precision != "mixed-refined")
+        throw std::runtime_error("--precision must be fp64, mixed or mixed-refined");
     return cli;
 }
 
@@ -244,7 +244,9 @@ int main(int argc, char** argv) {
         t = std::chrono::steady_clock::now();
         check(gwb200_sigma_c(h, omega.data(), weight.data(), static_cast<int64_t>(cli.freq_points), states.data(),
                              static_cast<int64_t>(states.size()), cli.eta,
-                             cli.precision == "mixed" ? GWB200_MIXED : GWB200_FP64,
+                             cli.precision == "mixed"           ? GWB200_MIXED
+                             : cli.precision == "mixed-refined" ? GWB200_MIXED_REFINED
+                                                                : GWB200_FP64,
                              reinterpret_cast<double*>(sigma.data()), &stats),
               "gwb200_sigma_c");
         const double sigma_seconds = seconds_since(t);
