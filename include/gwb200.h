@@ -122,6 +122,19 @@ int gwb200_load_system_states(gwb200_handle* h, int64_t nmo, int64_t nocc, const
                               const double* eri, const double* vxc, double fermi_energy,
                               const int64_t* states, int64_t nstates);
 
+/* gwb200_load_system_states from inputs the caller has already sliced, for callers that never hold
+ * the nmo^4 ERI (34 GB at nmo = 256): vph (n x n) V_ph[jb, ia] = (jb|ia); panel (nstates*nmo x n),
+ * row t*nmo + k = (states[t] k|ia); xdiag (nmo x nocc) = (p i|p i); vxc_diag (nmo) the diagonal of
+ * vxc_mo; all host memory, row-major, with n = nocc * (nmo - nocc) and ia = i*nvir + (a - nocc).
+ * Contiguous copies; later calls use `states` as after gwb200_load_system_states, and the results
+ * are bit-identical to loading the full ERI these slices were cut from.  Replaces the same
+ * reference code as gwb200_load_system_states, with the hyperslab reads of the input the reference
+ * does with its HDF5 reader (src/hdf5_input.cpp:192-212) moved to the caller. */
+int gwb200_load_system_slices(gwb200_handle* h, int64_t nmo, int64_t nocc, const double* mo_energy,
+                              const double* vph, const double* panel, const double* xdiag,
+                              const double* vxc_diag, double fermi_energy, const int64_t* states,
+                              int64_t nstates);
+
 /* Correlation self-energy Sigma_c(i w_n) on the imaginary grid for the requested states.
  * sigma_out is nmo x nfreq complex, row-major (gw::MatrixComplex); rows of states not
  * requested are set to zero.  eta == 0: real SPD Cholesky of eps = I + D^1/2 V D^1/2;
@@ -266,6 +279,20 @@ int gwb200_server_create(int device, int slots, int64_t hbm_budget_bytes, gwb200
 /* Queue one request (non-blocking).  GWB200_OOM if it cannot fit one slot's budget. */
 int gwb200_server_submit(gwb200_server* s, const gwb200_request* req, int64_t* ticket);
 
+/* The system of a request as pre-cut slices (gwb200_load_system_slices' inputs, host memory owned
+ * by the caller until the request completes). */
+typedef struct gwb200_request_slices {
+    const double* vph;       /* n x n */
+    const double* panel;     /* nstates*nmo x n */
+    const double* xdiag;     /* nmo x nocc */
+    const double* vxc_diag;  /* nmo */
+} gwb200_request_slices;
+
+/* gwb200_server_submit for a request whose system comes as slices: req->eri and req->vxc are not
+ * read (may be NULL), the worker loads with gwb200_load_system_slices. */
+int gwb200_server_submit_slices(gwb200_server* s, const gwb200_request* req, const gwb200_request_slices* slices,
+                                int64_t* ticket);
+
 /* Block until the request completes; its status is returned (and in *status), with the time it
  * waited for a slot, its service time (host, from admission to results) and its device time. */
 int gwb200_server_wait(gwb200_server* s, int64_t ticket, int* status, double* queue_ms, double* service_ms,
@@ -273,6 +300,17 @@ int gwb200_server_wait(gwb200_server* s, int64_t ticket, int* status, double* qu
 
 /* Finish every queued request, stop the workers, release their handles. */
 int gwb200_server_destroy(gwb200_server* s);
+
+/* Continuous batching across requests: a worker that frees up takes, besides the oldest request,
+ * up to max_requests - 1 further waiting requests that can share launches with it (eta == 0 and the
+ * same precision, GWB200_FP64 or GWB200_MIXED; their resident data plus one frequency of the largest
+ * tall matrix within 80% of the slot's budget) and solves them together with
+ * gwb200_run_g0w0_batch, each on a handle of its own.  Results are bit-identical to the requests'
+ * own solves.  1 turns merging off; the default is 8. */
+int gwb200_server_set_merge(gwb200_server* s, int max_requests);
+
+/* Batches of two or more requests solved so far, and the requests in them. */
+int gwb200_server_counters(gwb200_server* s, int64_t* merged_batches, int64_t* merged_requests);
 
 /* ---- Batched solves: many molecules of uneven size in shared launches (no reference counterpart;
  * the reference runs one molecule per process, src/main.cpp:68-103) ----

@@ -40,7 +40,8 @@ EXPORTS = (
     "gwb200_sigma_c", "gwb200_screened_forms", "gwb200_screened_forms_complex", "gwb200_sigma_x_diag", "gwb200_qp", "gwb200_pade_sweep",
     "gwb200_grid", "gwb200_read_input_h5", "gwb200_screened_forms_noalloc", "gwb200_fp64_peak_tflops",
     "gwb200_update_kernel", "gwb200_run_g0w0_batch", "gwb200_plan_buckets", "gwb200_read_resident",
-    "gwb200_kernel_profile",
+    "gwb200_kernel_profile", "gwb200_load_system_slices", "gwb200_server_submit_slices", "gwb200_server_set_merge",
+    "gwb200_server_counters",
 )
 
 
@@ -90,6 +91,11 @@ class Request(C.Structure):
     ]
 
 
+class RequestSlices(C.Structure):
+    """gwb200_request_slices (include/gwb200.h)."""
+    _fields_ = [("vph", _dp), ("panel", _dp), ("xdiag", _dp), ("vxc_diag", _dp)]
+
+
 def _load() -> C.CDLL:
     if not LIB_PATH.exists():
         raise ImportError(
@@ -129,6 +135,12 @@ def _load() -> C.CDLL:
     lib.gwb200_update_kernel.argtypes = [_vp, _ip]
     lib.gwb200_read_resident.argtypes = [_vp, _ip, C.c_int64, _dp, _dp]
     lib.gwb200_kernel_profile.argtypes = [_vp, _dp, _dp, _ip]
+    lib.gwb200_load_system_slices.argtypes = [_vp, C.c_int64, C.c_int64, _dp, _dp, _dp, _dp, _dp, C.c_double, _ip,
+                                              C.c_int64]
+    lib.gwb200_server_submit_slices.argtypes = [_vp, C.POINTER(Request), C.POINTER(RequestSlices),
+                                                C.POINTER(C.c_int64)]
+    lib.gwb200_server_set_merge.argtypes = [_vp, C.c_int]
+    lib.gwb200_server_counters.argtypes = [_vp, _ip, _ip]
     lib.gwb200_run_g0w0_batch.argtypes = [C.POINTER(_vp), C.c_int64, _ip, _ip, C.POINTER(_ip), _ip,
                                           C.c_int, C.POINTER(_dp), C.POINTER(_dp), _ip, C.POINTER(Stats)]
     lib.gwb200_plan_buckets.argtypes = [C.c_int64, _ip, _ip, C.c_int64, C.c_int, C.c_int64, C.c_double, C.c_double,

@@ -738,10 +738,25 @@ namespace {
 // Shared body of gwb200_load_system (states == NULL: the (pq|o.) block stays resident and panels
 // are gathered per call) and gwb200_load_system_states (V_ph and the panel rows of `states` copied
 // from the host straight into their device layouts; nothing else of the ERI is uploaded).
+// Caller-sliced inputs of gwb200_load_system_slices (host memory, contiguous, row-major).
+struct HostSlices {
+    const double* vph;       // n x n
+    const double* panel;     // nstates*nmo x n
+    const double* xdiag;     // nmo x nocc: (p i|p i)
+    const double* vxc_diag;  // nmo
+};
+
 void load_system_impl(gwb200_handle* h, int64_t nmo, int64_t nocc, const double* mo_energy, const double* eri,
-                      const double* vxc, double fermi_energy, const int64_t* states, int64_t nstates) {
+                      const double* vxc, double fermi_energy, const int64_t* states, int64_t nstates,
+                      const HostSlices* sl = nullptr) {
     check_handle(h);
-    if (!mo_energy || !eri || !vxc) fail(GWB200_BAD_ARGUMENT, "null input array");
+    if (sl) {
+        if (!mo_energy || !sl->vph || !sl->panel || !sl->xdiag || !sl->vxc_diag)
+            fail(GWB200_BAD_ARGUMENT, "null input array");
+        if (!states) fail(GWB200_BAD_ARGUMENT, "null state list");
+    } else if (!mo_energy || !eri || !vxc) {
+        fail(GWB200_BAD_ARGUMENT, "null input array");
+    }
     if (nmo <= 0) fail(GWB200_BAD_SHAPE, "OrbitalSpace: empty MO energy vector");
     if (nocc <= 0 || nocc >= nmo) fail(GWB200_BAD_SHAPE, "OrbitalSpace: invalid number of occupied orbitals");
     if (nmo > 1024) fail(GWB200_BAD_SHAPE, "nmo > 1024 is not supported");
@@ -779,8 +794,12 @@ void load_system_impl(gwb200_handle* h, int64_t nmo, int64_t nocc, const double*
     size_buffer(h, h->v, sizeof(double) * (size_t)n * n);
     h->flag.ensure(sizeof(int));
     std::vector<double> vd((size_t)nmo);
-    for (int64_t p = 0; p < nmo; ++p) vd[(size_t)p] = vxc[p * nmo + p];
-    if (bound) {
+    for (int64_t p = 0; p < nmo; ++p) vd[(size_t)p] = sl ? sl->vxc_diag[p] : vxc[p * nmo + p];
+    if (sl) {  // already in the device layouts: contiguous copies
+        GWB_CUDA(cudaMemcpyAsync(h->v.p, sl->vph, sizeof(double) * (size_t)n * n, cudaMemcpyHostToDevice, s));
+        GWB_CUDA(cudaMemcpyAsync(h->xt.p, sl->panel, sizeof(double) * (size_t)nstates * nmo * n, cudaMemcpyHostToDevice,
+                                 s));
+    } else if (bound) {
         // One 3D copy per source block eri[p, ., ., .] (an nmo x nmo x nmo array of rows of nmo
         // doubles): x = the virtual index s (nvir doubles from nocc), y = the occupied index
         // r < nocc, z = q.  The destination rows are the n = nocc * nvir columns (i, a) of
@@ -807,7 +826,8 @@ void load_system_impl(gwb200_handle* h, int64_t nmo, int64_t nocc, const double*
                                    sizeof(double) * nocc * nmo, nmo2, cudaMemcpyHostToDevice, s));
     }
     // exchange diagonal eri[p,i,p,i]: for each p, nocc elements with stride nmo^2 + 1
-    for (int64_t p = 0; p < nmo; ++p)
+    if (sl) GWB_CUDA(cudaMemcpyAsync(h->xdiag.p, sl->xdiag, sizeof(double) * nmo * nocc, cudaMemcpyHostToDevice, s));
+    for (int64_t p = 0; p < nmo && !sl; ++p)
         GWB_CUDA(cudaMemcpy2DAsync(h->xdiag.as<double>() + p * nocc, sizeof(double),
                                    eri + ((size_t)p * nmo * nmo + p) * nmo, sizeof(double) * (nmo2 + 1),
                                    sizeof(double), nocc, cudaMemcpyHostToDevice, s));
@@ -868,6 +888,15 @@ int gwb200_read_resident(gwb200_handle* h, const int64_t* states, int64_t nstate
             GWB_CUDA(cudaMemcpyAsync(panel_out, h->xt.p, nb, cudaMemcpyDeviceToHost, s));
         }
         GWB_CUDA(cudaStreamSynchronize(s));
+    });
+}
+
+int gwb200_load_system_slices(gwb200_handle* h, int64_t nmo, int64_t nocc, const double* mo_energy,
+                              const double* vph, const double* panel, const double* xdiag, const double* vxc_diag,
+                              double fermi_energy, const int64_t* states, int64_t nstates) {
+    return guarded([&] {
+        const HostSlices sl{vph, panel, xdiag, vxc_diag};
+        load_system_impl(h, nmo, nocc, mo_energy, nullptr, nullptr, fermi_energy, states, nstates, &sl);
     });
 }
 

@@ -23,8 +23,9 @@ from typing import Optional, Sequence
 import ctypes as C
 import numpy as np
 
-from ._lib import FP64, MIXED, MIXED_REFINED, GwB200Error, Request, Stats, _dp, _ip, check, dptr, iptr, lib
-from .gw_input import GwInput
+from ._lib import (FP64, MIXED, MIXED_REFINED, GwB200Error, Request, RequestSlices, Stats, _dp, _ip, check, dptr,
+                   iptr, lib)
+from .gw_input import GwInput, GwSlices
 
 HARTREE_TO_EV = 27.211386245988  # include/types.hpp:12
 
@@ -168,6 +169,16 @@ class B200Backend:
             check(lib.gwb200_load_system_states(self._h, nmo, int(inp.nocc), dptr(mo), dptr(eri), dptr(vxc),
                                                 float(inp.fermi_energy), iptr(st), st.shape[0]))
         self.nmo, self.nocc, self.fermi = nmo, int(inp.nocc), float(inp.fermi_energy)
+
+    def load_slices(self, sl: GwSlices) -> None:
+        """Upload a system from pre-cut slices (gwb200_load_system_slices); later calls must use
+        sl.states."""
+        st = np.ascontiguousarray(sl.states, dtype=np.int64)
+        arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in (sl.mo_energy, sl.vph, sl.panel, sl.xdiag,
+                                                                    sl.vxc_diag)]
+        check(lib.gwb200_load_system_slices(self._h, sl.nmo, int(sl.nocc), *[dptr(a) for a in arrs],
+                                            float(sl.fermi_energy), iptr(st), st.shape[0]))
+        self.nmo, self.nocc, self.fermi = sl.nmo, int(sl.nocc), float(sl.fermi_energy)
 
     def sigma_c(self, omegas, weights, states, eta: float = 0.0, precision="fp64"):
         om = np.ascontiguousarray(omegas, dtype=np.float64)
@@ -392,31 +403,54 @@ class B200Server:
     handle and stream and a device-memory cap of hbm_budget/slots; requests are admitted FIFO as
     workers free up and run concurrently on the GPU."""
 
-    def __init__(self, device: int = 0, slots: int = 4, hbm_budget_bytes: int = 64 << 30):
+    def __init__(self, device: int = 0, slots: int = 4, hbm_budget_bytes: int = 64 << 30, merge: int | None = None):
         srv = C.c_void_p()
         check(lib.gwb200_server_create(device, slots, int(hbm_budget_bytes), C.byref(srv)))
         self._s = srv
         self._live = {}
+        if merge is not None:
+            check(lib.gwb200_server_set_merge(self._s, int(merge)))
 
-    def submit(self, inp: GwInput, nfreq: int, npade: int, states, eta: float = 0.0, precision="fp64") -> int:
+    def submit(self, inp: GwInput | GwSlices, nfreq: int, npade: int, states, eta: float = 0.0,
+               precision="fp64") -> int:
+        """Queue one solve; `inp` is a full system (its ERI is read at load) or GwSlices (whose state
+        list must be `states`)."""
         nmo = inp.nmo
+        sliced = isinstance(inp, GwSlices)
         keep = {
             "mo": np.ascontiguousarray(inp.mo_energy, dtype=np.float64),
-            "eri": np.ascontiguousarray(inp.eri_mo, dtype=np.float64),
-            "vxc": np.ascontiguousarray(inp.vxc_mo, dtype=np.float64),
             "states": np.ascontiguousarray(states, dtype=np.int64),
             "omegas": np.zeros(nfreq), "weights": np.zeros(nfreq),
             "sigma": np.zeros((nmo, nfreq), dtype=np.complex128), "sigma_x_diag": np.zeros(nmo), "qp": np.zeros(nmo),
         }
-        req = Request(nmo, int(inp.nocc), dptr(keep["mo"]), dptr(keep["eri"]), dptr(keep["vxc"]),
+        if sliced:
+            if not np.array_equal(np.asarray(inp.states), keep["states"]):
+                raise GwB200Error(7, "the state list must be the one the slices were cut for")
+            for k in ("vph", "panel", "xdiag", "vxc_diag"):
+                keep[k] = np.ascontiguousarray(getattr(inp, k), dtype=np.float64)
+        else:
+            keep["eri"] = np.ascontiguousarray(inp.eri_mo, dtype=np.float64)
+            keep["vxc"] = np.ascontiguousarray(inp.vxc_mo, dtype=np.float64)
+        req = Request(nmo, int(inp.nocc), dptr(keep["mo"]), dptr(keep.get("eri")), dptr(keep.get("vxc")),
                       float(inp.fermi_energy), int(nfreq), int(npade), iptr(keep["states"]), len(keep["states"]),
                       float(eta), _precision_code(precision), dptr(keep["omegas"]), dptr(keep["weights"]),
                       dptr(keep["sigma"]), dptr(keep["sigma_x_diag"]), dptr(keep["qp"]))
         keep["req"] = req
         ticket = C.c_int64()
-        check(lib.gwb200_server_submit(self._s, C.byref(req), C.byref(ticket)))
+        if sliced:
+            sl = RequestSlices(dptr(keep["vph"]), dptr(keep["panel"]), dptr(keep["xdiag"]), dptr(keep["vxc_diag"]))
+            keep["slices"] = sl
+            check(lib.gwb200_server_submit_slices(self._s, C.byref(req), C.byref(sl), C.byref(ticket)))
+        else:
+            check(lib.gwb200_server_submit(self._s, C.byref(req), C.byref(ticket)))
         self._live[ticket.value] = keep
         return ticket.value
+
+    def counters(self) -> dict:
+        """Batches of two or more requests merged so far, and the requests in them."""
+        b, r = C.c_int64(), C.c_int64()
+        check(lib.gwb200_server_counters(self._s, C.byref(b), C.byref(r)))
+        return {"merged_batches": b.value, "merged_requests": r.value}
 
     def wait(self, ticket: int) -> dict:
         st = C.c_int()

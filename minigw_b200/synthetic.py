@@ -147,3 +147,45 @@ def make_input_on_device(nmo: int, nocc: int, seed: int = 0, device: int = 0, pi
     inp = GwInput(eri_mo=eri, mo_energy=mo, vxc_mo=vxc, nocc=nocc, fermi_energy=float(fermi))
     inp._pinned_owner = host  # keep the pinned tensor alive with the array view
     return inp
+
+
+def make_slices_on_device(nmo: int, nocc: int, states, seed: int = 0, device: int = 0):
+    """The slices of the system make_input(nmo, nocc, seed) describes (GwSlices: V_ph, the states'
+    panel rows, the exchange diagonal, the vxc diagonal), computed from the Cholesky-like factors L
+    with torch on the GPU, without ever forming the nmo^4 ERI (34 GB at nmo = 256).  Same random
+    draws and recipe as make_input; the values differ from slices of make_input's ERI only by the
+    rounding of the sums over K (V_ph is symmetrised the same way, 0.5 (A + A^T))."""
+    import torch
+
+    from .gw_input import GwSlices
+
+    rng = np.random.default_rng(seed)
+    nvir = nmo - nocc
+    occ = np.sort(rng.uniform(-1.2, -0.3, nocc))
+    vir = np.sort(rng.uniform(0.05, 3.0, nvir))
+    mo = np.concatenate([occ, vir])
+    fermi = 0.5 * (occ[-1] + vir[0])
+    nk = 2 * nmo
+    idx = np.arange(nmo)
+    decay = 0.3 * np.exp(-np.abs(idx[:, None] - idx[None, :]) / 8.0)
+    g = rng.standard_normal((nk, nmo, nmo))
+    lfac = (np.triu(g) + np.transpose(np.triu(g, 1), (0, 2, 1))) * decay
+    vxc = rng.normal(0.0, 0.01, (nmo, nmo))
+    vxc = np.triu(vxc, 1)
+    vxc = vxc + vxc.T
+    vxc[idx, idx] = rng.uniform(-0.6, -0.2, nmo)
+    st = np.ascontiguousarray(states, dtype=np.int64)
+    n = nocc * nvir
+    dev = torch.device("cuda", device)
+    lt = torch.from_numpy(np.ascontiguousarray(lfac)).to(dev)          # [K, p, q]
+    lov = lt[:, :nocc, nocc:].reshape(nk, n)                           # [K, ia]
+    v = lov.t() @ lov
+    v = 0.5 * (v + v.t())
+    panel = torch.cat([lt[:, int(p), :].t() @ lov for p in st], dim=0)  # [(t, k), ia]
+    xdiag = (lt[:, :, :nocc] ** 2).sum(dim=0)                          # [p, i]
+    out = GwSlices(mo_energy=mo, nocc=nocc, fermi_energy=float(fermi), states=st,
+                   vph=v.cpu().numpy(), panel=panel.cpu().numpy(), xdiag=xdiag.cpu().numpy(),
+                   vxc_diag=np.ascontiguousarray(np.diag(vxc)))
+    del lt, lov, v, panel, xdiag
+    torch.cuda.empty_cache()
+    return out

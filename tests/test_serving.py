@@ -48,3 +48,54 @@ def test_server_matches_backend_and_rejects_oversize():
             with pytest.raises(GwB200Error) as e:
                 tiny.submit(big, 16, 8, [9])
             assert e.value.status == "GWB200_OOM"
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_merged_requests_identical_to_alone(precision):
+    """Requests that wait while the worker is busy are merged into one gwb200_run_g0w0_batch; each
+    result is bit-identical to the same request solved alone (merging off), and a request that
+    cannot share launches (refined mixed form) runs alone in between."""
+    from minigw_b200 import B200Server
+
+    reqs = _requests()
+    with B200Server(0, slots=1, hbm_budget_bytes=8 << 30, merge=1) as alone:
+        ref = [alone.wait(alone.submit(inp, nf, 12, st, precision=precision)) for inp, nf, st in reqs]
+        odd = reqs[2]
+        ref_odd = alone.wait(alone.submit(odd[0], odd[1], 12, odd[2], precision="mixed-refined"))
+        assert alone.counters()["merged_requests"] == 0
+    with B200Server(0, slots=1, hbm_budget_bytes=8 << 30, merge=8) as srv:
+        tickets = [srv.submit(inp, nf, 12, st, precision=precision) for inp, nf, st in reqs[:3]]
+        t_odd = srv.submit(odd[0], odd[1], 12, odd[2], precision="mixed-refined")
+        tickets += [srv.submit(inp, nf, 12, st, precision=precision) for inp, nf, st in reqs[3:]]
+        got = [srv.wait(t) for t in tickets]
+        got_odd = srv.wait(t_odd)
+        counters = srv.counters()
+    assert counters["merged_batches"] >= 1 and counters["merged_requests"] >= 2, counters
+    for a, b, (inp, nf, st) in zip(ref, got, reqs):
+        np.testing.assert_array_equal(a["sigma"], b["sigma"])
+        np.testing.assert_array_equal(a["qp"][st], b["qp"][st])
+        np.testing.assert_array_equal(a["sigma_x_diag"], b["sigma_x_diag"])
+        np.testing.assert_array_equal(a["omegas"], b["omegas"])
+        np.testing.assert_array_equal(a["weights"], b["weights"])
+    np.testing.assert_array_equal(ref_odd["sigma"], got_odd["sigma"])
+
+
+def test_sliced_requests():
+    """A request whose system arrives as slices (no ERI) gives the backend's own result."""
+    from minigw_b200 import B200Backend, B200Server
+    from minigw_b200.gw_input import slices_from_input
+    from minigw_b200.synthetic import make_input
+
+    inp = make_input(26, 4, seed=12)
+    states = [3, 4, 5]
+    sl = slices_from_input(inp, states)
+    with B200Backend(0) as be:
+        be.load_system(inp, states)
+        ref = be.run_g0w0(30, 12, states)
+    with B200Server(0, slots=2, hbm_budget_bytes=4 << 30) as srv:
+        ts = [srv.submit(sl, 30, 12, states), srv.submit(inp, 30, 12, states), srv.submit(sl, 30, 12, states)]
+        out = [srv.wait(t) for t in ts]
+    for r in out:
+        np.testing.assert_array_equal(r["sigma"], ref["sigma"])
+        np.testing.assert_array_equal(r["qp"][states], ref["qp"][states])
+        np.testing.assert_array_equal(r["sigma_x_diag"], ref["sigma_x_diag"])
