@@ -302,11 +302,12 @@ int gwb200_server_wait(gwb200_server* s, int64_t ticket, int* status, double* qu
 int gwb200_server_destroy(gwb200_server* s);
 
 /* Continuous batching across requests: a worker that frees up takes, besides the oldest request,
- * up to max_requests - 1 further waiting requests that can share launches with it (eta == 0 and the
- * same precision, GWB200_FP64 or GWB200_MIXED; their resident data plus one frequency of the largest
- * tall matrix within 80% of the slot's budget) and solves them together with
- * gwb200_run_g0w0_batch, each on a handle of its own.  Results are bit-identical to the requests'
- * own solves.  1 turns merging off; the default is 8. */
+ * further waiting requests that can share launches with it (eta == 0, the same precision, GWB200_FP64
+ * or GWB200_MIXED, at most 1536 particle-hole pairs: larger requests fill the GPU alone; their
+ * resident data plus one frequency of the largest tall matrix within 80% of the slot's budget), up
+ * to max_requests in all and to a fair share of the waiting requests per worker, and solves them
+ * together with gwb200_run_g0w0_batch, each on a handle of its own.  Results are bit-identical to
+ * the requests' own solves.  1 turns merging off; the default is 8. */
 int gwb200_server_set_merge(gwb200_server* s, int max_requests);
 
 /* Batches of two or more requests solved so far, and the requests in them. */

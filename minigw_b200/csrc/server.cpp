@@ -10,7 +10,8 @@
 // a result is bit-identical whether the request ran alone or in a mix.
 //
 // Merging: when a worker frees up and several compatible requests wait (eta = 0, the same
-// precision, FP64 or the unrefined mixed form), it takes up to `max_merge` of them at once, loads
+// precision, FP64 or the unrefined mixed form, small enough not to fill the GPU alone), it takes up
+// to `max_merge` of them at once (and no more than a fair share of the queue per worker), loads
 // each into a handle of its own (the worker's handle leads, the others come from the worker's
 // member handles), and solves them with one gwb200_run_g0w0_batch: their frequency work is
 // bucketed by size and factored in shared launches.  The batch is bit-identical to each request's
@@ -108,8 +109,14 @@ size_t matrix_bytes(const gwb200_request& r) {
     return (n64 + m64) * n64 * (r.precision == GWB200_MIXED ? sizeof(float) : sizeof(double));
 }
 
+// Above this many particle-hole pairs one request's launches already fill the GPU (a 64-wide block
+// step of n = 1536 has 24 x 24 tiles per frequency), so merging it only makes the small requests
+// of its batch wait for it.
+constexpr int64_t kMergeMaxNph = 1536;
+
 bool mergeable(const gwb200_request& r) {
-    return r.eta == 0.0 && (r.precision == GWB200_FP64 || r.precision == GWB200_MIXED);
+    const int64_t n = r.nocc * (r.nmo - r.nocc);
+    return r.eta == 0.0 && (r.precision == GWB200_FP64 || r.precision == GWB200_MIXED) && n <= kMergeMaxNph;
 }
 
 int make_slot_handle(gwb200_server* s, gwb200_handle** out) {
@@ -277,8 +284,11 @@ void worker_main(gwb200_server* s) {
             s->queue.pop_front();
             // continuous batching: compatible requests already waiting join this one
             if (s->max_merge > 1 && mergeable(jobs[0].req)) {
+                // a fair share of what waits, so that the other workers get requests too
+                const int share = (int)((s->queue.size() + 1 + (size_t)s->slots - 1) / (size_t)s->slots);
+                const int take = std::min(s->max_merge, std::max(2, share));
                 size_t need = resident_bytes(jobs[0].req), big = matrix_bytes(jobs[0].req);
-                for (auto it = s->queue.begin(); it != s->queue.end() && (int)jobs.size() < s->max_merge;) {
+                for (auto it = s->queue.begin(); it != s->queue.end() && (int)jobs.size() < take;) {
                     const gwb200_request& r = it->req;
                     const size_t need2 = need + resident_bytes(r), big2 = std::max(big, matrix_bytes(r));
                     if (mergeable(r) && r.precision == jobs[0].req.precision &&
