@@ -50,7 +50,8 @@ typedef enum gwb200_precision {
                                   * are the energy functional -(2 x^T D^1/2 z - z^T eps z) evaluated in FP64
                                   * (error quadratic in the FP32 solve error, ~1e-14 relative); y^T V y
                                   * through a pivoted Cholesky factor of V computed once per loaded system.
-                                  * gwb200_screened_forms / sigma_c / sigma_c_shard / run_g0w0 only */
+                                  * Every screening entry point and gwb200_run_g0w0_batch; not the
+                                  * no-allocation entry */
 } gwb200_precision;
 
 typedef struct gwb200_stats {
@@ -302,8 +303,8 @@ int gwb200_server_wait(gwb200_server* s, int64_t ticket, int* status, double* qu
 int gwb200_server_destroy(gwb200_server* s);
 
 /* Continuous batching across requests: a worker that frees up takes, besides the oldest request,
- * further waiting requests that can share launches with it (eta == 0, the same precision, GWB200_FP64
- * or GWB200_MIXED, at most 1536 particle-hole pairs: larger requests fill the GPU alone; their
+ * further waiting requests that can share launches with it (eta == 0, the same precision, at most
+ * 1536 particle-hole pairs: larger requests fill the GPU alone; their
  * resident data plus one frequency of the largest tall matrix within 80% of the slot's budget), up
  * to max_requests in all and to a fair share of the waiting requests per worker, and solves them
  * together with gwb200_run_g0w0_batch, each on a handle of its own.  Results are bit-identical to
@@ -317,7 +318,7 @@ int gwb200_server_counters(gwb200_server* s, int64_t* merged_batches, int64_t* m
  * the reference runs one molecule per process, src/main.cpp:68-103) ----
  * systems[i] holds molecule i (gwb200_load_system or gwb200_load_system_states), all on one device,
  * no handle twice, at most 65535.  Molecule i is solved as gwb200_run_g0w0(systems[i], nfreq[i],
- * npade[i], states[i], nstates[i], 0, precision, ...) would solve it (eta = 0; frequency and Pade
+ * npade[i], states[i], nstates[i], 0, precision, ...) would solve it (eta = 0, any precision; frequency and Pade
  * counts may differ between molecules).  The molecules are sorted by size and grouped into
  * buckets; a bucket's matrices (every member x every one of its frequencies) take the bucket's
  * largest geometry (identity / zero padding, exact) and are factored by shared launches on up to 4

@@ -84,8 +84,8 @@ struct PinnedBuf {
 struct BatchLane {
     cudaStream_t stream = nullptr;  // lanes >= 1 (created on first use)
     cudaEvent_t done = nullptr;
-    DevBuf a, linv, qacc, panel, sched;
-    size_t bytes() const { return a.bytes + linv.bytes + qacc.bytes + panel.bytes; }
+    DevBuf a, linv, qacc, panel, sched, refine;  // refine: the refined mixed form's correction terms
+    size_t bytes() const { return a.bytes + linv.bytes + qacc.bytes + panel.bytes + refine.bytes; }
 };
 constexpr int kMaxBatchLanes = 4;
 
@@ -530,8 +530,8 @@ struct BatchChunk {
 // each member).
 std::vector<BatchChunk> batch_chunks(const std::vector<gwb200_handle*>& hs, const std::vector<int64_t>& ms,
                                      const std::vector<int64_t>& fs, const std::vector<int>& order,
-                                     const std::vector<int64_t>& sizes, bool mixed, bool oz, size_t budget, int64_t cap,
-                                     std::vector<BatchGroup>& groups) {
+                                     const std::vector<int64_t>& sizes, bool mixed, bool oz, bool refine, size_t budget,
+                                     int64_t cap, std::vector<BatchGroup>& groups) {
     std::vector<BatchChunk> chunks;
     size_t pos = 0;
     for (int64_t bsz : sizes) {
@@ -542,7 +542,7 @@ std::vector<BatchChunk> batch_chunks(const std::vector<gwb200_handle*>& hs, cons
             mmax = std::max(mmax, ms[(size_t)i]);
         }
         const TallGeometry g = make_geometry(nmax, mmax);
-        int64_t fit = std::max<int64_t>(1, (int64_t)(budget / batch_bytes_per_matrix(g, mixed, oz)));
+        int64_t fit = std::max<int64_t>(1, (int64_t)(budget / batch_bytes_per_matrix(g, mixed, oz, refine)));
         if (cap > 0) fit = std::min(fit, cap);
         BatchChunk cur{g, 0, (int64_t)groups.size(), 0};
         for (int64_t t = 0; t < bsz; ++t) {
@@ -567,6 +567,8 @@ std::vector<BatchChunk> batch_chunks(const std::vector<gwb200_handle*>& hs, cons
                 gr.ldq_out = gi.m_pad;
                 gr.mat0 = cur.nmat;
                 gr.nf = nf;
+                gr.ct = refine ? h->pchol_ct : nullptr;
+                gr.r_pad = refine ? std::max<int64_t>(kNb, round_up(h->pchol_rank, kNb)) : 0;
                 groups.push_back(gr);
                 ++cur.ngroups;
                 cur.nmat += nf;
@@ -581,10 +583,10 @@ std::vector<BatchChunk> batch_chunks(const std::vector<gwb200_handle*>& hs, cons
 
 // Workspace bytes of a set of chunks: the largest tall matrices, inverses, accumulators, operands.
 struct BatchNeed {
-    size_t a = 0, linv = 0, qacc = 0, panel = 0;
-    size_t total() const { return a + linv + qacc + panel; }
+    size_t a = 0, linv = 0, qacc = 0, panel = 0, refine = 0;
+    size_t total() const { return a + linv + qacc + panel + refine; }
 };
-void batch_need(const std::vector<BatchChunk>& chunks, bool mixed, bool oz, BatchNeed& need) {
+void batch_need(const std::vector<BatchChunk>& chunks, bool mixed, bool oz, bool refine, BatchNeed& need) {
     const size_t el = mixed ? sizeof(float) : sizeof(double);
     for (const BatchChunk& c : chunks) {
         const size_t nm = (size_t)c.nmat;
@@ -593,13 +595,16 @@ void batch_need(const std::vector<BatchChunk>& chunks, bool mixed, bool oz, Batc
         need.qacc = std::max(need.qacc, sizeof(double) * nm * (size_t)c.g.m_pad);
         const size_t op = mixed ? tc_panel_bytes_per_freq(c.g) : (oz ? oz_slice_bytes_per_freq(c.g) : 0);
         need.panel = std::max(need.panel, op * nm);
+        // the correction terms of one molecule at a time, bounded by the chunk's geometry
+        if (refine) need.refine = std::max(need.refine, refine_bytes_per_freq(c.g, c.g.n_pad) * nm);
     }
 }
 
 // The chunks `idx` of a plan on one lane (build, factor, forms per chunk), on stream `s`.
 int64_t batch_screen(gwb200_handle* w, BatchLane& lane, cudaStream_t s, int max_ctas,
                      const std::vector<BatchChunk>& chunks, const std::vector<size_t>& idx, const BatchGroup* dgroups,
-                     const std::vector<int>& variants, bool mixed, bool mixed_tc, bool oz) {
+                     const std::vector<BatchGroup>& hgroups, const std::vector<int>& variants, bool mixed,
+                     bool mixed_tc, bool oz, bool refine) {
     int64_t launches = 0;
     unsigned long long* err = w->err.as<unsigned long long>();
     unsigned long long* sched = lane.sched.as<unsigned long long>();
@@ -608,11 +613,29 @@ int64_t batch_screen(gwb200_handle* w, BatchLane& lane, cudaStream_t s, int max_
         const BatchGroup* gp = dgroups + c.group0;
         GWB_CUDA(cudaMemsetAsync(lane.qacc.p, 0, sizeof(double) * (size_t)c.nmat * c.g.m_pad, s));
         launches += launch_build_tall_batch(c.g, gp, c.ngroups, mixed, lane.a.p, s);
-        if (mixed)
+        if (mixed) {
             launches += launch_factor_chunk32(c.g, c.nmat, lane.a.as<float>(), lane.linv.as<float>(),
                                               lane.qacc.as<double>(), err, s, nullptr,
                                               mixed_tc ? lane.panel.as<float>() : nullptr, sched, max_ctas);
-        else
+            if (refine) {  // each molecule's factor reversed in its own n_pad, one backward solve of the
+                           // chunk, then each molecule's correction in its own geometry
+                for (int64_t q = 0; q < c.ngroups; ++q) {
+                    const BatchGroup& gr = hgroups[(size_t)(c.group0 + q)];
+                    launches += launch_refine_flip(c.g, gr.nf, lane.a.as<float>() + (size_t)gr.mat0 * c.g.stride,
+                                                   gr.n_pad, s);
+                }
+                launches += launch_refine_solve(c.g, c.nmat, lane.a.as<float>(), lane.linv.as<float>(), err, s,
+                                                mixed_tc ? lane.panel.as<float>() : nullptr, sched, max_ctas,
+                                                /*flip=*/false);
+                for (int64_t q = 0; q < c.ngroups; ++q) {
+                    const BatchGroup& gr = hgroups[(size_t)(c.group0 + q)];
+                    launches += launch_refine_terms(c.g, gr.nf, lane.a.as<float>() + (size_t)gr.mat0 * c.g.stride,
+                                                    make_geometry(gr.n, gr.m), gr.xt, gr.dvec, gr.ct, gr.r_pad,
+                                                    lane.refine.p, lane.qacc.as<double>() + (size_t)gr.mat0 * c.g.m_pad,
+                                                    c.g.m_pad, s);
+                }
+            }
+        } else
             launches += launch_factor_chunk(c.g, c.nmat, lane.a.as<double>(), lane.linv.as<double>(),
                                             lane.qacc.as<double>(), err, s, nullptr, variants[k],
                                             oz ? lane.panel.p : nullptr, sched, max_ctas);
@@ -704,7 +727,7 @@ int gwb200_destroy(gwb200_handle* h) {
         b->release();
     for (BatchLane& l : h->lanes) {
         if (l.stream) cudaStreamSynchronize(l.stream);
-        for (DevBuf* b : {&l.a, &l.linv, &l.qacc, &l.panel, &l.sched}) b->release();
+        for (DevBuf* b : {&l.a, &l.linv, &l.qacc, &l.panel, &l.sched, &l.refine}) b->release();
         if (l.done) cudaEventDestroy(l.done);
         if (l.stream) cudaStreamDestroy(l.stream);
     }
@@ -1253,6 +1276,8 @@ std::vector<int64_t> batch_graph_key(const gwb200_handle* w, const std::vector<g
         for (const DevBuf* b : {&h->pqo, &h->v, &h->xt, &h->dvec, &h->qall, &h->sigma, &h->qp, &h->qp_scratch, &h->omega,
                                 &h->weight, &h->states, &h->delta, &h->mo, &h->sigx, &h->vxc_diag})
             put(b->p);
+        put(h->pchol_ct);
+        gkey.push_back(h->pchol_rank);
     }
     put(w->batch_desc.p);
     put(w->err.p);
@@ -1260,7 +1285,7 @@ std::vector<int64_t> batch_graph_key(const gwb200_handle* w, const std::vector<g
     put(w->batch_fork);
     for (int l = 0; l < lanes; ++l) {
         const BatchLane& ln = w->lanes[l];
-        for (const DevBuf* b : {&ln.a, &ln.linv, &ln.qacc, &ln.panel, &ln.sched}) put(b->p);
+        for (const DevBuf* b : {&ln.a, &ln.linv, &ln.qacc, &ln.panel, &ln.sched, &ln.refine}) put(b->p);
         put(ln.stream);
         put(ln.done);
     }
@@ -1273,8 +1298,9 @@ int gwb200_plan_buckets(int64_t nsys, const int64_t* nph, const int64_t* ncols, 
     return guarded([&] {
         if (nsys <= 0 || !nph || !ncols || !bucket_of || !nbuckets) fail(GWB200_BAD_ARGUMENT, "empty or null batch");
         if (nfreq <= 0 || budget_bytes <= 0) fail(GWB200_BAD_SHAPE, "nfreq and the budget must be positive");
-        if (precision != GWB200_FP64 && precision != GWB200_MIXED) fail(GWB200_BAD_ARGUMENT, "unknown precision");
-        const bool mixed = precision == GWB200_MIXED;
+        if (precision != GWB200_FP64 && precision != GWB200_MIXED && precision != GWB200_MIXED_REFINED)
+            fail(GWB200_BAD_ARGUMENT, "unknown precision");
+        const bool mixed = precision != GWB200_FP64;
         std::vector<int64_t> ns(nph, nph + nsys), ms(ncols, ncols + nsys);
         for (int64_t i = 0; i < nsys; ++i)
             if (ns[(size_t)i] <= 0 || ms[(size_t)i] <= 0) fail(GWB200_BAD_SHAPE, "nph and ncols must be positive");
@@ -1308,7 +1334,8 @@ int gwb200_run_g0w0_batch(gwb200_handle* const* systems, int64_t nsys, const int
             if (fs[(size_t)i] <= 0) fail(GWB200_BAD_SHAPE, "--freq-points must be positive");
             if (ps[(size_t)i] <= 0) fail(GWB200_BAD_SHAPE, "--pade-params must be positive");
         }
-        if (precision != GWB200_FP64 && precision != GWB200_MIXED) fail(GWB200_BAD_ARGUMENT, "unknown precision");
+        if (precision != GWB200_FP64 && precision != GWB200_MIXED && precision != GWB200_MIXED_REFINED)
+            fail(GWB200_BAD_ARGUMENT, "unknown precision");
         std::vector<gwb200_handle*> hs(systems, systems + nsys);
         for (gwb200_handle* h : hs)
             if (!h) fail(GWB200_BAD_ARGUMENT, "null handle in the batch");
@@ -1334,9 +1361,16 @@ int gwb200_run_g0w0_batch(gwb200_handle* const* systems, int64_t nsys, const int
             ns[(size_t)i] = h->n;
             ms[(size_t)i] = nstates[i] * h->nmo;
         }
-        const bool mixed = precision == GWB200_MIXED;
+        const bool mixed = precision != GWB200_FP64;
+        const bool refine = precision == GWB200_MIXED_REFINED;
         const bool mixed_tc = mixed && mixed_update_on_tcgen05(w);
         const bool oz = !mixed && fp64_update_mode() != 1 && (w->mem_limit <= 0 || fp64_update_mode() == 2);
+        if (refine)  // each molecule's pivoted Cholesky factor of V, on its own stream, before any capture
+            for (gwb200_handle* h : hs)
+                if (h->pchol_rank < 0) {
+                    size_buffer(h, h->pchol, pchol_bytes(h->n));
+                    h->pchol_rank = launch_pchol(h->v.as<double>(), h->n, h->pchol.p, &h->pchol_ct, h->stream);
+                }
         gwb200_stats local{};
         gwb200_stats* st = stats ? stats : &local;
         *st = gwb200_stats{};
@@ -1385,7 +1419,7 @@ int gwb200_run_g0w0_batch(gwb200_handle* const* systems, int64_t nsys, const int
             batch_candidates(key, n_sorted, m_sorted, f_sorted, mixed, (size_t)(0.85 * (double)avail / lanes));
         // chunks of every candidate inside one budget (all candidates share the workspaces)
         const TallGeometry gmax = make_geometry(n_sorted.back(), *std::max_element(m_sorted.begin(), m_sorted.end()));
-        if (batch_bytes_per_matrix(gmax, mixed, oz) > avail)
+        if (batch_bytes_per_matrix(gmax, mixed, oz, refine) > avail)
             fail(GWB200_OOM, "not enough device memory for one frequency of the largest eps(iw) in the batch");
         size_t budget = (size_t)(0.85 * (double)avail / lanes);  // per lane
         // GWB200_MAX_FREQ_CHUNK caps the matrices per launch sequence (tests use it to split buckets)
@@ -1399,8 +1433,8 @@ int gwb200_run_g0w0_batch(gwb200_handle* const* systems, int64_t nsys, const int
             groups.clear();
             need = BatchNeed{};
             for (const auto& p : cands) {
-                chunks.push_back(batch_chunks(hs, ms, fs, order, p, mixed, oz, budget, cap, groups));
-                batch_need(chunks.back(), mixed, oz, need);
+                chunks.push_back(batch_chunks(hs, ms, fs, order, p, mixed, oz, refine, budget, cap, groups));
+                batch_need(chunks.back(), mixed, oz, refine, need);
             }
             if (need.total() * (size_t)lanes <= (size_t)(0.9 * (double)avail) || attempt >= 12) break;
             budget = (size_t)(0.7 * (double)budget);
@@ -1411,6 +1445,7 @@ int gwb200_run_g0w0_batch(gwb200_handle* const* systems, int64_t nsys, const int
             size_buffer(w, ln.linv, need.linv);
             size_buffer(w, ln.qacc, need.qacc);
             if (need.panel) size_buffer(w, ln.panel, need.panel);
+            if (need.refine) size_buffer(w, ln.refine, need.refine);
             ln.sched.ensure(sizeof(unsigned long long));
             if (l > 0 && !ln.stream) {
                 GWB_CUDA(cudaStreamCreateWithFlags(&ln.stream, cudaStreamNonBlocking));
@@ -1506,7 +1541,7 @@ int gwb200_run_g0w0_batch(gwb200_handle* const* systems, int64_t nsys, const int
             fork();
             for (int l = 0; l < lanes; ++l)
                 n_launch += batch_screen(w, w->lanes[l], lane_stream(l), lane_ctas, chunks[c], assign[c][(size_t)l],
-                                         dgroups, variants[c], mixed, mixed_tc, oz);
+                                         dgroups, groups, variants[c], mixed, mixed_tc, oz, refine);
             join();
             return n_launch;
         };

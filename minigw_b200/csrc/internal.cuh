@@ -188,6 +188,18 @@ int launch_refine_chunk(const TallGeometry& g, int64_t nf, float* a, float* linv
                         const double* dvec, const double* ct, int64_t r_pad, void* work, double* qacc,
                         unsigned long long* err_pivot, cudaStream_t s, float* panel, unsigned long long* sched,
                         int max_ctas);
+// The parts of launch_refine_chunk, for batches: the in-place reversal-transpose of the factor and
+// the reversal of the right-hand sides within the first n_flip indices (a molecule's own n_pad: it
+// sits in the top-left corner of the chunk's matrices, identity-padded, so its blocks keep the
+// positions they have in its own solve); the backward solve of a chunk of geometry g (flip: first
+// the reversal over g.n_pad); the correction terms of one molecule (own geometry gm) for its nf
+// matrices from `a`, into qacc (row stride ldq).
+int launch_refine_flip(const TallGeometry& ga, int64_t nf, float* a, int64_t n_flip, cudaStream_t s);
+int launch_refine_solve(const TallGeometry& g, int64_t nf, float* a, float* linv, unsigned long long* err_pivot,
+                        cudaStream_t s, float* panel, unsigned long long* sched, int max_ctas, bool flip);
+int launch_refine_terms(const TallGeometry& ga, int64_t nf, const float* a, const TallGeometry& gm, const double* xt,
+                        const double* dvec, const double* ct, int64_t r_pad, void* work, double* qacc, int64_t ldq,
+                        cudaStream_t s);
 // kernels_tc.cu: tcgen05 3xTF32 trailing update C -= P P^T of the mixed form (K = kdim columns from
 // kb0, output columns [c_begin, n_pad), rows [c_begin, rows)).  Two launches; `sched` is one
 // device word the kernel's work counter lives in.  A device wait that expires records pivot 0 in
@@ -215,13 +227,15 @@ struct BatchGroup {
     double* q_out;       // forms of the group's first frequency, ldq_out apart
     int64_t n, m, n_pad, ldq_out;
     int64_t mat0, nf;    // first matrix of the chunk this group fills, and how many (frequencies)
+    const double* ct;    // refined mixed form: the molecule's pivoted Cholesky factor C^T (r_pad x n_pad)
+    int64_t r_pad;
 };
 int launch_build_tall_batch(const TallGeometry& g, const BatchGroup* groups, int64_t ngroups, bool fp32, void* a,
                             cudaStream_t s);
 int launch_forms_scatter(const BatchGroup* groups, int64_t ngroups, const double* qacc, int64_t ldq, cudaStream_t s);
 // device bytes of one batched matrix (tall matrix, 64x64 inverse, scale vector, norm accumulators,
 // tcgen05 / int8 operand workspace)
-size_t batch_bytes_per_matrix(const TallGeometry& g, bool mixed, bool fp64_oz);
+size_t batch_bytes_per_matrix(const TallGeometry& g, bool mixed, bool fp64_oz, bool refine = false);
 // bucket sizes over the molecules sorted by (n, m): minimises block-step latency + padded work
 std::vector<int64_t> plan_buckets(const std::vector<int64_t>& n_sorted, const std::vector<int64_t>& m_sorted,
                                   const std::vector<int64_t>& f_sorted, bool mixed, size_t budget, double step_us,

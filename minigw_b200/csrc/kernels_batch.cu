@@ -92,10 +92,10 @@ int launch_forms_scatter(const BatchGroup* groups, int64_t ngroups, const double
     return 1;
 }
 
-size_t batch_bytes_per_matrix(const TallGeometry& g, bool mixed, bool fp64_oz) {
-    if (mixed)
+size_t batch_bytes_per_matrix(const TallGeometry& g, bool mixed, bool fp64_oz, bool refine) {
+    if (mixed)  // refined: the correction's workspace at the bucket's geometry (rank <= n_pad)
         return sizeof(float) * ((size_t)g.stride + kNb * kNb) + sizeof(double) * (g.n_pad + g.m_pad) +
-               tc_panel_bytes_per_freq(g);
+               tc_panel_bytes_per_freq(g) + (refine ? refine_bytes_per_freq(g, g.n_pad) : 0);
     return sizeof(double) * ((size_t)g.stride + g.n_pad + kNb * kNb + g.m_pad) + (fp64_oz ? oz_slice_bytes_per_freq(g) : 0);
 }
 

@@ -72,29 +72,33 @@ __global__ void __launch_bounds__(256) k_flip_tiles32(float* __restrict__ a, int
     }
 }
 
-// Reverse [0, n_pad) of every right-hand-side row (rows n_pad .. n_pad + m_pad - 1).
-__global__ void k_reverse_rows32(float* __restrict__ a, int64_t ld, int64_t stride, int64_t n_pad, int64_t m_pad) {
+// Reverse [0, width) of every right-hand-side row (rows row0 .. row0 + m_pad - 1).
+__global__ void k_reverse_rows32(float* __restrict__ a, int64_t ld, int64_t stride, int64_t row0, int64_t width,
+                                 int64_t m_pad) {
     for (int64_t j = blockIdx.y; j < m_pad; j += gridDim.y) {
-        float* row = a + (size_t)blockIdx.z * stride + (size_t)(n_pad + j) * ld;
-        for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < n_pad / 2;
+        float* row = a + (size_t)blockIdx.z * stride + (size_t)(row0 + j) * ld;
+        for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < width / 2;
              c += (int64_t)gridDim.x * blockDim.x) {
             const float t = row[c];
-            row[c] = row[n_pad - 1 - c];
-            row[n_pad - 1 - c] = t;
+            row[c] = row[width - 1 - c];
+            row[width - 1 - c] = t;
         }
     }
 }
 
-// One CTA per right-hand side j of one frequency: z_j[i] = row[n_pad-1-i] (the solve ran on reversed
-// indices), y_j = dvec * z_j (FP64) into Y (m_pad x n_pad, zero past n and past m), t1 = x_j . y_j and
-// t2 = z_j . z_j (per-thread partial sums over a fixed stride, then a fixed tree).
+// One CTA per right-hand side j (row row0 + j of the tall matrix) of one frequency: z_j[i] =
+// row[na-1-i] (the solve ran on indices reversed within na, the molecule's own n_pad; a batched
+// molecule sits in the top-left corner of a bucket's larger matrix), y_j = dvec * z_j (FP64) into Y
+// (m_pad x n_pad of the molecule, zero past n and past m), t1 = x_j . y_j and t2 = z_j . z_j
+// (per-thread partial sums over a fixed stride, then a fixed tree).
 __global__ void __launch_bounds__(256) k_refine_prep(const float* __restrict__ a, int64_t ld, int64_t stride,
-                                                     int64_t n, int64_t n_pad, int64_t m, int64_t m_pad,
-                                                     const double* __restrict__ xt, const double* __restrict__ dvec,
-                                                     double* __restrict__ y, double* __restrict__ t12) {
+                                                     int64_t row0, int64_t na, int64_t n, int64_t n_pad, int64_t m,
+                                                     int64_t m_pad, const double* __restrict__ xt,
+                                                     const double* __restrict__ dvec, double* __restrict__ y,
+                                                     double* __restrict__ t12) {
     const int f = blockIdx.y;
     const int64_t j = blockIdx.x;
-    const float* row = a + (size_t)f * stride + (size_t)(n_pad + j) * ld;
+    const float* row = a + (size_t)f * stride + (size_t)(row0 + j) * ld;
     const double* d = dvec + (size_t)f * n_pad;
     double* yrow = y + ((size_t)f * m_pad + j) * n_pad;
     double s1 = 0.0, s2 = 0.0;
@@ -102,7 +106,7 @@ __global__ void __launch_bounds__(256) k_refine_prep(const float* __restrict__ a
     for (int64_t i = threadIdx.x; i < n_pad; i += blockDim.x) {
         double yi = 0.0;
         if (live && i < n) {
-            const double zi = (double)row[n_pad - 1 - i];
+            const double zi = (double)row[na - 1 - i];
             yi = d[i] * zi;
             s1 = fma(xt[j * n + i], yi, s1);
             s2 = fma(zi, zi, s2);
@@ -404,37 +408,53 @@ int64_t launch_pchol(const double* v, int64_t n, void* work, double** ct_out, cu
     return r;
 }
 
+int launch_refine_flip(const TallGeometry& ga, int64_t nf, float* a, int64_t n_flip, cudaStream_t s) {
+    const int nb = (int)(n_flip / kT);
+    k_flip_tiles32<<<dim3((unsigned)nb, (unsigned)nb, (unsigned)nf), 256, 0, s>>>(a, ga.ld, ga.stride, nb);
+    GWB_LAUNCH("k_flip_tiles32");
+    k_reverse_rows32<<<dim3((unsigned)std::max<int64_t>(1, n_flip / 512), (unsigned)std::min<int64_t>(ga.m_pad, 65535),
+                            (unsigned)nf),
+                       256, 0, s>>>(a, ga.ld, ga.stride, ga.n_pad, n_flip, ga.m_pad);
+    GWB_LAUNCH("k_reverse_rows32");
+    return 2;
+}
+
+int launch_refine_solve(const TallGeometry& g, int64_t nf, float* a, float* linv, unsigned long long* err_pivot,
+                        cudaStream_t s, float* panel, unsigned long long* sched, int max_ctas, bool flip) {
+    int launches = flip ? launch_refine_flip(g, nf, a, g.n_pad, s) : 0;
+    launches += launch_factor_chunk32(g, nf, a, linv, nullptr, err_pivot, s, nullptr, panel, sched, max_ctas,
+                                      /*solve_only=*/true);
+    return launches;
+}
+
+int launch_refine_terms(const TallGeometry& ga, int64_t nf, const float* a, const TallGeometry& gm, const double* xt,
+                        const double* dvec, const double* ct, int64_t r_pad, void* work, double* qacc, int64_t ldq,
+                        cudaStream_t s) {
+    double* y = static_cast<double*>(work);
+    double* t12 = y + (size_t)nf * gm.m_pad * gm.n_pad;
+    double* part = t12 + (size_t)nf * 2 * gm.m_pad;
+    // the solve ran on indices reversed within the molecule's own n_pad (launch_refine_flip), in the
+    // chunk's matrices (row stride ga.ld, right-hand sides from row ga.n_pad)
+    k_refine_prep<<<dim3((unsigned)gm.m_pad, (unsigned)nf), 256, 0, s>>>(a, ga.ld, ga.stride, ga.n_pad, gm.n_pad, gm.n,
+                                                                        gm.n_pad, gm.m, gm.m_pad, xt, dvec, y, t12);
+    GWB_LAUNCH("k_refine_prep");
+    const size_t smem = 4 * kT * kLdk * sizeof(double);
+    GWB_CUDA(cudaFuncSetAttribute(k_gram_sq, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k_gram_sq<<<dim3((unsigned)(gm.m_pad / kT), (unsigned)(r_pad / kT), (unsigned)nf), 256, smem, s>>>(
+        ct, y, gm.n_pad, gm.m_pad, r_pad, part);
+    GWB_LAUNCH("k_gram_sq");
+    k_refine_finish<<<dim3((unsigned)((gm.m + 255) / 256), (unsigned)nf), 256, 0, s>>>(t12, part, gm.m_pad, r_pad / kT,
+                                                                                      gm.m, qacc, ldq);
+    GWB_LAUNCH("k_refine_finish");
+    return 3;
+}
+
 int launch_refine_chunk(const TallGeometry& g, int64_t nf, float* a, float* linv, const double* xt,
                         const double* dvec, const double* ct, int64_t r_pad, void* work, double* qacc,
                         unsigned long long* err_pivot, cudaStream_t s, float* panel, unsigned long long* sched,
                         int max_ctas) {
-    int launches = 0;
-    const int nb = (int)(g.n_pad / kT);
-    k_flip_tiles32<<<dim3((unsigned)nb, (unsigned)nb, (unsigned)nf), 256, 0, s>>>(a, g.ld, g.stride, nb);
-    GWB_LAUNCH("k_flip_tiles32");
-    k_reverse_rows32<<<dim3((unsigned)std::max<int64_t>(1, g.n_pad / 512), (unsigned)std::min<int64_t>(g.m_pad, 65535),
-                            (unsigned)nf),
-                       256, 0, s>>>(a, g.ld, g.stride, g.n_pad, g.m_pad);
-    GWB_LAUNCH("k_reverse_rows32");
-    launches += 2;
-    launches += launch_factor_chunk32(g, nf, a, linv, nullptr, err_pivot, s, nullptr, panel, sched, max_ctas,
-                                      /*solve_only=*/true);
-    double* y = static_cast<double*>(work);
-    double* t12 = y + (size_t)nf * g.m_pad * g.n_pad;
-    double* part = t12 + (size_t)nf * 2 * g.m_pad;
-    k_refine_prep<<<dim3((unsigned)g.m_pad, (unsigned)nf), 256, 0, s>>>(a, g.ld, g.stride, g.n, g.n_pad, g.m, g.m_pad, xt,
-                                                                       dvec, y, t12);
-    GWB_LAUNCH("k_refine_prep");
-    const size_t smem = 4 * kT * kLdk * sizeof(double);
-    GWB_CUDA(cudaFuncSetAttribute(k_gram_sq, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    k_gram_sq<<<dim3((unsigned)(g.m_pad / kT), (unsigned)(r_pad / kT), (unsigned)nf), 256, smem, s>>>(
-        ct, y, g.n_pad, g.m_pad, r_pad, part);
-    GWB_LAUNCH("k_gram_sq");
-    k_refine_finish<<<dim3((unsigned)((g.m + 255) / 256), (unsigned)nf), 256, 0, s>>>(t12, part, g.m_pad, r_pad / kT,
-                                                                                     g.m, qacc, g.m_pad);
-    GWB_LAUNCH("k_refine_finish");
-    launches += 3;
-    return launches;
+    return launch_refine_solve(g, nf, a, linv, err_pivot, s, panel, sched, max_ctas, /*flip=*/true) +
+           launch_refine_terms(g, nf, a, g, xt, dvec, ct, r_pad, work, qacc, g.m_pad, s);
 }
 
 } // namespace gwb200

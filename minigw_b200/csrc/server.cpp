@@ -10,7 +10,7 @@
 // a result is bit-identical whether the request ran alone or in a mix.
 //
 // Merging: when a worker frees up and several compatible requests wait (eta = 0, the same
-// precision, FP64 or the unrefined mixed form, small enough not to fill the GPU alone), it takes up
+// precision, small enough not to fill the GPU alone), it takes up
 // to `max_merge` of them at once (and no more than a fair share of the queue per worker), loads
 // each into a handle of its own (the worker's handle leads, the others come from the worker's
 // member handles), and solves them with one gwb200_run_g0w0_batch: their frequency work is
@@ -97,7 +97,9 @@ size_t resident_bytes(const gwb200_request& r) {
     const size_t nmo = (size_t)r.nmo, nocc = (size_t)r.nocc, n = nocc * (nmo - nocc);
     const size_t m = (size_t)r.nstates * nmo;
     const size_t n64 = (n + 63) / 64 * 64, m64 = (m + 63) / 64 * 64;
-    return sizeof(double) * (n * n + m * n + nmo * nocc + (size_t)r.nfreq * (n64 + m64) + 4 * nmo * (size_t)r.nfreq) +
+    const size_t pchol = r.precision == GWB200_MIXED_REFINED ? 2 * n * n64 : 0;  // the factor of V (refined form)
+    return sizeof(double) * (n * n + m * n + nmo * nocc + (size_t)r.nfreq * (n64 + m64) + 4 * nmo * (size_t)r.nfreq +
+                             pchol) +
            ((size_t)1 << 16);
 }
 
@@ -116,7 +118,8 @@ constexpr int64_t kMergeMaxNph = 1536;
 
 bool mergeable(const gwb200_request& r) {
     const int64_t n = r.nocc * (r.nmo - r.nocc);
-    return r.eta == 0.0 && (r.precision == GWB200_FP64 || r.precision == GWB200_MIXED) && n <= kMergeMaxNph;
+    return r.eta == 0.0 && n <= kMergeMaxNph &&
+           (r.precision == GWB200_FP64 || r.precision == GWB200_MIXED || r.precision == GWB200_MIXED_REFINED);
 }
 
 int make_slot_handle(gwb200_server* s, gwb200_handle** out) {

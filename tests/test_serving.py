@@ -50,22 +50,22 @@ def test_server_matches_backend_and_rejects_oversize():
             assert e.value.status == "GWB200_OOM"
 
 
-@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+@pytest.mark.parametrize("precision", ["fp64", "mixed", "mixed-refined"])
 def test_merged_requests_identical_to_alone(precision):
     """Requests that wait while the worker is busy are merged into one gwb200_run_g0w0_batch; each
     result is bit-identical to the same request solved alone (merging off), and a request that
-    cannot share launches (refined mixed form) runs alone in between."""
+    cannot share launches (eta != 0, the complex symmetric path) runs alone in between."""
     from minigw_b200 import B200Server
 
     reqs = _requests()
     with B200Server(0, slots=1, hbm_budget_bytes=8 << 30, merge=1) as alone:
         ref = [alone.wait(alone.submit(inp, nf, 12, st, precision=precision)) for inp, nf, st in reqs]
         odd = reqs[2]
-        ref_odd = alone.wait(alone.submit(odd[0], odd[1], 12, odd[2], precision="mixed-refined"))
+        ref_odd = alone.wait(alone.submit(odd[0], odd[1], 12, odd[2], eta=0.01))
         assert alone.counters()["merged_requests"] == 0
     with B200Server(0, slots=1, hbm_budget_bytes=8 << 30, merge=8) as srv:
         tickets = [srv.submit(inp, nf, 12, st, precision=precision) for inp, nf, st in reqs[:3]]
-        t_odd = srv.submit(odd[0], odd[1], 12, odd[2], precision="mixed-refined")
+        t_odd = srv.submit(odd[0], odd[1], 12, odd[2], eta=0.01)
         tickets += [srv.submit(inp, nf, 12, st, precision=precision) for inp, nf, st in reqs[3:]]
         got = [srv.wait(t) for t in tickets]
         got_odd = srv.wait(t_odd)
