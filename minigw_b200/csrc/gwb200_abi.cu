@@ -133,7 +133,7 @@ struct gwb200_handle {
     DevBuf tc_sched;  // work counter of the tcgen05 update kernel
     // GWB200_MIXED_REFINED: pivoted Cholesky factor of the resident V_ph (computed on first use after
     // a load; pchol_rank < 0: not yet) and the per-chunk refinement workspace
-    DevBuf pchol, refine;
+    DevBuf pchol, pchol_sl, refine;  // pchol_sl: the factor's int8 digit slices
     int64_t pchol_rank = -1;
     double* pchol_ct = nullptr;
     DevBuf batch_desc;  // BatchGroup tables of gwb200_run_g0w0_batch (when this handle leads a batch)
@@ -251,6 +251,21 @@ void check_states(const gwb200_handle* h, const int64_t* states, int64_t nstates
     if (std::adjacent_find(seen.begin(), seen.end()) != seen.end()) fail(GWB200_BAD_SHAPE, "duplicate state in the state list");
 }
 
+// The pivoted Cholesky factor of the resident V_ph (and its int8 digit slices), computed on `s` on
+// first use after a load (this synchronises `s`).
+RefineFactor refine_factor(gwb200_handle* h, cudaStream_t s) {
+    if (h->pchol_rank < 0) {
+        size_buffer(h, h->pchol, pchol_bytes(h->n));
+        const int64_t r = launch_pchol(h->v.as<double>(), h->n, h->pchol.p, &h->pchol_ct, s);
+        const int64_t n_pad = round_up(h->n, kNb);
+        size_buffer(h, h->pchol_sl, gram_oz_system_bytes(n_pad, r));
+        launch_slice_ct(h->pchol_ct, r, n_pad, h->pchol_sl.p, s);
+        h->pchol_rank = r;
+    }
+    return RefineFactor{h->pchol_ct, std::max<int64_t>(kNb, round_up(h->pchol_rank, kNb)), h->pchol_sl.p,
+                        h->pchol_rank};
+}
+
 float elapsed(cudaEvent_t a, cudaEvent_t b) {
     float ms = 0.f;
     GWB_CUDA(cudaEventElapsedTime(&ms, a, b));
@@ -315,12 +330,10 @@ void compute_forms(gwb200_handle* h, const double* omega, int64_t nfreq, const i
     const bool fp64_oz = !mixed && !cplx && fp64_update_mode() != 1 && (h->mem_limit <= 0 || fp64_update_mode() == 2);
     // refined mixed form: V_ph = C C^T once per loaded system (its rank sizes the correction's work)
     int64_t r_pad = 0;
+    RefineFactor fac{};
     if (refine) {
-        if (h->pchol_rank < 0) {
-            size_buffer(h, h->pchol, pchol_bytes(h->n));
-            h->pchol_rank = launch_pchol(h->v.as<double>(), h->n, h->pchol.p, &h->pchol_ct, s);
-        }
-        r_pad = std::max<int64_t>(kNb, round_up(h->pchol_rank, kNb));
+        fac = refine_factor(h, s);
+        r_pad = fac.r_pad;
     }
     const size_t per_freq = mixed ? sizeof(float) * ((size_t)g.stride + kNb * kNb) + sizeof(double) * (g.n_pad + g.m_pad) +
                                         (mixed_tc ? tc_panel_bytes_per_freq(g) : 0) +
@@ -343,7 +356,8 @@ void compute_forms(gwb200_handle* h, const double* omega, int64_t nfreq, const i
         size_t budget = (size_t)((double)avail * 0.85);
         if (h->mem_limit > 0) {  // the handle's cap minus what the system and panels already hold
             const size_t resident = h->pqo.bytes + h->xdiag.bytes + h->v.bytes + h->xt.bytes + h->qall.bytes +
-                                    h->sigma.bytes + h->qp_scratch.bytes + h->pchol.bytes + ((size_t)1 << 20);
+                                    h->sigma.bytes + h->qp_scratch.bytes + h->pchol.bytes + h->pchol_sl.bytes +
+                                    ((size_t)1 << 20);
             const size_t lim = (size_t)h->mem_limit;
             const size_t room = lim > resident ? lim - resident : 0;
             budget = std::min(budget, room);
@@ -413,7 +427,7 @@ void compute_forms(gwb200_handle* h, const double* omega, int64_t nfreq, const i
                                               h->tc_sched.as<unsigned long long>(), h->persistent_ctas);
             if (refine)  // qacc <- 2 x^T y - z^T z - y^T V y (FP64 energy functional at the FP32 solve)
                 launches += launch_refine_chunk(g, nf, h->a.as<float>(), h->linv.as<float>(), h->xt.as<double>(),
-                                                h->dvec.as<double>(), h->pchol_ct, r_pad, h->refine.p,
+                                                h->dvec.as<double>(), fac, h->refine.p,
                                                 h->qacc.as<double>(), h->err.as<unsigned long long>(), s,
                                                 mixed_tc ? h->panel32.as<float>() : nullptr,
                                                 h->tc_sched.as<unsigned long long>(), h->persistent_ctas);
@@ -567,8 +581,9 @@ std::vector<BatchChunk> batch_chunks(const std::vector<gwb200_handle*>& hs, cons
                 gr.ldq_out = gi.m_pad;
                 gr.mat0 = cur.nmat;
                 gr.nf = nf;
-                gr.ct = refine ? h->pchol_ct : nullptr;
-                gr.r_pad = refine ? std::max<int64_t>(kNb, round_up(h->pchol_rank, kNb)) : 0;
+                if (refine)
+                    gr.fac = RefineFactor{h->pchol_ct, std::max<int64_t>(kNb, round_up(h->pchol_rank, kNb)),
+                                          h->pchol_sl.p, h->pchol_rank};
                 groups.push_back(gr);
                 ++cur.ngroups;
                 cur.nmat += nf;
@@ -630,9 +645,9 @@ int64_t batch_screen(gwb200_handle* w, BatchLane& lane, cudaStream_t s, int max_
                 for (int64_t q = 0; q < c.ngroups; ++q) {
                     const BatchGroup& gr = hgroups[(size_t)(c.group0 + q)];
                     launches += launch_refine_terms(c.g, gr.nf, lane.a.as<float>() + (size_t)gr.mat0 * c.g.stride,
-                                                    make_geometry(gr.n, gr.m), gr.xt, gr.dvec, gr.ct, gr.r_pad,
+                                                    make_geometry(gr.n, gr.m), gr.xt, gr.dvec, gr.fac,
                                                     lane.refine.p, lane.qacc.as<double>() + (size_t)gr.mat0 * c.g.m_pad,
-                                                    c.g.m_pad, s);
+                                                    c.g.m_pad, err, s);
                 }
             }
         } else
@@ -721,7 +736,7 @@ int gwb200_destroy(gwb200_handle* h) {
     if (h->stream) cudaStreamSynchronize(h->stream);
     h->stage_in.release();
     h->stage_out.release();
-    for (DevBuf* b : {&h->pchol, &h->refine, &h->pqo, &h->xdiag, &h->mo, &h->vxc_diag, &h->delta, &h->v, &h->sigx, &h->flag, &h->xt, &h->dvec, &h->a,
+    for (DevBuf* b : {&h->pchol, &h->pchol_sl, &h->refine, &h->pqo, &h->xdiag, &h->mo, &h->vxc_diag, &h->delta, &h->v, &h->sigx, &h->flag, &h->xt, &h->dvec, &h->a,
                       &h->linv, &h->qacc, &h->qall, &h->sigma, &h->omega, &h->weight, &h->states, &h->err, &h->qp,
                       &h->qp_scratch, &h->omega_out, &h->panel32, &h->tc_sched, &h->batch_desc})
         b->release();
@@ -801,7 +816,8 @@ void load_system_impl(gwb200_handle* h, int64_t nmo, int64_t nocc, const double*
     const size_t nmo2 = (size_t)nmo * nmo;
     const int64_t nvir = nmo - nocc, n = nocc * nvir;
     if (h->mem_limit > 0)  // drop the previous request's workspaces before sizing this system
-        for (DevBuf* b : {&h->xt, &h->dvec, &h->a, &h->linv, &h->qacc, &h->qall, &h->panel32, &h->pchol, &h->refine})
+        for (DevBuf* b : {&h->xt, &h->dvec, &h->a, &h->linv, &h->qacc, &h->qall, &h->panel32, &h->pchol, &h->pchol_sl,
+                          &h->refine})
             b->release();
     if (bound) {
         h->pqo.release();
@@ -1277,6 +1293,7 @@ std::vector<int64_t> batch_graph_key(const gwb200_handle* w, const std::vector<g
                                 &h->weight, &h->states, &h->delta, &h->mo, &h->sigx, &h->vxc_diag})
             put(b->p);
         put(h->pchol_ct);
+        put(h->pchol_sl.p);
         gkey.push_back(h->pchol_rank);
     }
     put(w->batch_desc.p);
@@ -1366,11 +1383,7 @@ int gwb200_run_g0w0_batch(gwb200_handle* const* systems, int64_t nsys, const int
         const bool mixed_tc = mixed && mixed_update_on_tcgen05(w);
         const bool oz = !mixed && fp64_update_mode() != 1 && (w->mem_limit <= 0 || fp64_update_mode() == 2);
         if (refine)  // each molecule's pivoted Cholesky factor of V, on its own stream, before any capture
-            for (gwb200_handle* h : hs)
-                if (h->pchol_rank < 0) {
-                    size_buffer(h, h->pchol, pchol_bytes(h->n));
-                    h->pchol_rank = launch_pchol(h->v.as<double>(), h->n, h->pchol.p, &h->pchol_ct, h->stream);
-                }
+            for (gwb200_handle* h : hs) refine_factor(h, h->stream);
         gwb200_stats local{};
         gwb200_stats* st = stats ? stats : &local;
         *st = gwb200_stats{};

@@ -181,13 +181,31 @@ int launch_factor_chunk32(const TallGeometry& g, int64_t nf, float* a, float* li
 // r_pad = max(64, r rounded up to 64)) in *ct_out (inside `work`).  launch_refine_chunk runs after
 // launch_factor_chunk32 on the same chunk: the backward solve against the FP32 factor (solve-only
 // pass), then qacc[f][j] = 2 x^T y - z^T z - y^T V y (`work`: refine_bytes_per_freq(g, r_pad) * nf).
+// The factor of V a correction uses: C^T (r_pad x n_pad FP64, r_pad = r rounded up to 64) for the
+// DMMA Gram product, and its digit slices (gram_oz_system_bytes, launch_slice_ct) for the int8 one.
+struct RefineFactor {
+    const double* ct;
+    int64_t r_pad;
+    const void* ct_slices;
+    int64_t rank;
+};
 size_t refine_bytes_per_freq(const TallGeometry& g, int64_t r_pad);
 size_t pchol_bytes(int64_t n);
 int64_t launch_pchol(const double* v, int64_t n, void* work, double** ct_out, cudaStream_t s);
 int launch_refine_chunk(const TallGeometry& g, int64_t nf, float* a, float* linv, const double* xt,
-                        const double* dvec, const double* ct, int64_t r_pad, void* work, double* qacc,
+                        const double* dvec, const RefineFactor& fac, void* work, double* qacc,
                         unsigned long long* err_pivot, cudaStream_t s, float* panel, unsigned long long* sched,
                         int max_ctas);
+// GWB200_REFINE_GRAM=dmma runs y^T V y on the FP64 pipe; by default on the int8 tensor cores.
+bool refine_gram_on_int8();
+// kernels_gram_oz.cu: y^T V y = ||C^T y||^2 from int8 digit slices (tcgen05 kind::i8).
+int64_t gram_oz_rows(int64_t r);
+size_t gram_oz_system_bytes(int64_t n_pad, int64_t r);
+void launch_slice_ct(const double* ct, int64_t r, int64_t n_pad, void* out, cudaStream_t s);
+int launch_refine_terms_oz(const TallGeometry& ga, int64_t nf, const float* a, const TallGeometry& gm,
+                           const double* xt, const double* dvec, const void* ct_slices, int64_t r, void* work,
+                           unsigned long long* err, cudaStream_t s, double** t12_out, double** part_out,
+                           int64_t* nkt_out);
 // The parts of launch_refine_chunk, for batches: the in-place reversal-transpose of the factor and
 // the reversal of the right-hand sides within the first n_flip indices (a molecule's own n_pad: it
 // sits in the top-left corner of the chunk's matrices, identity-padded, so its blocks keep the
@@ -198,8 +216,8 @@ int launch_refine_flip(const TallGeometry& ga, int64_t nf, float* a, int64_t n_f
 int launch_refine_solve(const TallGeometry& g, int64_t nf, float* a, float* linv, unsigned long long* err_pivot,
                         cudaStream_t s, float* panel, unsigned long long* sched, int max_ctas, bool flip);
 int launch_refine_terms(const TallGeometry& ga, int64_t nf, const float* a, const TallGeometry& gm, const double* xt,
-                        const double* dvec, const double* ct, int64_t r_pad, void* work, double* qacc, int64_t ldq,
-                        cudaStream_t s);
+                        const double* dvec, const RefineFactor& fac, void* work, double* qacc, int64_t ldq,
+                        unsigned long long* err, cudaStream_t s);
 // kernels_tc.cu: tcgen05 3xTF32 trailing update C -= P P^T of the mixed form (K = kdim columns from
 // kb0, output columns [c_begin, n_pad), rows [c_begin, rows)).  Two launches; `sched` is one
 // device word the kernel's work counter lives in.  A device wait that expires records pivot 0 in
@@ -227,8 +245,7 @@ struct BatchGroup {
     double* q_out;       // forms of the group's first frequency, ldq_out apart
     int64_t n, m, n_pad, ldq_out;
     int64_t mat0, nf;    // first matrix of the chunk this group fills, and how many (frequencies)
-    const double* ct;    // refined mixed form: the molecule's pivoted Cholesky factor C^T (r_pad x n_pad)
-    int64_t r_pad;
+    RefineFactor fac;    // refined mixed form: the molecule's pivoted Cholesky factor of V
 };
 int launch_build_tall_batch(const TallGeometry& g, const BatchGroup* groups, int64_t ngroups, bool fp32, void* a,
                             cudaStream_t s);

@@ -35,6 +35,8 @@
 #include "internal.cuh"
 
 #include <cmath>
+#include <cstdlib>
+#include <cstring>
 
 namespace gwb200 {
 namespace {
@@ -428,33 +430,51 @@ int launch_refine_solve(const TallGeometry& g, int64_t nf, float* a, float* linv
 }
 
 int launch_refine_terms(const TallGeometry& ga, int64_t nf, const float* a, const TallGeometry& gm, const double* xt,
-                        const double* dvec, const double* ct, int64_t r_pad, void* work, double* qacc, int64_t ldq,
-                        cudaStream_t s) {
-    double* y = static_cast<double*>(work);
-    double* t12 = y + (size_t)nf * gm.m_pad * gm.n_pad;
-    double* part = t12 + (size_t)nf * 2 * gm.m_pad;
-    // the solve ran on indices reversed within the molecule's own n_pad (launch_refine_flip), in the
-    // chunk's matrices (row stride ga.ld, right-hand sides from row ga.n_pad)
-    k_refine_prep<<<dim3((unsigned)gm.m_pad, (unsigned)nf), 256, 0, s>>>(a, ga.ld, ga.stride, ga.n_pad, gm.n_pad, gm.n,
-                                                                        gm.n_pad, gm.m, gm.m_pad, xt, dvec, y, t12);
-    GWB_LAUNCH("k_refine_prep");
-    const size_t smem = 4 * kT * kLdk * sizeof(double);
-    GWB_CUDA(cudaFuncSetAttribute(k_gram_sq, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    k_gram_sq<<<dim3((unsigned)(gm.m_pad / kT), (unsigned)(r_pad / kT), (unsigned)nf), 256, smem, s>>>(
-        ct, y, gm.n_pad, gm.m_pad, r_pad, part);
-    GWB_LAUNCH("k_gram_sq");
-    k_refine_finish<<<dim3((unsigned)((gm.m + 255) / 256), (unsigned)nf), 256, 0, s>>>(t12, part, gm.m_pad, r_pad / kT,
-                                                                                      gm.m, qacc, ldq);
+                        const double* dvec, const RefineFactor& fac, void* work, double* qacc, int64_t ldq,
+                        unsigned long long* err, cudaStream_t s) {
+    double* t12;
+    double* part;
+    int64_t nkt;
+    int launches;
+    if (refine_gram_on_int8()) {  // y^T V y from exact int8 products of digit slices (kernels_gram_oz.cu)
+        launches = launch_refine_terms_oz(ga, nf, a, gm, xt, dvec, fac.ct_slices, fac.rank, work, err, s, &t12, &part,
+                                          &nkt);
+    } else {  // on the FP64 tensor pipe (DMMA)
+        const int64_t r_pad = fac.r_pad;
+        double* y = static_cast<double*>(work);
+        t12 = y + (size_t)nf * gm.m_pad * gm.n_pad;
+        part = t12 + (size_t)nf * 2 * gm.m_pad;
+        // the solve ran on indices reversed within the molecule's own n_pad (launch_refine_flip), in
+        // the chunk's matrices (row stride ga.ld, right-hand sides from row ga.n_pad)
+        k_refine_prep<<<dim3((unsigned)gm.m_pad, (unsigned)nf), 256, 0, s>>>(a, ga.ld, ga.stride, ga.n_pad, gm.n_pad,
+                                                                            gm.n, gm.n_pad, gm.m, gm.m_pad, xt, dvec, y,
+                                                                            t12);
+        GWB_LAUNCH("k_refine_prep");
+        const size_t smem = 4 * kT * kLdk * sizeof(double);
+        GWB_CUDA(cudaFuncSetAttribute(k_gram_sq, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        k_gram_sq<<<dim3((unsigned)(gm.m_pad / kT), (unsigned)(r_pad / kT), (unsigned)nf), 256, smem, s>>>(
+            fac.ct, y, gm.n_pad, gm.m_pad, r_pad, part);
+        GWB_LAUNCH("k_gram_sq");
+        nkt = r_pad / kT;
+        launches = 2;
+    }
+    k_refine_finish<<<dim3((unsigned)((gm.m + 255) / 256), (unsigned)nf), 256, 0, s>>>(t12, part, gm.m_pad, nkt, gm.m,
+                                                                                      qacc, ldq);
     GWB_LAUNCH("k_refine_finish");
-    return 3;
+    return launches + 1;
 }
 
 int launch_refine_chunk(const TallGeometry& g, int64_t nf, float* a, float* linv, const double* xt,
-                        const double* dvec, const double* ct, int64_t r_pad, void* work, double* qacc,
+                        const double* dvec, const RefineFactor& fac, void* work, double* qacc,
                         unsigned long long* err_pivot, cudaStream_t s, float* panel, unsigned long long* sched,
                         int max_ctas) {
     return launch_refine_solve(g, nf, a, linv, err_pivot, s, panel, sched, max_ctas, /*flip=*/true) +
-           launch_refine_terms(g, nf, a, g, xt, dvec, ct, r_pad, work, qacc, g.m_pad, s);
+           launch_refine_terms(g, nf, a, g, xt, dvec, fac, work, qacc, g.m_pad, err_pivot, s);
+}
+
+bool refine_gram_on_int8() {
+    const char* e = std::getenv("GWB200_REFINE_GRAM");
+    return !(e && std::strcmp(e, "dmma") == 0);
 }
 
 } // namespace gwb200

@@ -132,3 +132,19 @@ def test_cfg2_refined_against_reference():
         rq = ref.forms(inp, om[fsel], states, backend="blas-lapack")
         err = np.abs(q[fsel] - rq.real).max() / np.abs(rq.real).max()
         assert err <= FORMS_RTOL, err
+
+
+@pytest.mark.parametrize("nmo,nocc,states,nfreq", [(14, 4, [3, 4], 9), (60, 10, [8, 9, 10, 11], 12)])
+def test_refined_gram_int8_matches_dmma(backend, monkeypatch, nmo, nocc, states, nfreq):
+    """The correction's y^T V y on the int8 tensor cores (digit slices, the default) against the FP64
+    DMMA product (GWB200_REFINE_GRAM=dmma): the same forms to FP64 rounding."""
+    from minigw_b200 import generate_transformed_legendre_grid
+    from minigw_b200.synthetic import make_input
+
+    inp = make_input(nmo, nocc, seed=nmo + 77)
+    om, _ = generate_transformed_legendre_grid(nfreq)
+    backend.load_system(inp)
+    q8, _ = backend.screened_forms(om, states, precision="mixed-refined")
+    monkeypatch.setenv("GWB200_REFINE_GRAM", "dmma")
+    q64, _ = backend.screened_forms(om, states, precision="mixed-refined")
+    assert np.abs(q8 - q64).max() <= 1e-12 * np.abs(q64).max()
