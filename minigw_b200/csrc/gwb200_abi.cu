@@ -258,8 +258,10 @@ RefineFactor refine_factor(gwb200_handle* h, cudaStream_t s) {
         size_buffer(h, h->pchol, pchol_bytes(h->n));
         const int64_t r = launch_pchol(h->v.as<double>(), h->n, h->pchol.p, &h->pchol_ct, s);
         const int64_t n_pad = round_up(h->n, kNb);
-        size_buffer(h, h->pchol_sl, gram_oz_system_bytes(n_pad, r));
-        launch_slice_ct(h->pchol_ct, r, n_pad, h->pchol_sl.p, s);
+        if (gram_oz_fits(n_pad)) {
+            size_buffer(h, h->pchol_sl, gram_oz_system_bytes(n_pad, r));
+            launch_slice_ct(h->pchol_ct, r, n_pad, h->pchol_sl.p, s);
+        }
         h->pchol_rank = r;
     }
     return RefineFactor{h->pchol_ct, std::max<int64_t>(kNb, round_up(h->pchol_rank, kNb)), h->pchol_sl.p,

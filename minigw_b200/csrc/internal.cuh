@@ -196,10 +196,14 @@ int launch_refine_chunk(const TallGeometry& g, int64_t nf, float* a, float* linv
                         const double* dvec, const RefineFactor& fac, void* work, double* qacc,
                         unsigned long long* err_pivot, cudaStream_t s, float* panel, unsigned long long* sched,
                         int max_ctas);
-// GWB200_REFINE_GRAM=dmma runs y^T V y on the FP64 pipe; by default on the int8 tensor cores.
-bool refine_gram_on_int8();
+// GWB200_REFINE_GRAM=dmma runs y^T V y on the FP64 pipe; by default on the int8 tensor cores
+// (when gram_oz_fits).
+bool refine_gram_on_int8(int64_t n_pad);
 // kernels_gram_oz.cu: y^T V y = ||C^T y||^2 from int8 digit slices (tcgen05 kind::i8).
 int64_t gram_oz_rows(int64_t r);
+// the int8 path's int32 accumulators hold the exact sums for n_pad up to 65536; beyond, DMMA
+bool gram_oz_fits(int64_t n_pad);
+size_t refine_oz_bytes_per_freq(const TallGeometry& g, int64_t r);
 size_t gram_oz_system_bytes(int64_t n_pad, int64_t r);
 void launch_slice_ct(const double* ct, int64_t r, int64_t n_pad, void* out, cudaStream_t s);
 int launch_refine_terms_oz(const TallGeometry& ga, int64_t nf, const float* a, const TallGeometry& gm,

@@ -3,24 +3,33 @@
 //
 // V = C C^T (pivoted Cholesky, kernels_refine.cu) with C^T r x n.  For every frequency f and right-
 // hand side j the correction needs t3 = sum_k (C^T y_j)_k^2 to FP64 accuracy: a GEMM G = C^T Y
-// (r x m per frequency, K = n) reduced by squares over k.  Here the operands are cut into signed
-// 7-bit digits with one power-of-two scale per row:
-//     C^T[k][i] = 2^{e_k} sum_{s=1..7} A_s[k][i] 2^{-7s} + (< 2^{e_k - 49})
-//     y_j[i]    = 2^{e_j} sum_{t=1..3} B_t[j][i] 2^{-7t}          (y rounded to 21 bits)
-// so that G[k][j] = 2^{e_k + e_j} sum_{l=2..8} 2^{-7l} S_l[k][j],  S_l = sum_{s+t=l, t<=3} A_s . B_t,
-// dropping only s + t > 8 (below 2^{-56} of the row scales).  Each S_l is an exact int32 sum over
-// the whole K (at most three (s, t) pairs per level: |S_l| <= 3 * 127^2 * n < 2^31 for n < 44000),
-// accumulated by 18 int8 tensor-core products per 32-deep K step in 7 TMEM accumulators.
+// (r x m per frequency, K = n) reduced by squares over k.  Here the operands are cut into balanced
+// digits in [-64, 64] (each the nearest integer to the scaled remainder) with one power-of-two scale
+// 2^{e} > 2 max|row| per row:
+//     C^T[k][i] = 2^{e_k} sum_{s=1..7} A_s[k][i] 2^{-7s} + (|.| <= 2^{e_k - 50})
+//     y_j[i]    = 2^{e_j} sum_{t=1..4} B_t[j][i] 2^{-7t}          (y rounded to 28 bits)
+// so that G[k][j] = 2^{e_k + e_j} sum_{l=2..9} 2^{-7l} S_l[k][j],  S_l = sum_{s+t=l} A_s . B_t,
+// dropping only s + t > 9 (products below 2^{-58} of the row scales, of either sign).  Each S_l is an
+// exact int32 sum over the whole K (at most four (s, t) pairs per level: |S_l| <= 4 * 64^2 * nk <
+// 2^31 for nk <= 65536, the K extent this path accepts), accumulated by 25 int8 tensor-core
+// products per 32-deep K step in 8 TMEM accumulators of 64 columns (the whole 512).
 //
-// Rounding y to 21 bits is free: the refined form evaluates the energy functional F(z) = 2 b^T z -
-// z^T eps z, which is stationary at the solution, so moving z by 2^-21 relative changes F by
-// ~2^-42; what matters is that t1 = x^T y, t2 = z^T z and t3 = y^T V y all use the same rounded
-// y.  k_refine_prep_oz therefore computes t1 and t2 from the rounded values it slices.
+// G sums n products of partly cancelling terms, so its error is set by the digits' error relative
+// to the row scale: truncated digits (a one-sided error of up to 2^-49) left the forms 1e-12 away
+// from the FP64 Gram on n = 336 and n = 500 (1.6e-10 Ha in Sigma_c on n = 2000); rounded digits and
+// the ninth level bring them to the FP64 product's own rounding level.
+//
+// Rounding y is nearly free: the refined form evaluates the energy functional F(z) = 2 b^T z -
+// z^T eps z, which is stationary at the solution, so a perturbation dz changes F by dz^T eps dz
+// only; what matters is that t1 = x^T y, t2 = z^T z and t3 = y^T V y all use the same rounded y
+// (k_refine_prep_oz computes t1 and t2 from the values it slices).  The rounding is absolute
+// (2^{e_j - 29} per element) and z = y / D^1/2 magnifies it where D is small: 3 digits (21 bits)
+// left 1e-11 relative in the forms, 4 digits are at the FP64 level.
 //
 // k_gram_oz: one CTA per (frequency, 128-row tile of C^T, 64 right-hand sides); warp 0 streams
-// the B slices of a 128-deep K chunk (3 x 8 KB, double-buffered) and the A slices (16 KB each)
+// the B slices of a 128-deep K chunk (4 x 8 KB, double-buffered) and the A slices (16 KB each)
 // through an 8-stage ring with bulk copies; warp 1 allocates TMEM (512 columns) and its lane 0
-// issues the MMAs; warps 2-5 read the 7 levels of their 32-row quadrant (warp % 4), form G in FP64, square,
+// issues the MMAs; warps 2-5 read the 8 levels of their 32-row quadrant (warp % 4), form G in FP64, square,
 // and sum each column over the rows (fixed shuffle tree, then the four quadrants in order): one
 // partial sum per (frequency, row tile, j), summed over row tiles by k_refine_finish.  Every
 // mbarrier wait is bounded (tc_common.cuh: expiry -> pivot 0 -> GWB200_DEVICE_TIMEOUT).
@@ -34,7 +43,8 @@ using namespace tc;
 
 constexpr int kGM = 128;                      // C^T rows per tile (TMEM lanes)
 constexpr int kGN = 64;                       // right-hand sides per tile (accumulator columns per level)
-constexpr int kASl = 7, kBSl = 3, kLevels = 7;
+constexpr int kASl = 7, kBSl = 4, kLevels = 8;  // levels l = 2 .. kLevels + 1
+constexpr int64_t kMaxNk = 65536;                 // 4 pairs * 64^2 * kMaxNk = 2^30
 constexpr int kKc = 128;                      // K bytes per chunk (one 128-byte swizzled row)
 constexpr int kSliceA = kGM * kKc;            // 16 KB
 constexpr int kSliceB = kGN * kKc;            // 8 KB
@@ -47,6 +57,7 @@ constexpr int kOffAF = 0, kOffAE = kOffAF + 8 * kAStages, kOffBF = kOffAE + 8 * 
               kOffTF = kOffBE + 16, kOffDrain = kOffTF + 8, kOffTmem = kOffDrain + 8, kOffAbort = kOffTmem + 4;
 static_assert(kOffAbort + 4 <= kHdr, "header");
 static_assert(kGramSmem <= 227 * 1024, "shared memory");
+static_assert(kLevels * kGN <= 512, "TMEM columns");
 
 // kind::i8: D S32, A and B signed 8-bit, K-major, N = 64, M = 128.
 constexpr uint32_t kIdesc = (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(kGN >> 3) << 17) | ((uint32_t)(kGM >> 4) << 24);
@@ -68,9 +79,18 @@ __device__ __forceinline__ size_t swz(int64_t row, int k) {
     return (size_t)row * kKc + (size_t)(((chunk ^ (int)(row & 7)) << 4) + in);
 }
 
+// Next balanced digit of v (|v| <= 1/2 in units of the current digit): rint(128 v) in [-64, 64],
+// v <- 128 v - digit, again |v| <= 1/2.  Exact in FP64.
+__device__ __forceinline__ int next_digit(double& v) {
+    const double t = v * 128.0;
+    const double d = rint(t);
+    v = t - d;
+    return (int)d;
+}
+
 // C^T (r x n_pad FP64, row stride n_pad) into 7 digit slices over nk = n_pad rounded up to 128 (zero
-// beyond n_pad and from row r), layout [kc][s][row < r128][128 B], one exponent per row.  One warp
-// per row.
+// beyond n_pad and from row r), layout [kc][s][row < r128][128 B], one exponent e per row with
+// max|row| < 2^{e-1}.  One warp per row.
 __global__ void __launch_bounds__(256) k_slice_ct(const double* __restrict__ ct, int64_t r, int64_t n_pad, int64_t nk,
                                                   int64_t r128, uint8_t* __restrict__ out, int32_t* __restrict__ exps) {
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -84,6 +104,7 @@ __global__ void __launch_bounds__(256) k_slice_ct(const double* __restrict__ ct,
     for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
     int e = 0;
     if (m > 0.0) frexp(m, &e);  // |x| < 2^e
+    ++e;                        // |x| < 2^{e-1}
     const double inv = pow2i(-e);
     const int64_t nkc = nk / kKc;
     for (int64_t kc = 0; kc < nkc; ++kc) {
@@ -92,18 +113,13 @@ __global__ void __launch_bounds__(256) k_slice_ct(const double* __restrict__ ct,
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
             const int64_t i = kc * kKc + k0 + q;
-            v[q] = (row < r && i < n_pad) ? src[i] * inv : 0.0;  // |v| < 1, exact
+            v[q] = (row < r && i < n_pad) ? src[i] * inv : 0.0;  // |v| < 1/2, exact
         }
 #pragma unroll
         for (int s = 0; s < kASl; ++s) {
             uint32_t word = 0;
 #pragma unroll
-            for (int q = 0; q < 4; ++q) {
-                const double t = v[q] * 128.0;
-                const double d = trunc(t);
-                v[q] = t - d;
-                word |= ((uint32_t)(int)d & 0xFFu) << (8 * q);
-            }
+            for (int q = 0; q < 4; ++q) word |= ((uint32_t)next_digit(v[q]) & 0xFFu) << (8 * q);
             *reinterpret_cast<uint32_t*>(out + ((size_t)(kc * kASl + s) * r128) * kKc + swz(row, k0)) = word;
         }
     }
@@ -111,7 +127,7 @@ __global__ void __launch_bounds__(256) k_slice_ct(const double* __restrict__ ct,
 }
 
 // One CTA per right-hand side j of one frequency (k_refine_prep's inputs): y_j = dvec * z_j in FP64,
-// rounded to 3 digits of 7 bits below its row scale; the digits into B slices [kc][t][j][128 B] of
+// rounded to kBSl balanced digits below its row scale; the digits into B slices [kc][t][j][128 B] of
 // the frequency, the exponent into yexp; t1 = x_j . y^ and t2 = z^ . z^ (z^ = y^ / dvec) from the
 // rounded values (fixed-order sums).
 __global__ void __launch_bounds__(256) k_refine_prep_oz(const float* __restrict__ a, int64_t ld, int64_t stride,
@@ -141,25 +157,24 @@ __global__ void __launch_bounds__(256) k_refine_prep_oz(const float* __restrict_
     }
     int e = 0;
     if (rm[0] > 0.0) frexp(rm[0], &e);
+    ++e;  // |y| < 2^{e-1}
     const double inv = pow2i(-e), scale = pow2i(e);
     uint8_t* out = yslices + (size_t)f * fbytes;
     double s1 = 0.0, s2 = 0.0;
     for (int64_t w4 = threadIdx.x; w4 < nk / 4; w4 += blockDim.x) {  // 4 consecutive elements per word
         const int64_t i0 = w4 * 4, kc = i0 / kKc;
         const int kb = (int)(i0 % kKc);
-        uint32_t word[kBSl] = {0u, 0u, 0u};
+        uint32_t word[kBSl] = {};
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
             const int64_t i = i0 + q;
-            double v = i < n_pad ? yrow[i] * inv : 0.0;  // |v| < 1, exact
-            double rec = 0.0;          // the rounded value, in units of the row scale
+            double v = i < n_pad ? yrow[i] * inv : 0.0;  // |v| < 1/2, exact
+            double rec = 0.0;          // the rounded value, in units of the last digit
 #pragma unroll
             for (int t = 0; t < kBSl; ++t) {
-                const double tt = v * 128.0;
-                const double dg = trunc(tt);
-                v = tt - dg;
-                rec = fma(rec, 128.0, dg);
-                word[t] |= ((uint32_t)(int)dg & 0xFFu) << (8 * q);
+                const int dg = next_digit(v);
+                rec = fma(rec, 128.0, (double)dg);  // exact: |rec| < 2^{7 kBSl}
+                word[t] |= ((uint32_t)dg & 0xFFu) << (8 * q);
             }
             if (live && i < n) {
                 const double yh = rec * pow2i(-7 * kBSl) * scale;  // exact
@@ -198,7 +213,7 @@ __global__ void __launch_bounds__(kGramThreads, 1)
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int64_t jt = blockIdx.x, it = blockIdx.y, f = blockIdx.z;
     const uint32_t base = smem_u32(gsm);
-    const uint32_t bbuf = (base + kHdr + 1023u) & ~1023u;   // 2 x 3 B slices
+    const uint32_t bbuf = (base + kHdr + 1023u) & ~1023u;   // 2 x kBSl B slices
     const uint32_t aring = bbuf + 2 * kBSl * kSliceB;        // A stages
     double* red = reinterpret_cast<double*>(gsm + (aring - base) + kAStages * kSliceA);  // 4 x 64
     volatile uint32_t* abort_flag = reinterpret_cast<volatile uint32_t*>(gsm + kOffAbort);
@@ -288,7 +303,7 @@ __global__ void __launch_bounds__(kGramThreads, 1)
                     break;
                 }
                 tc_fence_after();
-                for (int s = 0; s < kASl; ++s) {  // A slice s+1 against B slices 1 .. min(3, 7-s)
+                for (int s = 0; s < kASl; ++s) {  // A slice s+1 against B slices 1 .. min(kBSl, kLevels - s)
                     if (!mbar_wait(af(sa), pa, abort_flag, err)) {
                         ok = false;
                         break;
@@ -332,21 +347,31 @@ __global__ void __launch_bounds__(kGramThreads, 1)
             tc_fence_after();
             const int64_t krow = it * kGM + q * 32 + lane;
             const int ek = aexp[krow];
+            constexpr int kHalf = kLevels / 2;
             for (int c16 = 0; c16 < kGN / 16; ++c16) {
-                uint32_t v[kLevels][16];
+                double g[16];  // sum_l S_l 2^{-7l}, smallest level first (each term exact)
+                uint32_t v[kHalf][16];
 #pragma unroll
-                for (int L = 0; L < kLevels; ++L)
-                    tmem_ld16_nowait(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(L * kGN + 16 * c16), v[L]);
-                tmem_wait_ld();
+                for (int h = 1; h >= 0; --h) {  // levels kHalf.. (the small ones), then 0..kHalf-1
+#pragma unroll
+                    for (int L = 0; L < kHalf; ++L)
+                        tmem_ld16_nowait(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)((h * kHalf + L) * kGN + 16 * c16),
+                                         v[L]);
+                    tmem_wait_ld();
+#pragma unroll
+                    for (int c = 0; c < 16; ++c) {
+                        if (h == 1) g[c] = 0.0;
+#pragma unroll
+                        for (int L = kHalf - 1; L >= 0; --L)
+                            g[c] += (double)(int32_t)v[L][c] * pow2i(-7 * (h * kHalf + L + 2));
+                    }
+                }
 #pragma unroll
                 for (int c = 0; c < 16; ++c) {
                     const int64_t jj = jt * kGN + 16 * c16 + c;
                     const int ej = yexp[(size_t)f * m_pad + jj];
-                    double g = 0.0;  // sum_l S_l 2^{-7l}, smallest level first (each term exact)
-#pragma unroll
-                    for (int L = kLevels - 1; L >= 0; --L) g += (double)(int32_t)v[L][c] * pow2i(-7 * (L + 2));
-                    g *= pow2i(ek + ej);
-                    double sq = g * g;
+                    const double gg = g[c] * pow2i(ek + ej);
+                    double sq = gg * gg;
 #pragma unroll
                     for (int o = 16; o > 0; o >>= 1) sq += __shfl_xor_sync(0xffffffffu, sq, o);
                     if (lane == 0) red[q * kGN + 16 * c16 + c] = sq;
@@ -373,6 +398,8 @@ __global__ void __launch_bounds__(kGramThreads, 1)
 } // namespace
 
 int64_t gram_oz_rows(int64_t r) { return std::max<int64_t>(kGM, round_up(r, kGM)); }
+
+bool gram_oz_fits(int64_t n_pad) { return round_up(n_pad, kKc) <= kMaxNk; }
 
 size_t gram_oz_system_bytes(int64_t n_pad, int64_t r) {
     const int64_t r128 = gram_oz_rows(r), nk = round_up(n_pad, kKc);

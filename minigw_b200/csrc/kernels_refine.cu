@@ -34,6 +34,7 @@
 // Everything here is deterministic: sums run in a fixed order, no floating-point atomics.
 #include "internal.cuh"
 
+#include <algorithm>
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
@@ -362,8 +363,9 @@ constexpr int kPcholCtas = 128;
 
 } // namespace
 
-size_t refine_bytes_per_freq(const TallGeometry& g, int64_t r_pad) {
-    return sizeof(double) * ((size_t)g.m_pad * g.n_pad + 2 * (size_t)g.m_pad + (size_t)(r_pad / kT) * g.m_pad);
+size_t refine_bytes_per_freq(const TallGeometry& g, int64_t r_pad) {  // either Gram path's workspace
+    return std::max(sizeof(double) * ((size_t)g.m_pad * g.n_pad + 2 * (size_t)g.m_pad + (size_t)(r_pad / kT) * g.m_pad),
+                    refine_oz_bytes_per_freq(g, r_pad));
 }
 
 size_t pchol_bytes(int64_t n) {
@@ -436,7 +438,7 @@ int launch_refine_terms(const TallGeometry& ga, int64_t nf, const float* a, cons
     double* part;
     int64_t nkt;
     int launches;
-    if (refine_gram_on_int8()) {  // y^T V y from exact int8 products of digit slices (kernels_gram_oz.cu)
+    if (refine_gram_on_int8(gm.n_pad)) {  // y^T V y from exact int8 products of digit slices (kernels_gram_oz.cu)
         launches = launch_refine_terms_oz(ga, nf, a, gm, xt, dvec, fac.ct_slices, fac.rank, work, err, s, &t12, &part,
                                           &nkt);
     } else {  // on the FP64 tensor pipe (DMMA)
@@ -472,9 +474,9 @@ int launch_refine_chunk(const TallGeometry& g, int64_t nf, float* a, float* linv
            launch_refine_terms(g, nf, a, g, xt, dvec, fac, work, qacc, g.m_pad, err_pivot, s);
 }
 
-bool refine_gram_on_int8() {
+bool refine_gram_on_int8(int64_t n_pad) {
     const char* e = std::getenv("GWB200_REFINE_GRAM");
-    return !(e && std::strcmp(e, "dmma") == 0);
+    return !(e && std::strcmp(e, "dmma") == 0) && gram_oz_fits(n_pad);
 }
 
 } // namespace gwb200

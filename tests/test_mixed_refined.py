@@ -134,7 +134,8 @@ def test_cfg2_refined_against_reference():
         assert err <= FORMS_RTOL, err
 
 
-@pytest.mark.parametrize("nmo,nocc,states,nfreq", [(14, 4, [3, 4], 9), (60, 10, [8, 9, 10, 11], 12)])
+@pytest.mark.parametrize("nmo,nocc,states,nfreq", [
+    (14, 4, [3, 4], 9), (40, 12, [11, 12], 24), (60, 10, [8, 9, 10, 11], 12)])
 def test_refined_gram_int8_matches_dmma(backend, monkeypatch, nmo, nocc, states, nfreq):
     """The correction's y^T V y on the int8 tensor cores (digit slices, the default) against the FP64
     DMMA product (GWB200_REFINE_GRAM=dmma): the same forms to FP64 rounding."""
