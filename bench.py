@@ -631,7 +631,7 @@ def run_b200(args, wl):
             "vs_fp64_dmma_peak": achieved / peak_fp64, "launches": upd_n, "traffic": traffic_oz(wl.name),
             "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum per k_update64_oz launch "
                               "(profiles/k_update64_oz_traffic.json)" if traffic_oz(wl.name) else None}
-    if args.precision == "mixed" and achieved:
+    if args.precision in ("mixed", "mixed-refined") and achieved:
         # the tcgen05 3xTF32 trailing update (k_split_panel32 + k_update32_tc, timed together) is
         # bound by the FP32 C read+write, 8 bytes per updated element per K = 128 pass, i.e.
         # flops_update / 32 bytes (flops = 2 K per element)
@@ -649,9 +649,9 @@ def run_b200(args, wl):
                                           barrier)
         for prec in ("mixed-refined", "mixed"):
             result["mixed"][prec]["ratio_vs_plain"] = result["mixed"][prec]["value"] / value
-    if args.precision == "mixed":
+    if args.precision in ("mixed", "mixed-refined"):
         # error of the mixed form against the plain FP64 form on the same system (untimed)
-        r32 = be.run_g0w0(wl.nfreq, wl.npade, states, precision="mixed")
+        r32 = be.run_g0w0(wl.nfreq, wl.npade, states, precision=args.precision)
         r64 = be.run_g0w0(wl.nfreq, wl.npade, states, precision="fp64")
         import numpy as np
 

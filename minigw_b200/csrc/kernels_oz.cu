@@ -21,22 +21,30 @@
 //                    each slice a 128-byte row in the 128-byte-swizzled K-major layout
 //                    ([slice][row][128 bytes]) the tensor core reads;
 //   k_update64_oz    persistent, warp-specialised, one CTA per SM (10 warps, 222 KB of shared
-//                    memory, 448 TMEM columns):
+//                    memory, 512 TMEM columns):
 //                      warp 0     producer: units from a global counter handed on through a
 //                                 4-slot mbarrier ring; loads the unit's A slices 3-7 (128 rows,
 //                                 80 KB, resident for the unit) and streams the B slices (64
-//                                 rows, 8 KB each) through a 9-stage ring;
+//                                 rows, 8 KB each) through a 13-stage ring;
 //                      warp 1     TMEM allocation; lane 0 issues tcgen05.mma kind::i8 (M = 128,
 //                                 N = 64, K = 32 per instruction; A slices 1-2, which take part
 //                                 in 13 of the 28 products, from TMEM (columns 448-511), the
 //                                 others and B from shared memory) into 7 int32 accumulators,
 //                                 one per level l (columns 64 (l - 2));
 //                      warps 2-9  epilogue: at each unit start, write A slices 1-2 into TMEM;
-//                                 per tile, warp w reads lane quadrant w % 4, 32 columns (all 7
-//                                 levels of 16 columns per tcgen05.wait::ld), releases the
-//                                 accumulators, combines the levels, scales by 2^{e_r + e_c},
-//                                 stages -value per row (256 bytes) and adds it to C with a bulk
-//                                 reduction (cp.reduce.async.bulk .add.f64) per row.
+//                                 per tile, warp w reads lane quadrant w % 4, 32 columns (16
+//                                 columns per tcgen05.wait::ld), combines the levels, scales by
+//                                 2^{e_r + e_c}, stages -value per row (128 bytes per half) and
+//                                 adds it to C with a bulk reduction (cp.reduce.async.bulk
+//                                 .add.f64) per row and half.
+// The accumulators are drained in two level groups so that the tensor core does not wait for the
+// whole drain: per tile the MMAs of group X (levels 4-8, 22 of the 28 products) run first and are
+// committed, then those of group Y (levels 2-3, 6 products).  The epilogue reads group X (keeping
+// S4 2^7 + S5 and the exact low part (S6 2^14 + S7 2^7 + S8) per element) and releases it while
+// group Y runs; the next tile's group X then runs while the epilogue reads group Y and finishes
+// the tile.  (At N = 64 a tcgen05.mma kind::i8 costs ~48 cycles whatever its operands, so these
+// are the tile's 112 instructions back to back; 7 levels x 64 columns leave no room for a second
+// accumulator buffer.)
 // A work unit is (frequency, 128-row tile i, up to kOzSeg column tiles of 64); column tile c of
 // row tile i has work iff c < 2 (i + 1); rows are written from the column tile's first column
 // (the diagonal 64 x 64 blocks in full, as the other update kernels do).  Every mbarrier wait is
@@ -55,7 +63,8 @@ constexpr int kOzM = 128;                    // accumulator rows = TMEM lanes
 constexpr int kOzN = 64;                     // accumulator columns per level
 constexpr int kOzSlices = 7;                 // digit slices per value
 constexpr int kOzSeg = 32;                   // column tiles per work unit
-constexpr int kOzStages = 9;                 // B ring depth (one slice per stage)
+constexpr int kOzStages = 13;                // B ring depth (one slice per stage): a tile's 7, the 2 held
+                                             // for group Y, and 4 ahead
 constexpr int kOzTmemSlices = 2;             // A slices 1-2 (13 of the 28 products) read from TMEM
 constexpr int kSchedSlots = 4;
 constexpr int kSliceA = kOzM * 128;          // one slice of 128 rows: 16 KB
@@ -64,16 +73,16 @@ constexpr int kEpiWarps = 8;                 // 4 lane quadrants x 2 column halv
 constexpr int kOzThreads = 32 * (2 + kEpiWarps);
 constexpr int kTmemCols = 512;               // 7 levels x 64 columns, then A slices 1-2 (32 each)
 constexpr int kTmemA = kOzSlices * kOzN;     // first column of the A slices held in TMEM
-constexpr int kStgRow = 256 + 16;            // staging row stride: 32 doubles + 16 bytes (banks)
+constexpr int kStgRow = 128 + 16;            // staging row stride: 16 doubles + 16 bytes (banks)
 constexpr int kStgBytes = 32 * kStgRow;      // per epilogue warp
 constexpr int kHeader = 1024;
 constexpr int kOzSmem = kHeader + 1024 + (kOzSlices - kOzTmemSlices) * kSliceA + kOzStages * kSliceB + kEpiWarps * kStgBytes;
 
 constexpr int kOffFull = 0;
 constexpr int kOffEmpty = kOffFull + 8 * kOzStages;
-constexpr int kOffTFull = kOffEmpty + 8 * kOzStages;    // accumulators ready (tcgen05.commit)
-constexpr int kOffTEmpty = kOffTFull + 8;               // accumulators drained (kEpiWarps arrivals)
-constexpr int kOffAFull = kOffTEmpty + 8;               // A slices 3-7 of the unit in smem (tx bytes)
+constexpr int kOffTFull = kOffEmpty + 8 * kOzStages;    // level group g (0 = X, 1 = Y) ready (tcgen05.commit)
+constexpr int kOffTEmpty = kOffTFull + 16;              // group g drained (kEpiWarps arrivals)
+constexpr int kOffAFull = kOffTEmpty + 16;              // A slices 3-7 of the unit in smem (tx bytes)
 constexpr int kOffAEmpty = kOffAFull + 8;               // MMAs of the unit complete
 constexpr int kOffATmem = kOffAEmpty + 8;               // A slices 1-2 in TMEM (kEpiWarps arrivals)
 constexpr int kOffDrain = kOffATmem + 8;
@@ -117,6 +126,14 @@ __device__ __forceinline__ void tmem_st32u(uint32_t taddr, const uint32_t (&v)[3
         "r"(v[19]), "r"(v[20]), "r"(v[21]), "r"(v[22]), "r"(v[23]), "r"(v[24]), "r"(v[25]), "r"(v[26]), "r"(v[27]),
         "r"(v[28]), "r"(v[29]), "r"(v[30]), "r"(v[31])
         : "memory");
+}
+
+// 8 consecutive 32-bit accumulator columns of the warp's lane quadrant (no wait).
+__device__ __forceinline__ void tmem_ld8_nowait(uint32_t taddr, uint32_t (&r)[8]) {
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
+                 : "r"(taddr)
+                 : "memory");
 }
 
 __device__ __forceinline__ double pow2(int k) {  // 2^k for -1022 <= k <= 1023, exact
@@ -202,7 +219,8 @@ __global__ void __launch_bounds__(kOzThreads, 1)
     auto empty = [&](int s) { return base + kOffEmpty + 8 * s; };
     auto ufull = [&](int j) { return base + kOffUFull + 8 * j; };
     auto uempty = [&](int j) { return base + kOffUEmpty + 8 * j; };
-    const uint32_t tfull = base + kOffTFull, tempty = base + kOffTEmpty;
+    auto tfull = [&](int g) { return base + kOffTFull + 8 * g; };
+    auto tempty = [&](int g) { return base + kOffTEmpty + 8 * g; };
     const uint32_t afull = base + kOffAFull, aempty = base + kOffAEmpty, drain = base + kOffDrain;
     const uint32_t atmem = base + kOffATmem;
 
@@ -215,8 +233,10 @@ __global__ void __launch_bounds__(kOzThreads, 1)
             mbar_init(ufull(j), 1);
             mbar_init(uempty(j), 1 + kEpiWarps);
         }
-        mbar_init(tfull, 1);
-        mbar_init(tempty, kEpiWarps);
+        for (int g = 0; g < 2; ++g) {
+            mbar_init(tfull(g), 1);
+            mbar_init(tempty(g), kEpiWarps);
+        }
         mbar_init(afull, 1);
         mbar_init(atmem, kEpiWarps);
         mbar_init(aempty, 1);
@@ -334,38 +354,45 @@ __global__ void __launch_bounds__(kOzThreads, 1)
             if (!mbar_wait(atmem, aph, abort_flag, err)) break;
             tc_fence_after();
             aph ^= 1u;
+            // A slice sa+1 against B slice t+1 (in stage st) into level sa + t + 2; the first
+            // product of every level in issue order has t = 0, kk = 0 and starts the accumulator
+            auto pair = [&](int sa, int t, int st) {
+                // descriptors differ from the stage / A bases only in the address field (bytes >>
+                // 4, below 2^14 for shared memory): constant offsets, no carries
+                const uint64_t db0 = desc_b0 + (uint64_t)((uint32_t)(st * kSliceB) >> 4);
+                const uint32_t d = tmem + (uint32_t)((sa + t) * kOzN);
+#pragma unroll
+                for (int kk = 0; kk < 4; ++kk) {
+                    if (sa < kOzTmemSlices)  // A slice from TMEM: 32 bytes of K = 8 columns
+                        mma_i8_ts(d, tmem + (uint32_t)(kTmemA + 32 * sa + 8 * kk), db0 + (uint64_t)(2 * kk),
+                                  (t > 0 || kk > 0) ? 1u : 0u);
+                    else
+                        mma_i8(d, desc_a0 + (uint64_t)(((sa - kOzTmemSlices) * kSliceA + 32 * kk) >> 4),
+                               db0 + (uint64_t)(2 * kk), (t > 0 || kk > 0) ? 1u : 0u);
+                }
+            };
             for (int64_t c = c0; ok && c < c1; ++c) {
-                if (!mbar_wait(tempty, acc_ph ^ 1u, abort_flag, err)) {
+                // group X (levels 4-8, sa + t >= 2) once the epilogue has read the previous tile's
+                if (!mbar_wait(tempty(0), acc_ph ^ 1u, abort_flag, err)) {
                     ok = false;
                     break;
                 }
                 tc_fence_after();
+                int st01[2] = {0, 0};  // stages of B slices 1-2, held for group Y
 #pragma unroll
-                for (int t = 0; t < kOzSlices; ++t) {  // B slice t+1 against A slices 1 .. 7-t
+                for (int t = 0; t < kOzSlices; ++t) {
                     if (!mbar_wait(full(s), ph, abort_flag, err)) {
                         ok = false;
                         break;
                     }
                     tc_fence_after();
-                    // descriptors differ from the stage / A bases only in the address field
-                    // (bytes >> 4, below 2^14 for shared memory): constant offsets, no carries
-                    const uint64_t db0 = desc_b0 + (uint64_t)((uint32_t)(s * kSliceB) >> 4);
 #pragma unroll
-                    for (int sa = 0; sa < kOzSlices; ++sa) {
-                        if (sa < kOzSlices - t) {
-                            const uint32_t d = tmem + (uint32_t)((sa + t) * kOzN);  // level sa + t + 2
-#pragma unroll
-                            for (int kk = 0; kk < 4; ++kk) {
-                                if (sa < kOzTmemSlices)  // A slice from TMEM: 32 bytes of K = 8 columns
-                                    mma_i8_ts(d, tmem + (uint32_t)(kTmemA + 32 * sa + 8 * kk), db0 + (uint64_t)(2 * kk),
-                                              (t > 0 || kk > 0) ? 1u : 0u);
-                                else
-                                    mma_i8(d, desc_a0 + (uint64_t)(((sa - kOzTmemSlices) * kSliceA + 32 * kk) >> 4),
-                                           db0 + (uint64_t)(2 * kk), (t > 0 || kk > 0) ? 1u : 0u);
-                            }
-                        }
-                    }
-                    mma_commit(empty(s));
+                    for (int sa = 0; sa < kOzSlices; ++sa)
+                        if (sa + t >= 2 && sa < kOzSlices - t) pair(sa, t, s);
+                    if (t < 2)
+                        st01[t] = s;
+                    else
+                        mma_commit(empty(s));
                     issued = true;
                     if (++s == kOzStages) {
                         s = 0;
@@ -373,7 +400,19 @@ __global__ void __launch_bounds__(kOzThreads, 1)
                     }
                 }
                 if (!ok) break;
-                mma_commit(tfull);
+                mma_commit(tfull(0));
+                // group Y (levels 2-3) once the epilogue has read the previous tile's
+                if (!mbar_wait(tempty(1), acc_ph ^ 1u, abort_flag, err)) {
+                    ok = false;
+                    break;
+                }
+                tc_fence_after();
+                pair(0, 0, st01[0]);
+                pair(1, 0, st01[0]);
+                pair(0, 1, st01[1]);
+                mma_commit(empty(st01[0]));
+                mma_commit(empty(st01[1]));
+                mma_commit(tfull(1));
                 acc_ph ^= 1u;
             }
             if (!ok) break;
@@ -435,58 +474,83 @@ __global__ void __launch_bounds__(kOzThreads, 1)
                 const int64_t cj = c_begin + c * kOzN + half * 32;  // this warp's first column
                 const bool valid = r < rows && r >= c_begin + c * kOzN;
                 const int ec_lane = exps[c * kOzN + half * 32 + lane];  // exponent of column cj + lane
-                uint32_t got = 1;
-                if (lane == 0) got = mbar_wait(tfull, acc_ph, abort_flag, err) ? 1u : 0u;
-                got = __shfl_sync(0xffffffffu, got, 0);
-                if (!got) {
+                // Levels combined exactly: adjacent pairs in int32 (S_l <= (l-1) 127^2 128, so
+                // S2 2^7 + S3, S4 2^7 + S5, S6 2^7 + S7 < 2^31), then hi = (S2 2^7 + S3) 2^14 +
+                // S4 2^7 + S5 < 2^43 and lo = (S6 2^7 + S7) 2^7 + S8 < 2^39 in int64 (held as an
+                // exact double between the groups); value = hi 2^-35 + lo 2^-56 with one rounding,
+                // scaled by 2^{e_r + e_c}.
+                const uint32_t lanes = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(half * 32);
+                auto wait_group = [&](int g) {
+                    uint32_t got = 1;
+                    if (lane == 0) got = mbar_wait(tfull(g), acc_ph, abort_flag, err) ? 1u : 0u;
+                    got = __shfl_sync(0xffffffffu, got, 0);
+                    if (got) tc_fence_after();
+                    return got != 0u;
+                };
+                auto release_group = [&](int g) {  // the group's levels are in registers
+                    tc_fence_before();
+                    __syncwarp();
+                    if (lane == 0) mbar_arrive(tempty(g));
+                };
+                if (!wait_group(0)) {
+                    ok = false;
+                    break;
+                }
+                // group X leaves m = (S4 2^7 + S5) 2^21 + lo (|m| < 2^51: exact as a double), and
+                // value = p23 2^-21 + m 2^-56 = hi 2^-35 + lo 2^-56, the same sum rounded once
+                double m_d[32];
+#pragma unroll
+                for (int h8 = 0; h8 < 4; ++h8) {  // group X: levels 4-8, 8 columns per wait
+                    uint32_t v[kOzSlices - 2][8];
+#pragma unroll
+                    for (int L = 2; L < kOzSlices; ++L) tmem_ld8_nowait(lanes + (uint32_t)(L * kOzN + 8 * h8), v[L - 2]);
+                    tmem_wait_ld();
+                    if (h8 == 3) release_group(0);
+#pragma unroll
+                    for (int j = 0; j < 8; ++j) {
+                        const int32_t p45 = (int32_t)v[0][j] * 128 + (int32_t)v[1][j];
+                        const int32_t p67 = (int32_t)v[2][j] * 128 + (int32_t)v[3][j];
+                        const long long lo = (long long)p67 * 128 + (int32_t)v[4][j];
+                        m_d[8 * h8 + j] = (double)((long long)p45 * (1LL << 21) + lo);  // exact
+                    }
+                }
+                if (!wait_group(1)) {
                     ok = false;
                     break;
                 }
                 acc_ph ^= 1u;
-                tc_fence_after();
-                // Levels combined exactly: adjacent pairs in int32 (S_l <= (l-1) 127^2 128, so
-                // S2 2^7 + S3, S4 2^7 + S5, S6 2^7 + S7 < 2^31), then hi = (S2 2^7 + S3) 2^14 +
-                // S4 2^7 + S5 < 2^43 and lo = (S6 2^7 + S7) 2^7 + S8 < 2^39 in int64; value =
-                // hi 2^-35 + lo 2^-56 with one rounding, scaled by 2^{e_r + e_c}.
-                double val[32];
 #pragma unroll
-                for (int h16 = 0; h16 < 2; ++h16) {
-                    uint32_t v[kOzSlices][16];
-#pragma unroll
-                    for (int L = 0; L < kOzSlices; ++L)
-                        tmem_ld16_nowait(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(L * kOzN + half * 32 + 16 * h16), v[L]);
+                for (int h16 = 0; h16 < 2; ++h16) {  // group Y: levels 2-3, then the half's 16 columns to C
+                    uint32_t v[2][16];
+                    tmem_ld16_nowait(lanes + (uint32_t)(16 * h16), v[0]);
+                    tmem_ld16_nowait(lanes + (uint32_t)(kOzN + 16 * h16), v[1]);
                     tmem_wait_ld();
-                    if (h16 == 1) {  // every level is in registers: the accumulators are free
-                        tc_fence_before();
-                        __syncwarp();
-                        if (lane == 0) mbar_arrive(tempty);
-                    }
+                    if (h16 == 1) release_group(1);
+                    double val[16];
 #pragma unroll
                     for (int j = 0; j < 16; ++j) {
                         const int32_t p23 = (int32_t)v[0][j] * 128 + (int32_t)v[1][j];
-                        const int32_t p45 = (int32_t)v[2][j] * 128 + (int32_t)v[3][j];
-                        const int32_t p67 = (int32_t)v[4][j] * 128 + (int32_t)v[5][j];
-                        const long long hi = (long long)p23 * (1LL << 14) + p45;
-                        const long long lo = (long long)p67 * 128 + (int32_t)v[6][j];
                         const int ej = __shfl_sync(0xffffffffu, ec_lane, 16 * h16 + j);
-                        val[16 * h16 + j] = -fma((double)hi, 0x1p-35, (double)lo * 0x1p-56) * pow2(er + ej);
+                        val[j] = -fma((double)p23, 0x1p-21, m_d[16 * h16 + j] * 0x1p-56) * pow2(er + ej);
                     }
-                }
-                if (valid) {  // stage the row (256 bytes), then one bulk reduction
-                    if (reduced) asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
+                    if (valid) {  // stage the half row (128 bytes), then one bulk reduction
+                        if (reduced) asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
 #pragma unroll
-                    for (int j = 0; j < 32; j += 2)
-                        asm volatile("st.shared.v2.f64 [%0], {%1, %2};" ::"r"(stg + 8u * j), "d"(val[j]), "d"(val[j + 1])
+                        for (int j = 0; j < 16; j += 2)
+                            asm volatile("st.shared.v2.f64 [%0], {%1, %2};" ::"r"(stg + 8u * j), "d"(val[j]),
+                                         "d"(val[j + 1])
+                                         : "memory");
+                    }
+                    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                    if (valid) {
+                        double* dst = a + (size_t)f * stride + (size_t)r * ld + cj + 16 * h16;
+                        asm volatile("cp.reduce.async.bulk.global.shared::cta.bulk_group.add.f64 [%0], [%1], 128;" ::"l"(
+                                         dst),
+                                     "r"(stg)
                                      : "memory");
-                }
-                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-                if (valid) {
-                    double* dst = a + (size_t)f * stride + (size_t)r * ld + cj;
-                    asm volatile("cp.reduce.async.bulk.global.shared::cta.bulk_group.add.f64 [%0], [%1], 256;" ::"l"(dst),
-                                 "r"(stg)
-                                 : "memory");
-                    asm volatile("cp.async.bulk.commit_group;" ::: "memory");
-                    reduced = true;
+                        asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+                        reduced = true;
+                    }
                 }
             }
         }
