@@ -201,7 +201,7 @@ int launch_refine_chunk(const TallGeometry& g, int64_t nf, float* a, float* linv
 bool refine_gram_on_int8(int64_t n_pad);
 // kernels_gram_oz.cu: y^T V y = ||C^T y||^2 from int8 digit slices (tcgen05 kind::i8).
 int64_t gram_oz_rows(int64_t r);
-// the int8 path's int32 accumulators hold the exact sums for n_pad up to 65536; beyond, DMMA
+// the int8 path (exact int32 sums, y of a right-hand side in shared memory) takes n_pad up to 25600; beyond, DMMA
 bool gram_oz_fits(int64_t n_pad);
 size_t refine_oz_bytes_per_freq(const TallGeometry& g, int64_t r);
 size_t gram_oz_system_bytes(int64_t n_pad, int64_t r);

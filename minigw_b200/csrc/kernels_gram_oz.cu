@@ -129,7 +129,10 @@ __global__ void __launch_bounds__(256) k_slice_ct(const double* __restrict__ ct,
 // One CTA per right-hand side j of one frequency (k_refine_prep's inputs): y_j = dvec * z_j in FP64,
 // rounded to kBSl balanced digits below its row scale; the digits into B slices [kc][t][j][128 B] of
 // the frequency, the exponent into yexp; t1 = x_j . y^ and t2 = z^ . z^ (z^ = y^ / dvec) from the
-// rounded values (fixed-order sums).
+// rounded values (fixed-order sums).  The grid's x index is the frequency, so that the CTAs in flight
+// together share j and its row of xt (read from DRAM once, not once per frequency).
+constexpr int64_t kPrepMaxNpad = 25600;  // y staged in shared memory: 8 n_pad bytes <= 200 KB
+
 __global__ void __launch_bounds__(256) k_refine_prep_oz(const float* __restrict__ a, int64_t ld, int64_t stride,
                                                         int64_t row0, int64_t na, int64_t n, int64_t n_pad, int64_t nk,
                                                         int64_t m, int64_t m_pad, const double* __restrict__ xt,
@@ -138,8 +141,8 @@ __global__ void __launch_bounds__(256) k_refine_prep_oz(const float* __restrict_
                                                         double* __restrict__ t12) {
     extern __shared__ double yrow[];  // n_pad
     __shared__ double r1[256], r2[256], rm[256];
-    const int f = blockIdx.y;
-    const int64_t j = blockIdx.x;
+    const int f = blockIdx.x;
+    const int64_t j = blockIdx.y;
     const float* row = a + (size_t)f * stride + (size_t)(row0 + j) * ld;
     const double* d = dvec + (size_t)f * n_pad;
     const bool live = j < m;
@@ -399,7 +402,7 @@ __global__ void __launch_bounds__(kGramThreads, 1)
 
 int64_t gram_oz_rows(int64_t r) { return std::max<int64_t>(kGM, round_up(r, kGM)); }
 
-bool gram_oz_fits(int64_t n_pad) { return round_up(n_pad, kKc) <= kMaxNk; }
+bool gram_oz_fits(int64_t n_pad) { return round_up(n_pad, kKc) <= kMaxNk && n_pad <= kPrepMaxNpad; }
 
 size_t gram_oz_system_bytes(int64_t n_pad, int64_t r) {
     const int64_t r128 = gram_oz_rows(r), nk = round_up(n_pad, kKc);
@@ -426,7 +429,8 @@ int launch_refine_terms_oz(const TallGeometry& ga, int64_t nf, const float* a, c
     double* part = t12 + (size_t)nf * 2 * m_pad;
     const size_t prep_smem = sizeof(double) * (size_t)n_pad;
     GWB_CUDA(cudaFuncSetAttribute(k_refine_prep_oz, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)prep_smem));
-    k_refine_prep_oz<<<dim3((unsigned)m_pad, (unsigned)nf), 256, prep_smem, s>>>(
+    if (m_pad > 65535) fail(GWB200_BAD_SHAPE, "refined form: more than 65535 right-hand sides per frequency");
+    k_refine_prep_oz<<<dim3((unsigned)nf, (unsigned)m_pad), 256, prep_smem, s>>>(
         a, ga.ld, ga.stride, ga.n_pad, gm.n_pad, gm.n, n_pad, nk, gm.m, m_pad, xt, dvec, ysl, fbytes, yexp, t12);
     GWB_LAUNCH("k_refine_prep_oz");
     const uint8_t* asl = static_cast<const uint8_t*>(ct_slices);
