@@ -531,7 +531,10 @@ __global__ void __launch_bounds__(kOzThreads, 1)
                     for (int j = 0; j < 16; ++j) {
                         const int32_t p23 = (int32_t)v[0][j] * 128 + (int32_t)v[1][j];
                         const int ej = __shfl_sync(0xffffffffu, ec_lane, 16 * h16 + j);
-                        val[j] = -fma((double)p23, 0x1p-21, m_d[16 * h16 + j] * 0x1p-56) * pow2(er + ej);
+                        // (p23 2^35 + m) rounded once is 2^56 times the value rounded once: the
+                        // 2^-56 joins the exact power-of-two scale (one FP64 multiply less; the
+                        // epilogue's FP64 work is on this kernel's critical path)
+                        val[j] = -fma((double)p23, 0x1p35, m_d[16 * h16 + j]) * pow2(er + ej - 56);
                     }
                     if (valid) {  // stage the half row (128 bytes), then one bulk reduction
                         if (reduced) asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
