@@ -128,14 +128,6 @@ __device__ __forceinline__ void tmem_st32u(uint32_t taddr, const uint32_t (&v)[3
         : "memory");
 }
 
-// 8 consecutive 32-bit accumulator columns of the warp's lane quadrant (no wait).
-__device__ __forceinline__ void tmem_ld8_nowait(uint32_t taddr, uint32_t (&r)[8]) {
-    asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
-                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
-                 : "r"(taddr)
-                 : "memory");
-}
-
 __device__ __forceinline__ double pow2(int k) {  // 2^k for -1022 <= k <= 1023, exact
     return __longlong_as_double((long long)(k + 1023) << 52);
 }
@@ -500,18 +492,18 @@ __global__ void __launch_bounds__(kOzThreads, 1)
                 // value = p23 2^-21 + m 2^-56 = hi 2^-35 + lo 2^-56, the same sum rounded once
                 double m_d[32];
 #pragma unroll
-                for (int h8 = 0; h8 < 4; ++h8) {  // group X: levels 4-8, 8 columns per wait
-                    uint32_t v[kOzSlices - 2][8];
+                for (int h16 = 0; h16 < 2; ++h16) {  // group X: levels 4-8, 16 columns per wait
+                    uint32_t v[kOzSlices - 2][16];
 #pragma unroll
-                    for (int L = 2; L < kOzSlices; ++L) tmem_ld8_nowait(lanes + (uint32_t)(L * kOzN + 8 * h8), v[L - 2]);
+                    for (int L = 2; L < kOzSlices; ++L) tmem_ld16_nowait(lanes + (uint32_t)(L * kOzN + 16 * h16), v[L - 2]);
                     tmem_wait_ld();
-                    if (h8 == 3) release_group(0);
+                    if (h16 == 1) release_group(0);
 #pragma unroll
-                    for (int j = 0; j < 8; ++j) {
+                    for (int j = 0; j < 16; ++j) {
                         const int32_t p45 = (int32_t)v[0][j] * 128 + (int32_t)v[1][j];
                         const int32_t p67 = (int32_t)v[2][j] * 128 + (int32_t)v[3][j];
                         const long long lo = (long long)p67 * 128 + (int32_t)v[4][j];
-                        m_d[8 * h8 + j] = (double)((long long)p45 * (1LL << 21) + lo);  // exact
+                        m_d[16 * h16 + j] = (double)((long long)p45 * (1LL << 21) + lo);  // exact
                     }
                 }
                 if (!wait_group(1)) {
