@@ -301,13 +301,13 @@ __global__ void __launch_bounds__(kGramThreads, 1)
             for (int64_t kc = 0; ok && kc < nkc; ++kc) {
                 const int b = (int)(kc & 1);
                 const uint32_t pb = (uint32_t)((kc >> 1) & 1);
-                if (!mbar_wait(bf(b), pb, abort_flag, err)) {
+                if (!mbar_wait_fast(bf(b), pb, abort_flag, err)) {
                     ok = false;
                     break;
                 }
                 tc_fence_after();
                 for (int s = 0; s < kASl; ++s) {  // A slice s+1 against B slices 1 .. min(kBSl, kLevels - s)
-                    if (!mbar_wait(af(sa), pa, abort_flag, err)) {
+                    if (!mbar_wait_fast(af(sa), pa, abort_flag, err)) {
                         ok = false;
                         break;
                     }

@@ -331,14 +331,14 @@ __global__ void __launch_bounds__(kTcThreads, 1)
             tc_fence_after();
             aph ^= 1u;
             for (int64_t c = c0; ok && c < c1; ++c) {
-                if (!mbar_wait(tempty(ab), acc_ph ^ 1u, abort_flag, err)) {
+                if (!mbar_wait_fast(tempty(ab), acc_ph ^ 1u, abort_flag, err)) {
                     ok = false;
                     break;
                 }
                 tc_fence_after();
                 const uint32_t d = tmem + (uint32_t)(ab * kTcN);
                 for (int kb = 0; kb < nkc; ++kb) {
-                    if (!mbar_wait(full(s), ph, abort_flag, err)) {
+                    if (!mbar_wait_fast(full(s), ph, abort_flag, err)) {
                         ok = false;
                         break;
                     }

@@ -56,6 +56,12 @@ static __device__ __noinline__ bool mbar_wait(uint32_t bar, uint32_t parity, vol
         }
     }
 }
+// mbar_wait with its first poll inlined: for the MMA-issuing thread, where a phase that is already
+// complete should cost no call (a poll between tcgen05.mma instructions stalls their issue).
+__device__ __forceinline__ bool mbar_wait_fast(uint32_t bar, uint32_t parity, volatile uint32_t* abort_flag,
+                                               unsigned long long* err) {
+    return mbar_try(bar, parity) || mbar_wait(bar, parity, abort_flag, err);
+}
 // Bounded wait used only while draining: no abort check, no error record.
 __device__ __forceinline__ void mbar_drain(uint32_t bar, uint32_t parity) {
     if (mbar_try(bar, parity)) return;
