@@ -140,9 +140,10 @@ __global__ void __launch_bounds__(256) k_refine_prep_oz(const float* __restrict_
                                                         size_t fbytes, int32_t* __restrict__ yexp,
                                                         double* __restrict__ t12) {
     extern __shared__ double yrow[];  // n_pad
-    __shared__ double r1[256], r2[256], rm[256];
+    __shared__ double r1[8], r2[8], rm[8];  // one value per warp
     const int f = blockIdx.x;
     const int64_t j = blockIdx.y;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const float* row = a + (size_t)f * stride + (size_t)(row0 + j) * ld;
     const double* d = dvec + (size_t)f * n_pad;
     const bool live = j < m;
@@ -152,12 +153,17 @@ __global__ void __launch_bounds__(256) k_refine_prep_oz(const float* __restrict_
         yrow[i] = yi;
         mx = fmax(mx, fabs(yi));
     }
-    rm[threadIdx.x] = mx;
+    // block maximum: shuffle tree per warp, then the 8 warp values (two barriers)
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    if (lane == 0) rm[warp] = mx;
     __syncthreads();
-    for (int w = 128; w > 0; w >>= 1) {
-        if ((int)threadIdx.x < w) rm[threadIdx.x] = fmax(rm[threadIdx.x], rm[threadIdx.x + w]);
-        __syncthreads();
+    if (threadIdx.x == 0) {
+        double v = rm[0];
+        for (int w = 1; w < 8; ++w) v = fmax(v, rm[w]);
+        rm[0] = v;
     }
+    __syncthreads();
     int e = 0;
     if (rm[0] > 0.0) frexp(rm[0], &e);
     ++e;  // |y| < 2^{e-1}
@@ -190,19 +196,25 @@ __global__ void __launch_bounds__(256) k_refine_prep_oz(const float* __restrict_
         for (int t = 0; t < kBSl; ++t)
             *reinterpret_cast<uint32_t*>(out + ((size_t)(kc * kBSl + t) * m_pad) * kKc + swz(j, kb)) = word[t];
     }
-    r1[threadIdx.x] = s1;
-    r2[threadIdx.x] = s2;
-    __syncthreads();
-    for (int w = 128; w > 0; w >>= 1) {
-        if ((int)threadIdx.x < w) {
-            r1[threadIdx.x] += r1[threadIdx.x + w];
-            r2[threadIdx.x] += r2[threadIdx.x + w];
-        }
-        __syncthreads();
+    // block sums in a fixed order: shuffle tree per warp, then the 8 warp sums in warp order
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        s1 += __shfl_xor_sync(0xffffffffu, s1, o);
+        s2 += __shfl_xor_sync(0xffffffffu, s2, o);
     }
+    if (lane == 0) {
+        r1[warp] = s1;
+        r2[warp] = s2;
+    }
+    __syncthreads();
     if (threadIdx.x == 0) {
-        t12[((size_t)f * m_pad + j) * 2] = r1[0];
-        t12[((size_t)f * m_pad + j) * 2 + 1] = r2[0];
+        double u1 = r1[0], u2 = r2[0];
+        for (int w = 1; w < 8; ++w) {
+            u1 += r1[w];
+            u2 += r2[w];
+        }
+        t12[((size_t)f * m_pad + j) * 2] = u1;
+        t12[((size_t)f * m_pad + j) * 2 + 1] = u2;
         yexp[(size_t)f * m_pad + j] = e;
     }
 }
