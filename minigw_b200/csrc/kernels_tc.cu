@@ -31,7 +31,7 @@
 //                                 128-byte lines; the read-modify-write happens in L2);
 //                      warps 10-17 A loaders: fill the unit's A into TMEM (tcgen05.st) as soon as
 //                                 the previous unit's MMAs release it.
-// A work unit is (frequency, 128-row tile i, up to 16 column tiles of 128); column tile c of row
+// A work unit is (frequency, 128-row tile i, up to 48 column tiles of 128); column tile c of row
 // tile i has work iff c <= i, and units of the longest row tiles are handed out first.  Writes are
 // limited to the lower part at 64-column-block granularity (the diagonal 64 x 64 blocks in full,
 // as the other update kernels do).
@@ -57,7 +57,9 @@ constexpr int kTcM = 128;                   // accumulator rows = TMEM lanes = A
 constexpr int kTcN = 128;                   // accumulator columns per tile
 constexpr int kTcKc = 32;                   // floats of K per B pipeline stage
 constexpr int kTcStages = 6;                // B ring depth
-constexpr int kTcSeg = 16;                  // column tiles per work unit (A is loaded once per unit)
+constexpr int kTcSeg = 48;                  // column tiles per work unit (A is loaded once per unit, and
+                                            // the MMAs wait for it: 16 -> 48 took config 3's mixed
+                                            // solve from 127.8 to 124.2 ms)
 constexpr int kSchedSlots = 4;              // unit-index ring from the producer to the other roles
 constexpr int kRowBytes = kTcKc * 4;        // one row of a K slice: 128 bytes = one swizzle atom row
 constexpr int kSliceB = kTcN * kRowBytes;   // 16384 bytes
