@@ -134,6 +134,47 @@ def test_cfg2_refined_against_reference():
         assert err <= FORMS_RTOL, err
 
 
+def test_cfg2_chain_against_reference_forms():
+    """Config 2 (nmo=120, nph=2000, six states, 64 frequencies), whole chain: the reference's own
+    screened forms at every frequency (oracle/_ref, blas-lapack backend), contracted, continued and
+    solved by the oracle (Sigma_c(iw), the E_c Pade sweep, QP), against each form of this library.
+    Sigma_c within 1e-10 Ha for the plain and the refined forms (the unrefined mixed form at the
+    FP32 level); the E_c and QP differences are printed (QP on the synthetic generator is set by
+    its Pade conditioning: tests/test_oracle.py::test_pade_qp_sensitivity_synthetic_vs_h2o)."""
+    import oracle
+    from minigw_b200 import B200Backend, generate_transformed_legendre_grid
+    from minigw_b200.synthetic import WORKLOADS, make_workload_input
+
+    if not oracle.Ref.available:
+        pytest.skip("the reference's own code (oracle/_ref) is not built")
+    wl = WORKLOADS["cfg2"]
+    inp = make_workload_input(wl, seed=0)
+    om, w = generate_transformed_legendre_grid(wl.nfreq)
+    states = list(wl.states)
+    rq = oracle.Ref(blas_threads=os.cpu_count()).forms(inp, om, states, backend="blas-lapack")
+    o = oracle.Oracle()
+    ref_sig = o.sigma_from_forms(inp, om, w, states, rq)
+    ref_qp = o.qp(inp, np.diag(o.exchange(inp)).copy(), om, ref_sig, states, wl.npade)
+    npts = 2000
+    ref_ec = [o.ec_sweep(om, ref_sig[s], wl.npade, npts, inp.fermi_energy) for s in states]
+    report = {}
+    with B200Backend(0) as be:
+        be.load_system(inp, states)
+        for prec in ("fp64", "mixed-refined", "mixed"):
+            r = be.run_g0w0(wl.nfreq, wl.npade, states, precision=prec)
+            dsig = float(np.abs(r["sigma"][states] - ref_sig[states]).max())
+            dec = max(float(np.abs(be.pade_sweep(om, r["sigma"][s], wl.npade, npts=npts) - e).max())
+                      for s, e in zip(states, ref_ec))
+            dqp = np.abs(r["qp"][states] - ref_qp[states]) * HA_EV * 1e3
+            report[prec] = (dsig, dec, float(dqp.max()), float(np.median(dqp)))
+    for prec, (dsig, dec, dqp, dqp_med) in report.items():
+        print(f"cfg2 {prec}: |dSigma_c| {dsig:.2e} Ha, |dE_c sweep| {dec:.2e}, QP max {dqp:.3g} meV "
+              f"(median {dqp_med:.3g})")
+    assert report["fp64"][0] <= SIGMA_ATOL
+    assert report["mixed-refined"][0] <= SIGMA_ATOL
+    assert report["mixed"][0] > 100 * report["mixed-refined"][0]  # FP32 level without the correction
+
+
 @pytest.mark.parametrize("nmo,nocc,states,nfreq", [
     (14, 4, [3, 4], 9), (40, 12, [11, 12], 24), (60, 10, [8, 9, 10, 11], 12)])
 def test_refined_gram_int8_matches_dmma(backend, monkeypatch, nmo, nocc, states, nfreq):
