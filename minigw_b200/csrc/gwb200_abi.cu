@@ -1456,6 +1456,15 @@ int gwb200_run_g0w0_batch(gwb200_handle* const* systems, int64_t nsys, const int
         }
         for (int l = 0; l < lanes; ++l) {
             BatchLane& ln = w->lanes[l];
+            // batch_avail counted everything the lane holds as free: when a buffer must grow, or the
+            // lane holds one this call does not use (the correction terms of an earlier refined
+            // batch, the operand panel of another form), free them all before allocating, so the
+            // new sizes fit the budget they were planned in
+            const bool grow = need.a > ln.a.bytes || need.linv > ln.linv.bytes || need.qacc > ln.qacc.bytes ||
+                              need.panel > ln.panel.bytes || need.refine > ln.refine.bytes;
+            const bool unused = (!need.panel && ln.panel.bytes) || (!need.refine && ln.refine.bytes);
+            if (grow || unused)
+                for (DevBuf* b : {&ln.a, &ln.linv, &ln.qacc, &ln.panel, &ln.refine}) b->release();
             size_buffer(w, ln.a, need.a);
             size_buffer(w, ln.linv, need.linv);
             size_buffer(w, ln.qacc, need.qacc);

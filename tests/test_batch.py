@@ -326,3 +326,27 @@ def test_refined_batch_against_oracle(oracle_lib):
     for inp, st, s in zip(inputs, states, got["sigma"]):
         ref, _ = oracle_lib.sigma_c(inp, om, w, st)
         assert np.abs(s - ref).max() <= 1e-10
+
+
+@pytest.mark.gpu
+def test_batches_of_different_forms_on_the_same_handles():
+    """Refined, plain and mixed batches in turn on the same member handles: the lead handle's lane
+    workspaces are re-planned for each form (buffers one form does not use are freed before the
+    next form's are allocated), and each batch stays bit-identical to the molecules' own solves."""
+    from minigw_b200 import B200Backend, run_g0w0_batch
+
+    inputs = _systems([(16, 3), (26, 4), (40, 7)], seed0=1500)
+    states = [_states(inp) for inp in inputs]
+    bes = [B200Backend(0) for _ in inputs]
+    try:
+        for be, inp, st in zip(bes, inputs, states):
+            be.load_system(inp, st)
+        for prec in ("mixed-refined", "fp64", "mixed", "mixed-refined", "fp64"):
+            alone = [be.run_g0w0(16, 8, st, precision=prec) for be, st in zip(bes, states)]
+            got = run_g0w0_batch(bes, 16, 8, states, precision=prec)
+            for a, s, q, st in zip(alone, got["sigma"], got["qp"], states):
+                np.testing.assert_array_equal(s, a["sigma"])
+                np.testing.assert_array_equal(q[st], a["qp"][st])
+    finally:
+        for be in bes:
+            be.close()
