@@ -132,15 +132,16 @@ __global__ void __launch_bounds__(256) k_slice_ct(const double* __restrict__ ct,
 // rounded values (fixed-order sums).  The grid's x index is the frequency, so that the CTAs in flight
 // together share j and its row of xt (read from DRAM once, not once per frequency).
 constexpr int64_t kPrepMaxNpad = 25600;  // y staged in shared memory: 8 n_pad bytes <= 200 KB
+constexpr int kPrepThreads = 256;        // 8 warps: the block reductions keep one value per warp
 
-__global__ void __launch_bounds__(256) k_refine_prep_oz(const float* __restrict__ a, int64_t ld, int64_t stride,
+__global__ void __launch_bounds__(kPrepThreads) k_refine_prep_oz(const float* __restrict__ a, int64_t ld, int64_t stride,
                                                         int64_t row0, int64_t na, int64_t n, int64_t n_pad, int64_t nk,
                                                         int64_t m, int64_t m_pad, const double* __restrict__ xt,
                                                         const double* __restrict__ dvec, uint8_t* __restrict__ yslices,
                                                         size_t fbytes, int32_t* __restrict__ yexp,
                                                         double* __restrict__ t12) {
     extern __shared__ double yrow[];  // n_pad
-    __shared__ double r1[8], r2[8], rm[8];  // one value per warp
+    __shared__ double r1[kPrepThreads / 32], r2[kPrepThreads / 32], rm[kPrepThreads / 32];  // one value per warp
     const int f = blockIdx.x;
     const int64_t j = blockIdx.y;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -160,7 +161,7 @@ __global__ void __launch_bounds__(256) k_refine_prep_oz(const float* __restrict_
     __syncthreads();
     if (threadIdx.x == 0) {
         double v = rm[0];
-        for (int w = 1; w < 8; ++w) v = fmax(v, rm[w]);
+        for (int w = 1; w < kPrepThreads / 32; ++w) v = fmax(v, rm[w]);
         rm[0] = v;
     }
     __syncthreads();
@@ -209,7 +210,7 @@ __global__ void __launch_bounds__(256) k_refine_prep_oz(const float* __restrict_
     __syncthreads();
     if (threadIdx.x == 0) {
         double u1 = r1[0], u2 = r2[0];
-        for (int w = 1; w < 8; ++w) {
+        for (int w = 1; w < kPrepThreads / 32; ++w) {
             u1 += r1[w];
             u2 += r2[w];
         }
@@ -442,7 +443,7 @@ int launch_refine_terms_oz(const TallGeometry& ga, int64_t nf, const float* a, c
     const size_t prep_smem = sizeof(double) * (size_t)n_pad;
     GWB_CUDA(cudaFuncSetAttribute(k_refine_prep_oz, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)prep_smem));
     if (m_pad > 65535) fail(GWB200_BAD_SHAPE, "refined form: more than 65535 right-hand sides per frequency");
-    k_refine_prep_oz<<<dim3((unsigned)nf, (unsigned)m_pad), 256, prep_smem, s>>>(
+    k_refine_prep_oz<<<dim3((unsigned)nf, (unsigned)m_pad), kPrepThreads, prep_smem, s>>>(
         a, ga.ld, ga.stride, ga.n_pad, gm.n_pad, gm.n, n_pad, nk, gm.m, m_pad, xt, dvec, ysl, fbytes, yexp, t12);
     GWB_LAUNCH("k_refine_prep_oz");
     const uint8_t* asl = static_cast<const uint8_t*>(ct_slices);

@@ -365,7 +365,7 @@ __global__ void __launch_bounds__(kOzThreads, 1)
             };
             for (int64_t c = c0; ok && c < c1; ++c) {
                 // group X (levels 4-8, sa + t >= 2) once the epilogue has read the previous tile's
-                if (!mbar_try(tempty(0), acc_ph ^ 1u) && !mbar_wait(tempty(0), acc_ph ^ 1u, abort_flag, err)) {
+                if (!mbar_wait_fast(tempty(0), acc_ph ^ 1u, abort_flag, err)) {
                     ok = false;
                     break;
                 }
@@ -373,7 +373,7 @@ __global__ void __launch_bounds__(kOzThreads, 1)
                 int st01[2] = {0, 0};  // stages of B slices 1-2, held for group Y
 #pragma unroll
                 for (int t = 0; t < kOzSlices; ++t) {
-                    if (!mbar_try(full(s), ph) && !mbar_wait(full(s), ph, abort_flag, err)) {
+                    if (!mbar_wait_fast(full(s), ph, abort_flag, err)) {
                         ok = false;
                         break;
                     }
@@ -394,7 +394,7 @@ __global__ void __launch_bounds__(kOzThreads, 1)
                 if (!ok) break;
                 mma_commit(tfull(0));
                 // group Y (levels 2-3) once the epilogue has read the previous tile's
-                if (!mbar_try(tempty(1), acc_ph ^ 1u) && !mbar_wait(tempty(1), acc_ph ^ 1u, abort_flag, err)) {
+                if (!mbar_wait_fast(tempty(1), acc_ph ^ 1u, abort_flag, err)) {
                     ok = false;
                     break;
                 }
