@@ -148,6 +148,16 @@ int gwb200_sigma_c(gwb200_handle* h, const double* omega, const double* weight, 
                    const int64_t* states, int64_t nstates, double eta, int precision,
                    double* sigma_out, gwb200_stats* stats);
 
+/* Correlation self-energy between the requested states, Sigma_c(p_s, p_t; i w_n), plain FP64 form,
+ * eta = 0, 1 <= nstates <= 64: sigma_out is nstates x nstates x nfreq complex (element (s, t, n) at
+ * 2 * ((s * nstates + t) * nfreq + n)), symmetric in (s, t); its diagonal is gwb200_sigma_c's rows
+ * of the states to rounding.  The cross forms x_{p_s k}^T W_c x_{p_t k} come from the solved
+ * right-hand-side rows of the same factorisation, and the frequency contraction is the diagonal's.
+ * No counterpart in the reference: it computes the diagonal only (docs/formulation.md:186); this
+ * is the data an off-diagonal QP Hamiltonian would start from. */
+int gwb200_sigma_c_matrix(gwb200_handle* h, const double* omega, const double* weight, int64_t nfreq,
+                          const int64_t* states, int64_t nstates, double* sigma_out, gwb200_stats* stats);
+
 /* The contribution of the integration frequencies f' in [f_begin, f_end) of the grid to Sigma_c at
  * every output frequency of the grid: sigma_partial_out is nmo x nfreq complex.  The partial sums of
  * a partition of [0, nfreq) add up to gwb200_sigma_c's result (up to summation order); ranks that

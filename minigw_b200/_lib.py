@@ -41,7 +41,7 @@ EXPORTS = (
     "gwb200_grid", "gwb200_read_input_h5", "gwb200_screened_forms_noalloc", "gwb200_fp64_peak_tflops",
     "gwb200_update_kernel", "gwb200_run_g0w0_batch", "gwb200_plan_buckets", "gwb200_read_resident",
     "gwb200_kernel_profile", "gwb200_load_system_slices", "gwb200_server_submit_slices", "gwb200_server_set_merge",
-    "gwb200_server_counters",
+    "gwb200_server_counters", "gwb200_sigma_c_matrix",
 )
 
 
@@ -116,6 +116,7 @@ def _load() -> C.CDLL:
     lib.gwb200_load_system_states.argtypes = [_vp, C.c_int64, C.c_int64, _dp, _dp, _dp, C.c_double, _ip, C.c_int64]
     lib.gwb200_sigma_c.argtypes = [_vp, _dp, _dp, C.c_int64, _ip, C.c_int64, C.c_double, C.c_int, _dp,
                                    C.POINTER(Stats)]
+    lib.gwb200_sigma_c_matrix.argtypes = [_vp, _dp, _dp, C.c_int64, _ip, C.c_int64, _dp, C.POINTER(Stats)]
     lib.gwb200_sigma_c_shard.argtypes = [_vp, _dp, _dp, C.c_int64, C.c_int64, C.c_int64, _ip, C.c_int64, C.c_double,
                                          C.c_int, _dp, C.POINTER(Stats)]
     lib.gwb200_run_g0w0.argtypes = [_vp, C.c_int64, C.c_int64, _ip, C.c_int64, C.c_double, C.c_int, _dp, _dp, _dp,

@@ -24,7 +24,7 @@ GW_BIN = PKG / "bin" / "gw"
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 CU_SOURCES = ["kernels_fp64.cu", "kernels_f32.cu", "kernels_tc.cu", "kernels_oz.cu", "kernels_c64.cu",
-              "kernels_small.cu", "kernels_batch.cu", "kernels_refine.cu", "kernels_gram_oz.cu", "gwb200_abi.cu", "noalloc.cu"]
+              "kernels_small.cu", "kernels_batch.cu", "kernels_refine.cu", "kernels_gram_oz.cu", "kernels_offdiag.cu", "gwb200_abi.cu", "noalloc.cu"]
 CXX_SOURCES = ["host_grid.cpp", "host_h5.cpp", "server.cpp"]
 CLI_SOURCES = ["gw_main.cpp"]
 

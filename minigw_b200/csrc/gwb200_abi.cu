@@ -6,6 +6,7 @@
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
+#include <functional>
 #include <limits>
 #include <map>
 #include <mutex>
@@ -134,6 +135,7 @@ struct gwb200_handle {
     // GWB200_MIXED_REFINED: pivoted Cholesky factor of the resident V_ph (computed on first use after
     // a load; pchol_rank < 0: not yet) and the per-chunk refinement workspace
     DevBuf pchol, pchol_sl, refine;  // pchol_sl: the factor's int8 digit slices
+    DevBuf qx, sigmx;                // gwb200_sigma_c_matrix: cross forms, Sigma_c between the states
     int64_t pchol_rank = -1;
     double* pchol_ct = nullptr;
     DevBuf batch_desc;  // BatchGroup tables of gwb200_run_g0w0_batch (when this handle leads a batch)
@@ -276,8 +278,13 @@ float elapsed(cudaEvent_t a, cudaEvent_t b) {
 
 // Screened quadratic forms for all requested frequencies into h->qall ([nfreq][m] doubles,
 // x^T W_c x <= 0).  Records ev[0] (start), ev[1] (after gather), ev[2] (after screening).
+// after_factor (plain form only): called on the stream after each frequency chunk [f0, f0 + nf) is
+// factored, while h->a holds its tall matrices (the solved right-hand-side rows in their lower block).
+using ChunkHook = std::function<void(const TallGeometry& g, int64_t f0, int64_t nf)>;
+
 void compute_forms(gwb200_handle* h, const double* omega, int64_t nfreq, const int64_t* states, int64_t nstates,
-                   double eta, int precision, gwb200_stats* st, const double* weight = nullptr) {
+                   double eta, int precision, gwb200_stats* st, const double* weight = nullptr,
+                   const ChunkHook* after_factor = nullptr) {
     if (!omega) fail(GWB200_BAD_ARGUMENT, "null omega");
     if (nfreq <= 0) fail(GWB200_BAD_SHAPE, "--freq-points must be positive");
     check_states(h, states, nstates);
@@ -446,6 +453,10 @@ void compute_forms(gwb200_handle* h, const double* omega, int64_t nfreq, const i
                                             h->err.as<unsigned long long>(), s, prof.enabled ? &prof : nullptr,
                                             upd_variant, fp64_oz ? h->panel32.p : nullptr,
                                             h->tc_sched.as<unsigned long long>(), h->persistent_ctas);
+            if (after_factor) {
+                (*after_factor)(g, f0, nf);
+                ++launches;
+            }
         }
         launches += launch_negate_copy(h->qacc.as<double>(), nf, m, g.m_pad, h->qall.as<double>() + f0 * g.m_pad,
                                        g.m_pad, s);
@@ -740,7 +751,7 @@ int gwb200_destroy(gwb200_handle* h) {
     h->stage_out.release();
     for (DevBuf* b : {&h->pchol, &h->pchol_sl, &h->refine, &h->pqo, &h->xdiag, &h->mo, &h->vxc_diag, &h->delta, &h->v, &h->sigx, &h->flag, &h->xt, &h->dvec, &h->a,
                       &h->linv, &h->qacc, &h->qall, &h->sigma, &h->omega, &h->weight, &h->states, &h->err, &h->qp,
-                      &h->qp_scratch, &h->omega_out, &h->panel32, &h->tc_sched, &h->batch_desc})
+                      &h->qp_scratch, &h->omega_out, &h->panel32, &h->tc_sched, &h->batch_desc, &h->qx, &h->sigmx})
         b->release();
     for (BatchLane& l : h->lanes) {
         if (l.stream) cudaStreamSynchronize(l.stream);
@@ -819,7 +830,7 @@ void load_system_impl(gwb200_handle* h, int64_t nmo, int64_t nocc, const double*
     const int64_t nvir = nmo - nocc, n = nocc * nvir;
     if (h->mem_limit > 0)  // drop the previous request's workspaces before sizing this system
         for (DevBuf* b : {&h->xt, &h->dvec, &h->a, &h->linv, &h->qacc, &h->qall, &h->panel32, &h->pchol, &h->pchol_sl,
-                          &h->refine})
+                          &h->refine, &h->qx, &h->sigmx})
             b->release();
     if (bound) {
         h->pqo.release();
@@ -1008,6 +1019,40 @@ int gwb200_sigma_c(gwb200_handle* h, const double* omega, const double* weight, 
         GWB_CUDA(cudaMemcpyAsync(h->stage_out.p, h->sigma.p, nb_sig, cudaMemcpyDeviceToHost, h->stream));
         GWB_CUDA(cudaStreamSynchronize(h->stream));
         std::memcpy(sigma_out, h->stage_out.p, nb_sig);
+    });
+}
+
+int gwb200_sigma_c_matrix(gwb200_handle* h, const double* omega, const double* weight, int64_t nfreq,
+                          const int64_t* states, int64_t nstates, double* sigma_out, gwb200_stats* stats) {
+    return guarded([&] {
+        check_system(h);
+        if (!omega || !weight || !sigma_out || !states) fail(GWB200_BAD_ARGUMENT, "null input or output array");
+        if (nstates < 1 || nstates > 64) fail(GWB200_BAD_SHAPE, "the state-pair self-energy takes 1 to 64 states");
+        if (nfreq <= 0) fail(GWB200_BAD_SHAPE, "--freq-points must be positive");
+        gwb200_stats local{};
+        gwb200_stats* st = stats ? stats : &local;
+        *st = gwb200_stats{};
+        cudaStream_t s = h->stream;
+        const int64_t ns = nstates;
+        const size_t per_freq = (size_t)h->nmo * ns * ns;  // cross forms [k][s][t] of one frequency
+        size_buffer(h, h->qx, sizeof(double) * per_freq * (size_t)nfreq);
+        const ChunkHook hook = [&](const TallGeometry& g, int64_t f0, int64_t nf) {
+            launch_cross_forms(g, nf, h->a.as<double>(), h->nmo, ns, h->qx.as<double>() + (size_t)f0 * per_freq, s);
+        };
+        compute_forms(h, omega, nfreq, states, nstates, 0.0, GWB200_FP64, st, weight, &hook);
+        const size_t sig_bytes = sizeof(double) * 2 * (size_t)ns * ns * nfreq;
+        size_buffer(h, h->sigmx, sig_bytes);
+        st->kernel_launches += launch_sigma_contract_pairs(
+            h->qx.as<double>(), nfreq, h->nmo, ns, h->mo.as<double>(), h->fermi, h->omega.as<double>(),
+            h->weight.as<double>(), h->omega.as<double>(), nfreq, h->sigmx.as<double>(), s);
+        GWB_CUDA(cudaEventRecord(h->ev[3], s));
+        finish_forms(h, st);
+        st->device_ms_contract = elapsed(h->ev[2], h->ev[3]);
+        st->device_ms_total = elapsed(h->ev[0], h->ev[3]);
+        h->stage_out.ensure(sig_bytes);
+        GWB_CUDA(cudaMemcpyAsync(h->stage_out.p, h->sigmx.p, sig_bytes, cudaMemcpyDeviceToHost, s));
+        GWB_CUDA(cudaStreamSynchronize(s));
+        std::memcpy(sigma_out, h->stage_out.p, sig_bytes);
     });
 }
 

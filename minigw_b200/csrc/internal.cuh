@@ -149,6 +149,14 @@ int tune_update_variant(const TallGeometry& g, int64_t nf, double* a, cudaStream
                         unsigned long long* sched = nullptr, unsigned long long* err_pivot = nullptr,
                         bool timed = true);
 const char* update_variant_name(int v);
+// kernels_offdiag.cu: the cross forms q[f][k][s][t] = -w_{s,k} . w_{t,k} of a factored chunk of
+// nf tall matrices (nstates <= 64), and their contraction into Sigma_c(p_s, p_t; i w_n) (layout
+// [s][t][n] complex interleaved), the diagonal's G0 weighting.
+int launch_cross_forms(const TallGeometry& g, int64_t nf, const double* a, int64_t nmo, int64_t nstates, double* qx,
+                       cudaStream_t s);
+int launch_sigma_contract_pairs(const double* qx, int64_t nf_int, int64_t nmo, int64_t nstates, const double* mo,
+                                double fermi, const double* omega_int, const double* weight_int,
+                                const double* omega_out, int64_t nf_out, double* sigma, cudaStream_t s);
 // Contraction of the screened forms of nf_int integration frequencies onto nf_out output
 // frequencies (the full grid; a shard of integration frequencies gives a partial sum).
 int launch_sigma_contract(const double* qall, int64_t nf_int, int64_t nstates, int64_t nmo, int64_t ldq,

@@ -190,6 +190,20 @@ class B200Backend:
                                  _precision_code(precision), dptr(out), C.byref(stats)))
         return out, stats.as_dict()
 
+    def sigma_c_matrix(self, omegas, weights, states):
+        """Sigma_c(p_s, p_t; i w_n) between the requested states (plain FP64 form, eta = 0, at most
+        64 states): a complex array [nstates, nstates, nfreq], symmetric in (s, t), whose diagonal
+        is sigma_c's rows of the states to rounding (gwb200_sigma_c_matrix; the reference computes
+        the diagonal only)."""
+        om = np.ascontiguousarray(omegas, dtype=np.float64)
+        w = np.ascontiguousarray(weights, dtype=np.float64)
+        st = np.ascontiguousarray(states, dtype=np.int64)
+        out = np.zeros((st.shape[0], st.shape[0], om.shape[0]), dtype=np.complex128)
+        stats = Stats()
+        check(lib.gwb200_sigma_c_matrix(self._h, dptr(om), dptr(w), om.shape[0], iptr(st), st.shape[0], dptr(out),
+                                        C.byref(stats)))
+        return out, stats.as_dict()
+
     def sigma_c_shard(self, omegas, weights, f_begin: int, f_end: int, states, eta: float = 0.0, precision="fp64"):
         """Partial Sigma_c from the integration frequencies [f_begin, f_end) onto the whole grid."""
         om = np.ascontiguousarray(omegas, dtype=np.float64)

@@ -114,6 +114,41 @@ class Oracle:
         q = self.screened_forms(inp, omegas, states, eta, panel)
         return self.sigma_from_forms(inp, omegas, weights, states, q, panel), q
 
+    def sigma_c_matrix(self, inp, omegas, weights, states, eta=0.0):
+        """Sigma_c(p_s, p_t; i w_n) between the states, complex [nstates, nstates, nfreq]: an
+        extension beside the reference, which computes the diagonal only (docs/formulation.md:186).
+        Per frequency W_c is gwo_w_c's (src/workspace/screening_workspace.cpp:21-66) and the panels
+        gwo_panel's (src/workspace/pq_ph_panel.cpp:25-47); the cross forms are
+        q[f, k, s, t] = x_{p_s k}^T W_c x_{p_t k}, and the accumulation is gwo_sigma_from_forms's
+        (src/gw/sigma_c_driver.cpp:119-169) with q[f, s, k] replaced by q[f, k, s, t].  Its diagonal
+        is sigma_c's rows of the states."""
+        nmo, nocc = inp.nmo, inp.nocc
+        n = nocc * (nmo - nocc)
+        om = np.ascontiguousarray(omegas, dtype=np.float64)
+        wts = np.ascontiguousarray(weights, dtype=np.float64)
+        _, _, delta = self.ph_map(nmo, nocc, inp.mo_energy)
+        v = self.vph(inp)
+        ns, nf = len(states), om.shape[0]
+        xs = np.zeros((ns, n, nmo))  # xs[s] = the panel of state p_s over all k
+        for s, p in enumerate(states):
+            self.lib.gwo_panel(nmo, nocc, _d(inp.eri_mo), int(p), 0, nmo, _d(xs[s]))
+        q = np.zeros((nf, nmo, ns, ns), dtype=np.complex128)
+        for f in range(nf):
+            pi0 = np.zeros(n, dtype=np.complex128)
+            self.lib.gwo_pi0(0.0, float(om[f]), n, _d(delta), eta, _d(pi0))
+            wc = np.zeros((n, n), dtype=np.complex128)
+            if self.lib.gwo_w_c(n, _d(v), _d(pi0), _d(wc)):
+                raise RuntimeError("oracle W_c: near-singular pivot")
+            wx = wc @ xs  # [s, i, k]
+            q[f] = xs.transpose(2, 0, 1) @ wx.transpose(2, 1, 0)  # [k, s, t]
+        mo = np.asarray(inp.mo_energy, dtype=np.float64)
+        sig = np.zeros((ns, ns, nf), dtype=np.complex128)
+        for fn in range(nf):
+            den = 1j * om[fn] + inp.fermi_energy - mo
+            g0 = den[None, :] / (den[None, :] ** 2 + om[:, None] ** 2)  # (i w_p)^2 = -w_p^2
+            sig[:, :, fn] = -np.einsum("fk,f,fkst->st", g0, wts, q) / np.pi
+        return sig
+
     def pade_coeffs(self, x, y, npar):
         x = np.ascontiguousarray(x, dtype=np.complex128)
         y = np.ascontiguousarray(y, dtype=np.complex128)

@@ -1,0 +1,107 @@
+"""Sigma_c between states, Sigma_c(p_s, p_t; i w_n): gwb200_sigma_c_matrix against the oracle.
+
+The reference computes the diagonal only; the matrix is an extension beside it.  The oracle's
+restatement (Oracle.sigma_c_matrix) builds W_c per frequency from the same C functions as the
+pinned diagonal path, so its diagonal is pinned here against Oracle.sigma_c first (CPU test).
+The GPU tests then hold the whole matrix to the plain form's parity bar (1e-10 Ha absolute), its
+symmetry in (s, t), and its diagonal to the device's own diagonal Sigma_c (same solved rows,
+another summation order: 1e-12 relative).
+"""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+SIGMA_ATOL = 1e-10
+
+
+def _grid(oracle_lib, nfreq):
+    return oracle_lib.grid(nfreq)
+
+
+def test_oracle_matrix_diagonal_is_the_pinned_sigma(oracle_lib, h2o_input):
+    om, w = _grid(oracle_lib, 24)
+    states = [0, 3, 4, 5, 9, 17]
+    mat = oracle_lib.sigma_c_matrix(h2o_input, om, w, states)
+    diag, _ = oracle_lib.sigma_c(h2o_input, om, w, states)
+    assert mat.shape == (6, 6, 24)
+    for s, p in enumerate(states):
+        np.testing.assert_allclose(mat[s, s], diag[p], rtol=1e-12, atol=1e-14)
+    np.testing.assert_allclose(mat, mat.transpose(1, 0, 2), rtol=1e-12, atol=1e-14)
+    # states of different irreducible representations of the molecule's point group couple to zero;
+    # the others carry weight of their own
+    off = np.abs(mat).max(axis=2)[~np.eye(6, dtype=bool)]
+    assert off.max() > 1e-4 and off.min() < 1e-14
+
+
+def _check_against_oracle(be, oracle_lib, inp, nfreq, states):
+    om, w = _grid(oracle_lib, nfreq)
+    be.load_system(inp)
+    mat, stats = be.sigma_c_matrix(om, w, states)
+    ns = len(states)
+    assert mat.shape == (ns, ns, nfreq)
+    np.testing.assert_array_equal(mat, mat.transpose(1, 0, 2))  # both triangles from one sum
+    ref = oracle_lib.sigma_c_matrix(inp, om, w, states)
+    err = np.abs(mat - ref).max()
+    assert err <= SIGMA_ATOL, err
+    diag, _ = be.sigma_c(om, w, states)
+    for s, p in enumerate(states):
+        np.testing.assert_allclose(mat[s, s], diag[p], rtol=1e-12, atol=1e-15)
+    assert stats["kernel_launches"] > 0
+    return mat
+
+
+@pytest.mark.gpu
+def test_h2o_all_states(oracle_lib, h2o_input):
+    from minigw_b200 import B200Backend
+
+    with B200Backend(0) as be:
+        _check_against_oracle(be, oracle_lib, h2o_input, 32, list(range(18)))
+
+
+@pytest.mark.gpu
+def test_synthetic_subset_and_one_state(oracle_lib):
+    from minigw_b200 import B200Backend
+    from minigw_b200.synthetic import make_input
+
+    inp = make_input(40, 12, seed=3)
+    with B200Backend(0) as be:
+        mat = _check_against_oracle(be, oracle_lib, inp, 20, [0, 5, 11, 12, 20, 39])
+        one = _check_against_oracle(be, oracle_lib, inp, 20, [11])
+        np.testing.assert_allclose(one[0, 0], mat[2, 2], rtol=1e-12, atol=1e-15)
+
+
+@pytest.mark.gpu
+def test_sixty_four_states_several_row_chunks(oracle_lib):
+    """64 states (the cap): the cross-form kernel stages the rows in 32-column chunks, so n = 384
+    spans twelve of them; several frequency chunks are not needed for the kernel's correctness
+    but 10 frequencies exercise the per-chunk hook's offsets."""
+    from minigw_b200 import B200Backend
+    from minigw_b200.synthetic import make_input
+
+    inp = make_input(70, 6, seed=5)
+    states = list(range(3, 67))
+    with B200Backend(0) as be:
+        _check_against_oracle(be, oracle_lib, inp, 10, states)
+
+
+@pytest.mark.gpu
+def test_bad_state_lists():
+    from minigw_b200 import B200Backend, GwB200Error
+    from minigw_b200.synthetic import make_input
+
+    inp = make_input(70, 6, seed=5)
+    om = np.linspace(0.1, 2.0, 4)
+    w = np.full(4, 0.1)
+    with B200Backend(0) as be:
+        be.load_system(inp)
+        with pytest.raises(GwB200Error) as e:
+            be.sigma_c_matrix(om, w, list(range(65)))
+        assert e.value.status == "GWB200_BAD_SHAPE"
+        with pytest.raises(GwB200Error):
+            be.sigma_c_matrix(om, w, [])
+        with pytest.raises(GwB200Error):
+            be.sigma_c_matrix(om, w, [0, 70])
+        # the handle stays usable after the refusals
+        mat, _ = be.sigma_c_matrix(om, w, [0, 1])
+        assert np.isfinite(mat).all()
