@@ -247,9 +247,9 @@ int gwb200_read_input_h5(const char* path, int64_t* nmo, int64_t* nocc, double* 
  * library holds until exit; one frequency must fit: (n64 + m64) * n64 + n64 + 4096 + m64 doubles
  * <= 524256 (n64, m64 = n, m rounded up to 64), e.g. n = m = 320, else GWB200_BAD_SHAPE.  Every
  * buffer must be device (or managed) memory of the current device, else GWB200_BAD_ARGUMENT.  Each
- * call looks up that array's device address (cudaGetSymbolAddress); on the first call on a device
- * this loads the library's device code there, so make that first call before any stream capture.
- * The call reads the factorisation's pivot flag back and synchronises `stream` before it returns.
+ * call looks up that array's device address (cudaGetSymbolAddress; the first call on a device
+ * loads the library's device code there).  The call reads the factorisation's pivot flag back and
+ * synchronises `stream` before it returns, so it cannot be captured into a CUDA graph.
  * All calls share the array and it keeps the last call's contents: calls that overlap on the GPU
  * race and must be serialised by the caller.
  * No counterpart in the reference (an addition of this library). */
