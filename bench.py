@@ -619,15 +619,15 @@ def run_b200(args, wl):
     if args.precision == "fp64" and kernel_used == 6 and achieved:
         # the autotuner chose the int8 tensor-core emulation of the FP64 update (k_slice_panel64 +
         # k_update64_oz, timed together): bound by the FP64 C read+write, 16 bytes per updated
-        # element per K = 128 pass, i.e. flops_update / 16 bytes; the int8 work is 28 products of
-        # 7-digit slices per FP64 product
+        # element per K = 128 pass, i.e. flops_update / 16 bytes; the int8 work is 26 products of
+        # 6-digit slices per FP64 product
         gbs = upd_flops / 16.0 / (upd_ms * 1e-3) / 1e9
         result["roofline"] = {
             "bound": "hbm", "kernel": "k_update64_oz (FP64 trailing update emulated on int8 tcgen05, with "
                                       "k_slice_panel64)",
             "achieved": gbs, "peak": hbm_peak_gbs(), "unit": "GB/s", "frac": gbs / hbm_peak_gbs(),
             "peak_source": hbm_peak_source(),
-            "tflops_fp64_equivalent": achieved, "int8_tops": achieved * 28.0,
+            "tflops_fp64_equivalent": achieved, "int8_tops": achieved * 26.0,
             "vs_fp64_dmma_peak": achieved / peak_fp64, "launches": upd_n, "traffic": traffic_oz(wl.name),
             "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum per k_update64_oz launch "
                               "(profiles/k_update64_oz_traffic.json)" if traffic_oz(wl.name) else None}

@@ -129,7 +129,7 @@ int launch_factor_chunk(const TallGeometry& g, int64_t nf, double* a, double* li
                         unsigned long long* err_pivot, cudaStream_t s, UpdateProfiler* prof, int variant,
                         void* oz = nullptr, unsigned long long* sched = nullptr, int max_ctas = 0);
 // kernels_oz.cu: FP64 trailing update C -= P P^T (K = 128 from kb0, columns [c_begin, n_pad), rows
-// [c_begin, rows)) from exact int8 products of 7-digit row slices (tcgen05 kind::i8).  Two launches.
+// [c_begin, rows)) from exact int8 products of 6-digit row slices (tcgen05 kind::i8).  Two launches.
 size_t oz_slice_bytes_per_freq(const TallGeometry& g);
 // max_ctas > 0 caps the persistent grid (a handle that shares the GPU with other streams).
 int launch_update64_oz(const TallGeometry& g, int64_t nf, double* a, int64_t kb0, int64_t c_begin, void* slices,

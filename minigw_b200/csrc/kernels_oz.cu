@@ -3,32 +3,34 @@
 // The plain form's dominant work is C -= P_r . P_c over the trailing lower part after each outer
 // block of K = 128 columns (FP64; kernels_fp64.cu runs it on the FP64 DMMA pipe, 37 TFLOP/s
 // peak).  Here each panel row P_r (128 values) is written as
-//     P_r[k] = 2^e_r * sum_{s=1..7} D_s[r][k] 2^{-7 s} + (remainder below 2^{e_r - 49}),
-// with e_r the smallest power of two above max_k |P_r[k]| and D_s signed 7-bit digits (|D_s| <=
-// 127, truncation of the scaled value, so every digit carries the sign of the value).  The
-// product of two rows is then
+//     P_r[k] = 2^e_r * sum_{s=1..6} D_s[r][k] 2^{-7 s} + (remainder of at most 2^{e_r - 43}),
+// with 2^{e_r - 1} the smallest power of two above max_k |P_r[k]| and D_s balanced 7-bit digits
+// (round to nearest of the scaled remainder, |D_s| <= 64, so each digit and each remainder is
+// exact and the dropped remainder is centred on zero).  The product of two rows is then
 //     P_r . P_c ~= 2^{e_r + e_c} sum_{l=2..8} 2^{-7 l} S_l,   S_l = sum_{s+t=l} D_s[r] . D_t[c],
-// dropping only the terms with s + t > 8 (below 2^{-56} relative to the row maxima).  Each S_l is
-// an exact int32 sum of int8 products (|S_l| <= 7 * 127^2 * 128 < 2^24), accumulated by 28
+// dropping only the terms with s + t > 8 (below 2^{-58} relative to the row maxima).  Each S_l is
+// an exact int32 sum of int8 products (|S_l| <= 6 * 64^2 * 128 < 2^22), accumulated by 26
 // int8 tensor-core products per 32-deep K step; the levels are combined exactly in 64-bit
 // integers into two parts, converted, joined with one FP64 rounding and scaled by exact powers
 // of two.  The error per element is at the level of an FP64
-// dot product of the same rows (measured: screened forms within ~1e-14 relative of the FP64 DMMA
-// path); this is the Ozaki splitting scheme restated for power-of-two row scaling.
+// dot product of the same rows (measured: screened forms within ~1e-13 relative of the FP64 DMMA
+// path); this is the Ozaki splitting scheme restated for power-of-two row scaling.  (Six balanced
+// digits with levels <= 8 match seven truncated ones with levels <= 8 in accuracy -- the
+// remainder, not the level cut, dominates either way -- at 26 products instead of 28.)
 //
 // Two launches per update:
-//   k_slice_panel64  one warp per panel row: e_r, and the 7 digit slices of the row's 128 values,
+//   k_slice_panel64  one warp per panel row: e_r, and the 6 digit slices of the row's 128 values,
 //                    each slice a 128-byte row in the 128-byte-swizzled K-major layout
 //                    ([slice][row][128 bytes]) the tensor core reads;
 //   k_update64_oz    persistent, warp-specialised, one CTA per SM (10 warps, 222 KB of shared
 //                    memory, 512 TMEM columns):
 //                      warp 0     producer: units from a global counter handed on through a
-//                                 4-slot mbarrier ring; loads the unit's A slices 3-7 (128 rows,
-//                                 80 KB, resident for the unit) and streams the B slices (64
-//                                 rows, 8 KB each) through a 13-stage ring;
+//                                 4-slot mbarrier ring; loads the unit's A slices 3-6 (128 rows,
+//                                 64 KB, resident for the unit) and streams the B slices (64
+//                                 rows, 8 KB each) through a 15-stage ring;
 //                      warp 1     TMEM allocation; lane 0 issues tcgen05.mma kind::i8 (M = 128,
 //                                 N = 64, K = 32 per instruction; A slices 1-2, which take part
-//                                 in 13 of the 28 products, from TMEM (columns 448-511), the
+//                                 in 12 of the 26 products, from TMEM (columns 448-511), the
 //                                 others and B from shared memory) into 7 int32 accumulators,
 //                                 one per level l (columns 64 (l - 2));
 //                      warps 2-9  epilogue: at each unit start, write A slices 1-2 into TMEM;
@@ -38,8 +40,8 @@
 //                                 adds it to C with a bulk reduction (cp.reduce.async.bulk
 //                                 .add.f64) per row and half.
 // The accumulators are drained in two level groups so that the tensor core does not wait for the
-// whole drain: per tile the MMAs of group X (levels 4-8, 22 of the 28 products) run first and are
-// committed, then those of group Y (levels 2-3, 6 products).  The epilogue reads group X (keeping
+// whole drain: per tile the MMAs of group X (levels 4-8, 23 of the 26 products) run first and are
+// committed, then those of group Y (levels 2-3, 3 products).  The epilogue reads group X (keeping
 // S4 2^7 + S5 and the exact low part (S6 2^14 + S7 2^7 + S8) per element) and releases it while
 // group Y runs; the next tile's group X then runs while the epilogue reads group Y and finishes
 // the tile.  (At N = 64 a tcgen05.mma kind::i8 costs ~48 cycles whatever its operands, so these
@@ -61,18 +63,21 @@ using namespace tc;
 
 constexpr int kOzM = 128;                    // accumulator rows = TMEM lanes
 constexpr int kOzN = 64;                     // accumulator columns per level
-constexpr int kOzSlices = 7;                 // digit slices per value
+constexpr int kOzSlices = 6;                 // digit slices per value
+constexpr int kOzLevels = 7;                 // levels s + t = 2..8, one accumulator each
+constexpr int kOzMaxSum = kOzLevels - 1;     // 0-based slice indices: products with sa + t <= 6
 constexpr int kOzSeg = 32;                   // column tiles per work unit
-constexpr int kOzStages = 13;                // B ring depth (one slice per stage): a tile's 7, the 2 held
-                                             // for group Y, and 4 ahead
-constexpr int kOzTmemSlices = 2;             // A slices 1-2 (13 of the 28 products) read from TMEM
+constexpr int kOzStages = 15;                // B ring depth (one slice per stage): a tile's 6, the 2 held
+                                             // for group Y, and 7 ahead
+constexpr int kOzTmemSlices = 2;             // A slices 1-2 (12 of the 26 products) read from TMEM
 constexpr int kSchedSlots = 4;
 constexpr int kSliceA = kOzM * 128;          // one slice of 128 rows: 16 KB
 constexpr int kSliceB = kOzN * 128;          // of 64 rows: 8 KB
 constexpr int kEpiWarps = 8;                 // 4 lane quadrants x 2 column halves of 32
 constexpr int kOzThreads = 32 * (2 + kEpiWarps);
 constexpr int kTmemCols = 512;               // 7 levels x 64 columns, then A slices 1-2 (32 each)
-constexpr int kTmemA = kOzSlices * kOzN;     // first column of the A slices held in TMEM
+constexpr int kTmemA = kOzLevels * kOzN;     // first column of the A slices held in TMEM
+static_assert(kTmemA + 32 * kOzTmemSlices <= kTmemCols, "TMEM columns");
 constexpr int kStgRow = 128 + 16;            // staging row stride: 16 doubles + 16 bytes (banks)
 constexpr int kStgBytes = 32 * kStgRow;      // per epilogue warp
 constexpr int kHeader = 1024;
@@ -132,7 +137,7 @@ __device__ __forceinline__ double pow2(int k) {  // 2^k for -1022 <= k <= 1023, 
     return __longlong_as_double((long long)(k + 1023) << 52);
 }
 
-// Per frequency: 7 slices of rp rows x 128 bytes, then rp int32 exponents.
+// Per frequency: 6 slices of rp rows x 128 bytes, then rp int32 exponents.
 __host__ __device__ constexpr size_t oz_freq_bytes(int64_t rp) {
     return ((size_t)kOzSlices * rp * 128 + (size_t)rp * 4 + 1023) / 1024 * 1024;
 }
@@ -158,10 +163,11 @@ __global__ void __launch_bounds__(256) k_slice_panel64(const double* __restrict_
     for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
     int e = 0;
     if (m > 0.0) frexp(m, &e);  // m = frac * 2^e, frac in [0.5, 1): |x| < 2^e
+    ++e;                        // the row scale: |x| < 2^{e - 1}
     const double inv = pow2(-e);
     double v[4];
 #pragma unroll
-    for (int j = 0; j < 4; ++j) v[j] = x[j] * inv;  // |v| < 1, exact
+    for (int j = 0; j < 4; ++j) v[j] = x[j] * inv;  // |v| < 1/2, exact
     const uint32_t chunk = (uint32_t)(lane >> 2), in_chunk = (uint32_t)(lane & 3) * 4;
     const size_t pos = (size_t)((chunk ^ (uint32_t)(rr & 7)) * 16 + in_chunk);
 #pragma unroll
@@ -169,9 +175,9 @@ __global__ void __launch_bounds__(256) k_slice_panel64(const double* __restrict_
         uint32_t word = 0;
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
-            const double t = v[j] * 128.0;  // exact
-            const double d = trunc(t);       // |d| <= 127
-            v[j] = t - d;                    // exact
+            const double t = v[j] * 128.0;  // exact, |t| <= 64
+            const double d = rint(t);        // |d| <= 64
+            v[j] = t - d;                    // exact, |v| <= 1/2
             word |= ((uint32_t)(int)d & 0xFFu) << (8 * j);
         }
         *reinterpret_cast<uint32_t*>(slices + ((size_t)s * rp + rr) * 128 + pos) = word;
@@ -202,8 +208,8 @@ __global__ void __launch_bounds__(kOzThreads, 1)
     extern __shared__ __align__(1024) uint8_t osm[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const uint32_t base = smem_u32(osm);
-    const uint32_t abuf = (base + kHeader + 1023u) & ~1023u;  // 7 A slices, 1024-aligned
-    const uint32_t ring = abuf + (kOzSlices - kOzTmemSlices) * kSliceA;  // B stages (A slices 3-7 before)
+    const uint32_t abuf = (base + kHeader + 1023u) & ~1023u;  // A slices 3-6, 1024-aligned
+    const uint32_t ring = abuf + (kOzSlices - kOzTmemSlices) * kSliceA;  // B stages (A slices 3-6 before)
     const uint32_t stg0 = ring + kOzStages * kSliceB;          // epilogue staging rows
     volatile uint32_t* abort_flag = reinterpret_cast<volatile uint32_t*>(osm + kOffAbort);
     volatile int64_t* uslot = reinterpret_cast<volatile int64_t*>(osm + kOffUnit);
@@ -287,7 +293,7 @@ __global__ void __launch_bounds__(kOzThreads, 1)
             if (!got) break;
             if (lane == 0) mbar_expect_tx(afull, (uint32_t)((kOzSlices - kOzTmemSlices) * kSliceA));
             __syncwarp();
-            if (lane < kOzSlices - kOzTmemSlices)  // one 16 KB copy per smem slice (slices 3-7)
+            if (lane < kOzSlices - kOzTmemSlices)  // one 16 KB copy per smem slice (slices 3-6)
                 bulk_g2s(abuf + lane * kSliceA, slices + ((size_t)(lane + kOzTmemSlices) * rp + i * kOzM) * 128, kSliceA,
                          afull);
             a_filled = true;
@@ -346,21 +352,24 @@ __global__ void __launch_bounds__(kOzThreads, 1)
             if (!mbar_wait(atmem, aph, abort_flag, err)) break;
             tc_fence_after();
             aph ^= 1u;
-            // A slice sa+1 against B slice t+1 (in stage st) into level sa + t + 2; the first
-            // product of every level in issue order has t = 0, kk = 0 and starts the accumulator
+            // A slice sa+1 against B slice t+1 (in stage st) into level sa + t + 2.  Products are
+            // issued with t ascending, so the first product of level sa + t has the smallest t
+            // the level allows, t0 = max(0, sa + t - (kOzSlices - 1)); it starts the accumulator
+            // at kk = 0 (level 8 has no t = 0 product: it starts at sa = 6, t = 2, 1-based)
             auto pair = [&](int sa, int t, int st) {
                 // descriptors differ from the stage / A bases only in the address field (bytes >>
                 // 4, below 2^14 for shared memory): constant offsets, no carries
                 const uint64_t db0 = desc_b0 + (uint64_t)((uint32_t)(st * kSliceB) >> 4);
                 const uint32_t d = tmem + (uint32_t)((sa + t) * kOzN);
+                const bool starts = t == (sa + t > kOzSlices - 1 ? sa + t - (kOzSlices - 1) : 0);
 #pragma unroll
                 for (int kk = 0; kk < 4; ++kk) {
+                    const uint32_t acc = (!starts || kk > 0) ? 1u : 0u;
                     if (sa < kOzTmemSlices)  // A slice from TMEM: 32 bytes of K = 8 columns
-                        mma_i8_ts(d, tmem + (uint32_t)(kTmemA + 32 * sa + 8 * kk), db0 + (uint64_t)(2 * kk),
-                                  (t > 0 || kk > 0) ? 1u : 0u);
+                        mma_i8_ts(d, tmem + (uint32_t)(kTmemA + 32 * sa + 8 * kk), db0 + (uint64_t)(2 * kk), acc);
                     else
                         mma_i8(d, desc_a0 + (uint64_t)(((sa - kOzTmemSlices) * kSliceA + 32 * kk) >> 4),
-                               db0 + (uint64_t)(2 * kk), (t > 0 || kk > 0) ? 1u : 0u);
+                               db0 + (uint64_t)(2 * kk), acc);
                 }
             };
             for (int64_t c = c0; ok && c < c1; ++c) {
@@ -380,7 +389,7 @@ __global__ void __launch_bounds__(kOzThreads, 1)
                     tc_fence_after();
 #pragma unroll
                     for (int sa = 0; sa < kOzSlices; ++sa)
-                        if (sa + t >= 2 && sa < kOzSlices - t) pair(sa, t, s);
+                        if (sa + t >= 2 && sa + t <= kOzMaxSum) pair(sa, t, s);
                     if (t < 2)
                         st01[t] = s;
                     else
@@ -466,9 +475,9 @@ __global__ void __launch_bounds__(kOzThreads, 1)
                 const int64_t cj = c_begin + c * kOzN + half * 32;  // this warp's first column
                 const bool valid = r < rows && r >= c_begin + c * kOzN;
                 const int ec_lane = exps[c * kOzN + half * 32 + lane];  // exponent of column cj + lane
-                // Levels combined exactly: adjacent pairs in int32 (S_l <= (l-1) 127^2 128, so
-                // S2 2^7 + S3, S4 2^7 + S5, S6 2^7 + S7 < 2^31), then hi = (S2 2^7 + S3) 2^14 +
-                // S4 2^7 + S5 < 2^43 and lo = (S6 2^7 + S7) 2^7 + S8 < 2^39 in int64 (held as an
+                // Levels combined exactly: adjacent pairs in int32 (|S_l| <= 6 64^2 128 < 2^22, so
+                // S2 2^7 + S3, S4 2^7 + S5, S6 2^7 + S7 < 2^30), then hi = (S2 2^7 + S3) 2^14 +
+                // S4 2^7 + S5 < 2^44 and lo = (S6 2^7 + S7) 2^7 + S8 < 2^37 in int64 (held as an
                 // exact double between the groups); value = hi 2^-35 + lo 2^-56 with one rounding,
                 // scaled by 2^{e_r + e_c}.
                 const uint32_t lanes = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(half * 32);
@@ -493,9 +502,9 @@ __global__ void __launch_bounds__(kOzThreads, 1)
                 double m_d[32];
 #pragma unroll
                 for (int h16 = 0; h16 < 2; ++h16) {  // group X: levels 4-8, 16 columns per wait
-                    uint32_t v[kOzSlices - 2][16];
+                    uint32_t v[kOzLevels - 2][16];
 #pragma unroll
-                    for (int L = 2; L < kOzSlices; ++L) tmem_ld16_nowait(lanes + (uint32_t)(L * kOzN + 16 * h16), v[L - 2]);
+                    for (int L = 2; L < kOzLevels; ++L) tmem_ld16_nowait(lanes + (uint32_t)(L * kOzN + 16 * h16), v[L - 2]);
                     tmem_wait_ld();
                     if (h16 == 1) release_group(0);
 #pragma unroll

@@ -2,10 +2,10 @@
 checked on CPU against exact products, so that the slice and level counts the kernels use are
 pinned by a test and not only by the GPU comparisons:
 
-  * the plain form's trailing update (kernels_oz.cu): 7 truncated signed 7-bit digits per panel row
-    against a power-of-two row scale, products of levels s + t <= 8 (28 per K step): the product
-    of two panel rows within ~1e-12 of ||P_r|| ||P_c||, far inside what the FP64 DMMA comparison
-    (1e-12 on the forms) allows;
+  * the plain form's trailing update (kernels_oz.cu): 6 rounded (balanced) 7-bit digits per panel
+    row against a power-of-two row scale, products of levels s + t <= 8 (26 per K step): the
+    product of two panel rows within ~1e-12 of ||P_r|| ||P_c||, far inside what the FP64 DMMA
+    comparison (1e-12 on the forms) allows, and as close as 7 truncated digits at 28 products;
   * the refined mixed form's Gram term (kernels_gram_oz.cu): C^T in 7 and y in 4 rounded
     (balanced) digits, levels s + t <= 9: the corrected forms at the FP64 product's accuracy,
     where truncated digits or 3 y digits are not.
@@ -64,9 +64,10 @@ def _system(nmo: int, nocc: int, seed: int):
 
 @pytest.mark.parametrize("omega", [0.05, 1.0, 20.0])
 def test_update_scheme_product_error(omega):
-    """7 truncated digits, levels <= 8: the trailing-update product of two panel rows of a real
-    eps factorisation within 1e-12 of ||P_r|| ||P_c|| (measured 1-2e-13; an FP64 dot product
-    ~3e-16; 6 digits ~1e-11)."""
+    """6 rounded digits, levels <= 8 (26 products): the trailing-update product of two panel rows
+    of a real eps factorisation within 1e-12 of ||P_r|| ||P_c|| (measured ~2e-13; an FP64 dot
+    product ~3e-16), within 3x of 7 truncated digits at 28 products, while cutting the levels to
+    <= 7 (21 products) or truncating the 6 digits costs an order of magnitude."""
     _, de, v = _system(40, 12, seed=117)
     n = v.shape[0]
     d = 4 * de / (de * de + omega ** 2)
@@ -75,12 +76,16 @@ def test_update_scheme_product_error(omega):
     panel = chol[128:, :128]
     exact = panel.astype(np.longdouble) @ panel.T.astype(np.longdouble)
     scale = np.sqrt((panel * panel).sum(1)).max() ** 2
-    got, _, _ = _product(panel, panel, 7, 7, 8, rounded=False)
-    err = float(np.abs(got - exact).max() / scale)
-    assert err <= 1e-12, err
-    # and 6 digits would not be enough at FP64 level
-    got6, _, _ = _product(panel, panel, 6, 6, 7, rounded=False)
-    assert float(np.abs(got6 - exact).max() / scale) > 10 * err
+
+    def err(nd, lmax, rounded):
+        got, _, _ = _product(panel, panel, nd, nd, lmax, rounded)
+        return float(np.abs(got - exact).max() / scale)
+
+    e = err(6, 8, True)
+    assert e <= 1e-12, e
+    assert e <= 3 * err(7, 8, False)
+    assert err(6, 7, True) > 5 * e
+    assert err(6, 7, False) > 10 * e
 
 
 def _pchol(v: np.ndarray, tau_rel: float = 1e-13) -> np.ndarray:
