@@ -366,7 +366,7 @@ void compute_forms(gwb200_handle* h, const double* omega, int64_t nfreq, const i
         if (h->mem_limit > 0) {  // the handle's cap minus what the system and panels already hold
             const size_t resident = h->pqo.bytes + h->xdiag.bytes + h->v.bytes + h->xt.bytes + h->qall.bytes +
                                     h->sigma.bytes + h->qp_scratch.bytes + h->pchol.bytes + h->pchol_sl.bytes +
-                                    ((size_t)1 << 20);
+                                    h->qx.bytes + h->sigmx.bytes + ((size_t)1 << 20);
             const size_t lim = (size_t)h->mem_limit;
             const size_t room = lim > resident ? lim - resident : 0;
             budget = std::min(budget, room);

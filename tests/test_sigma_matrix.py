@@ -72,6 +72,26 @@ def test_synthetic_subset_and_one_state(oracle_lib):
 
 
 @pytest.mark.gpu
+def test_several_frequency_chunks(oracle_lib, monkeypatch):
+    """The cross forms are taken per frequency chunk, after that chunk's factorisation: with
+    chunks of 3 frequencies the matrix is the one-chunk matrix to rounding, and the oracle's."""
+    from minigw_b200 import B200Backend
+    from minigw_b200.synthetic import make_input
+
+    inp = make_input(36, 9, seed=11)
+    states = [6, 8, 9, 12]
+    om, w = _grid(oracle_lib, 11)
+    with B200Backend(0) as be:
+        be.load_system(inp)
+        whole, st1 = be.sigma_c_matrix(om, w, states)
+        monkeypatch.setenv("GWB200_MAX_FREQ_CHUNK", "3")
+        chunked, st3 = be.sigma_c_matrix(om, w, states)
+    assert st1["frequency_chunks"] == 1 and st3["frequency_chunks"] == 4
+    np.testing.assert_allclose(chunked, whole, rtol=1e-13, atol=1e-16)
+    assert np.abs(chunked - oracle_lib.sigma_c_matrix(inp, om, w, states)).max() <= SIGMA_ATOL
+
+
+@pytest.mark.gpu
 def test_sixty_four_states_several_row_chunks(oracle_lib):
     """64 states (the cap): the cross-form kernel stages the rows in 32-column chunks, so n = 384
     spans twelve of them; several frequency chunks are not needed for the kernel's correctness
