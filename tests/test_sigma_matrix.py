@@ -34,6 +34,42 @@ def test_oracle_matrix_diagonal_is_the_pinned_sigma(oracle_lib, h2o_input):
     assert off.max() > 1e-4 and off.min() < 1e-14
 
 
+def test_oracle_matrix_against_numpy_restatement(oracle_lib):
+    """The off-diagonal has no reference counterpart, so the oracle's matrix is checked against a
+    second, independent restatement: W_c = (I - diag(Pi0) V)^-1 diag(Pi0) by numpy's LU solve (the
+    oracle uses its Gauss-Jordan inverse, src/linalg/linalg.cpp:44-91), panels from the ERI tensor
+    by fancy indexing (eri[p, k, i, a], src/workspace/pq_ph_panel.cpp:25-47), and the G0 sum written
+    out per (n, f', k) as in src/gw/sigma_c_driver.cpp:154-168."""
+    from minigw_b200.synthetic import make_input
+
+    nmo, nocc = 18, 5
+    inp = make_input(nmo, nocc, seed=21)
+    om, w = _grid(oracle_lib, 6)
+    states = [2, 4, 5, 9]
+    mat = oracle_lib.sigma_c_matrix(inp, om, w, states)
+
+    nvir = nmo - nocc
+    eri = np.asarray(inp.eri_mo).reshape(nmo, nmo, nmo, nmo)
+    mo = np.asarray(inp.mo_energy)
+    io = np.repeat(np.arange(nocc), nvir)
+    av = nocc + np.tile(np.arange(nvir), nocc)
+    delta = mo[av] - mo[io]
+    v = eri[io[:, None], av[:, None], io[None, :], av[None, :]]  # V[ia, jb] = (ia|jb)
+    x = {p: eri[p][:, io, av].T for p in states}  # x_p[ia, k] = (p k|i a)
+    ref = np.zeros_like(mat)
+    for fp, wp in enumerate(om):
+        pi0 = 2.0 * (1.0 / (1j * wp - delta) - 1.0 / (1j * wp + delta))
+        wc = np.linalg.solve(np.eye(len(delta)) - pi0[:, None] * v, np.diag(pi0))
+        for s, ps in enumerate(states):
+            for t, pt in enumerate(states):
+                q = np.einsum("ik,ij,jk->k", x[ps], wc, x[pt])
+                for fn, wn in enumerate(om):
+                    den = 1j * wn + inp.fermi_energy - mo
+                    g0 = den / (den * den - (1j * wp) ** 2)
+                    ref[s, t, fn] -= np.sum(g0 * q) * w[fp] / np.pi
+    assert np.abs(mat - ref).max() <= 1e-12 * np.abs(ref).max()
+
+
 def _check_against_oracle(be, oracle_lib, inp, nfreq, states):
     om, w = _grid(oracle_lib, nfreq)
     be.load_system(inp)
