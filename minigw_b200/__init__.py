@@ -18,7 +18,8 @@ _LIB_NAMES = ("FP64", "MIXED", "MIXED_REFINED", "STATUS", "GwB200Error", "versio
 _GW_NAMES = (
     "B200Backend", "B200Server", "GwInput", "GwResult", "GwSettings", "GwSlices", "GwTimings",
     "generate_transformed_legendre_grid", "output_final_energy_table", "output_self_energy_after_pade",
-    "output_self_energy_before_pade", "plan_buckets", "read_gw_input_hdf5", "run_g0w0", "run_g0w0_batch",
+    "output_self_energy_before_pade", "plan_buckets", "read_gw_input_hdf5", "read_gw_input_slices", "run_g0w0",
+    "run_g0w0_batch",
     "selected_states",
 )
 

@@ -41,7 +41,7 @@ EXPORTS = (
     "gwb200_grid", "gwb200_read_input_h5", "gwb200_screened_forms_noalloc", "gwb200_fp64_peak_tflops",
     "gwb200_update_kernel", "gwb200_run_g0w0_batch", "gwb200_plan_buckets", "gwb200_read_resident",
     "gwb200_kernel_profile", "gwb200_load_system_slices", "gwb200_server_submit_slices", "gwb200_server_set_merge",
-    "gwb200_server_counters", "gwb200_sigma_c_matrix",
+    "gwb200_server_counters", "gwb200_sigma_c_matrix", "gwb200_read_input_h5_slices",
 )
 
 
@@ -131,6 +131,7 @@ def _load() -> C.CDLL:
                                       C.c_double, _dp]
     lib.gwb200_grid.argtypes = [C.c_int64, _dp, _dp]
     lib.gwb200_read_input_h5.argtypes = [C.c_char_p, _ip, _ip, _dp, _dp, _dp, _dp]
+    lib.gwb200_read_input_h5_slices.argtypes = [C.c_char_p, _ip, C.c_int64, _ip, _ip, _dp, _dp, _dp, _dp, _dp, _dp]
     lib.gwb200_screened_forms_noalloc.argtypes = [C.c_int64, C.c_int64, _vp, _vp, _vp, _vp, C.c_int64, _vp, _vp]
     lib.gwb200_fp64_peak_tflops.argtypes = [_vp, _dp]
     lib.gwb200_update_kernel.argtypes = [_vp, _ip]

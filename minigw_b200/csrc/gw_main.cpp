@@ -186,12 +186,12 @@ int main(int argc, char** argv) {
         const std::string path = join_path(cli.input_dir, "gw_input.h5");
         int64_t nmo = 0, nocc = 0;
         double fermi = 0.0;
-        check(gwb200_read_input_h5(path.c_str(), &nmo, &nocc, &fermi, nullptr, nullptr, nullptr), "read_gw_input_hdf5");
-        std::vector<double> mo(static_cast<size_t>(nmo)), vxc(static_cast<size_t>(nmo * nmo));
-        std::vector<double> eri(static_cast<size_t>(nmo) * nmo * nmo * nmo);
-        check(gwb200_read_input_h5(path.c_str(), &nmo, &nocc, &fermi, mo.data(), eri.data(), vxc.data()),
+        // Sizes first; the data is read once the state list is known, and only the slices the path
+        // uses (gwb200_read_input_h5_slices), never the nmo^4 ERI tensor.
+        check(gwb200_read_input_h5_slices(path.c_str(), nullptr, 0, &nmo, &nocc, &fermi, nullptr, nullptr, nullptr,
+                                          nullptr, nullptr),
               "read_gw_input_hdf5");
-        const double read_seconds = seconds_since(t_read);
+        double read_seconds = seconds_since(t_read);
         const int64_t nvirt = nmo - nocc, n_ph = nocc * nvirt;
         std::cout << "  - Vxc MO basis shape: (" << nmo << ", " << nmo << ")\n";
         std::cout << "  - Fermi energy (eV): " << fermi * kHartreeToEv << '\n';
@@ -215,6 +215,15 @@ int main(int argc, char** argv) {
         }
         for (auto s : states)
             if (s >= nmo) throw std::runtime_error("Selected state is out of range");
+        const auto t_slices = std::chrono::steady_clock::now();
+        const size_t ns = states.size();
+        std::vector<double> mo(static_cast<size_t>(nmo)), vxc_diag(static_cast<size_t>(nmo));
+        std::vector<double> vph(static_cast<size_t>(n_ph) * n_ph), panel(ns * static_cast<size_t>(nmo) * n_ph);
+        std::vector<double> xdiag(static_cast<size_t>(nmo) * nocc);
+        check(gwb200_read_input_h5_slices(path.c_str(), states.data(), static_cast<int64_t>(ns), &nmo, &nocc, &fermi,
+                                          mo.data(), vph.data(), panel.data(), xdiag.data(), vxc_diag.data()),
+              "read_gw_input_hdf5");
+        read_seconds += seconds_since(t_slices);
 
         int ndev = 1;
         const int device = (local_rank_from_env() / static_cast<int>(cli.tasks_per_gpu)) % std::max(1, ndev);
@@ -230,9 +239,9 @@ int main(int argc, char** argv) {
         }
         const auto t_total = std::chrono::steady_clock::now();
         auto t = std::chrono::steady_clock::now();
-        check(gwb200_load_system_states(h, nmo, nocc, mo.data(), eri.data(), vxc.data(), fermi, states.data(),
-                                        static_cast<int64_t>(states.size())),
-              "gwb200_load_system_states");
+        check(gwb200_load_system_slices(h, nmo, nocc, mo.data(), vph.data(), panel.data(), xdiag.data(),
+                                        vxc_diag.data(), fermi, states.data(), static_cast<int64_t>(ns)),
+              "gwb200_load_system_slices");
         const double setup_seconds = seconds_since(t);
         std::vector<double> omega(cli.freq_points), weight(cli.freq_points);
         check(gwb200_grid(static_cast<int64_t>(cli.freq_points), omega.data(), weight.data()), "generate grid");
@@ -308,7 +317,7 @@ int main(int argc, char** argv) {
                   << "---------" << '\n';
         for (const auto idx : states) {
             const size_t i = static_cast<size_t>(idx);
-            const double vxx = vxc[i * static_cast<size_t>(nmo) + i];
+            const double vxx = vxc_diag[i];
             const double sigma_c_qp = qp[i] + vxx - mo[i] - sigx[i];
             std::cout << std::left << std::setw(10) << (idx + 1) << std::setw(15) << mo[i] * kHartreeToEv
                       << std::setw(15) << sigx[i] * kHartreeToEv << std::setw(15) << sigma_c_qp * kHartreeToEv

@@ -1201,6 +1201,16 @@ int gwb200_read_input_h5(const char* path, int64_t* nmo, int64_t* nocc, double* 
     });
 }
 
+int gwb200_read_input_h5_slices(const char* path, const int64_t* states, int64_t nstates, int64_t* nmo,
+                                int64_t* nocc, double* fermi_energy, double* mo_energy, double* vph, double* panel,
+                                double* xdiag, double* vxc_diag) {
+    return guarded([&] {
+        if (!path || !nmo || !nocc || !fermi_energy) fail(GWB200_BAD_ARGUMENT, "null argument");
+        read_gw_input_h5_slices(path, states, nstates, nmo, nocc, fermi_energy, mo_energy, vph, panel, xdiag,
+                                vxc_diag);
+    });
+}
+
 int gwb200_screened_forms_noalloc(int64_t n, int64_t m, const double* d_v, const double* d_xt,
                                   const double* d_delta, const double* d_omega, int64_t nfreq, double* d_q_out,
                                   void* stream) {

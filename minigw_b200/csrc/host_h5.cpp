@@ -139,6 +139,26 @@ public:
         read_into(d.address, reinterpret_cast<uint8_t*>(out), bytes);
     }
 
+    // Reads elements [first, first + count) of the dataset (C order) as float64: one contiguous
+    // run of the file (contiguous layout) or of the compact data.
+    void read_f64_range(const Dataset& d, uint64_t first, uint64_t count, double* out, const std::string& name) {
+        if (d.type.cls != 1 || d.type.size != 8 || !d.type.little) io_fail(name + " is not little-endian float64");
+        uint64_t total = 1;
+        for (auto x : d.dims) total *= x;
+        if (first > total || count > total - first) io_fail(name + ": element range beyond the dataset");
+        const uint64_t bytes = count * 8;
+        if (d.layout == 0) {
+            if (d.compact.size() < (first + count) * 8) io_fail(name + ": compact data too short");
+            std::memcpy(out, d.compact.data() + first * 8, bytes);
+            return;
+        }
+        if (d.address == UINT64_MAX) {
+            std::memset(out, 0, bytes);
+            return;
+        }
+        read_into(d.address + first * 8, reinterpret_cast<uint8_t*>(out), bytes);
+    }
+
     // Root attributes: name -> (type, raw bytes).
     std::map<std::string, std::pair<TypeInfo, std::vector<uint8_t>>> attributes(const std::vector<Message>& msgs) {
         std::map<std::string, std::pair<TypeInfo, std::vector<uint8_t>>> out;
@@ -307,11 +327,15 @@ private:
     }
 };
 
-} // namespace
+// The three datasets and two attributes of a validated gw_input.h5.
+struct Input {
+    Dataset dmo, deri, dvxc;
+    uint64_t nmo = 0;
+    int64_t nocc = 0;
+    double fermi = 0.0;
+};
 
-void read_gw_input_h5(const std::string& path, int64_t* nmo_out, int64_t* nocc_out, double* fermi_out, double* mo,
-                      double* eri, double* vxc) {
-    Reader r(path);
+Input open_input(Reader& r) {
     const auto root_msgs = r.object_messages(r.root_header());
     const auto members = r.group_members(root_msgs);
     auto need = [&](const char* name) {
@@ -361,12 +385,62 @@ void read_gw_input_h5(const std::string& path, int64_t* nmo_out, int64_t* nocc_o
     }
     if (nocc < 0) io_fail("HDF5 input error: nocc attribute is negative");
     if (nocc == 0 || static_cast<uint64_t>(nocc) >= nmo) io_fail("HDF5 input error: nocc must be in [1, nmo-1]");
+    return Input{dmo, deri, dvxc, nmo, nocc, fermi};
+}
+
+} // namespace
+
+void read_gw_input_h5(const std::string& path, int64_t* nmo_out, int64_t* nocc_out, double* fermi_out, double* mo,
+                      double* eri, double* vxc) {
+    Reader r(path);
+    const Input in = open_input(r);
+    const uint64_t nmo = in.nmo;
     *nmo_out = static_cast<int64_t>(nmo);
-    *nocc_out = nocc;
-    *fermi_out = fermi;
-    if (mo) r.read_f64(dmo, mo, nmo, "/mo_energy");
-    if (eri) r.read_f64(deri, eri, nmo * nmo * nmo * nmo, "/eri_mo");
-    if (vxc) r.read_f64(dvxc, vxc, nmo * nmo, "/vxc_mo");
+    *nocc_out = in.nocc;
+    *fermi_out = in.fermi;
+    if (mo) r.read_f64(in.dmo, mo, nmo, "/mo_energy");
+    if (eri) r.read_f64(in.deri, eri, nmo * nmo * nmo * nmo, "/eri_mo");
+    if (vxc) r.read_f64(in.dvxc, vxc, nmo * nmo, "/vxc_mo");
+}
+
+// The slices of the file's ERI tensor that the screening path reads for a known state list, read
+// straight from /eri_mo without the nmo^4 tensor in memory (the layouts gwb200_load_system_slices
+// takes):
+//   vph[(j nvir + b) n + i nvir + a]        = eri[j, nocc + b, i, nocc + a]   (n x n)
+//   panel[(t nmo + k) n + i nvir + a]       = eri[states[t], k, i, nocc + a]  ((nstates nmo) x n)
+//   xdiag[p nocc + i]                       = eri[p, i, p, i]                 (nmo x nocc)
+//   vxc_diag[p]                             = vxc_mo[p, p]
+// Each (j, b) row of V and each (t, k) row of the panel is one read of the contiguous run
+// eri[., ., 0:nocc, 0:nmo] (nocc nmo doubles), scattered to the nvir-long runs the layout keeps.
+void read_gw_input_h5_slices(const std::string& path, const int64_t* states, int64_t nstates, int64_t* nmo_out,
+                             int64_t* nocc_out, double* fermi_out, double* mo, double* vph, double* panel,
+                             double* xdiag, double* vxc_diag) {
+    Reader r(path);
+    const Input in = open_input(r);
+    const uint64_t nmo = in.nmo, nocc = static_cast<uint64_t>(in.nocc), nvir = nmo - nocc, n = nocc * nvir;
+    *nmo_out = static_cast<int64_t>(nmo);
+    *nocc_out = in.nocc;
+    *fermi_out = in.fermi;
+    if (!mo && !vph && !panel && !xdiag && !vxc_diag) return;  // size query
+    if (!mo || !vph || !panel || !xdiag || !vxc_diag) fail(GWB200_BAD_ARGUMENT, "null output array");
+    if (!states || nstates <= 0) fail(GWB200_BAD_SHAPE, "at least one state is required");
+    for (int64_t t = 0; t < nstates; ++t)
+        if (states[t] < 0 || static_cast<uint64_t>(states[t]) >= nmo) fail(GWB200_BAD_SHAPE, "Selected state is out of range");
+    r.read_f64(in.dmo, mo, nmo, "/mo_energy");
+    std::vector<double> run(static_cast<size_t>(nocc * nmo));
+    auto cut = [&](uint64_t p, uint64_t q, double* row) {  // row[i nvir + a] = eri[p, q, i, nocc + a]
+        r.read_f64_range(in.deri, (p * nmo + q) * nmo * nmo, nocc * nmo, run.data(), "/eri_mo");
+        for (uint64_t i = 0; i < nocc; ++i) std::memcpy(row + i * nvir, run.data() + i * nmo + nocc, nvir * sizeof(double));
+    };
+    for (uint64_t j = 0; j < nocc; ++j)
+        for (uint64_t b = 0; b < nvir; ++b) cut(j, nocc + b, vph + (j * nvir + b) * n);
+    for (int64_t t = 0; t < nstates; ++t)
+        for (uint64_t k = 0; k < nmo; ++k)
+            cut(static_cast<uint64_t>(states[t]), k, panel + (static_cast<uint64_t>(t) * nmo + k) * n);
+    for (uint64_t p = 0; p < nmo; ++p)
+        for (uint64_t i = 0; i < nocc; ++i)
+            r.read_f64_range(in.deri, ((p * nmo + i) * nmo + p) * nmo + i, 1, xdiag + p * nocc + i, "/eri_mo");
+    for (uint64_t p = 0; p < nmo; ++p) r.read_f64_range(in.dvxc, p * nmo + p, 1, vxc_diag + p, "/vxc_mo");
 }
 
 } // namespace gwb200

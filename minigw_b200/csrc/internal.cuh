@@ -279,5 +279,8 @@ void screened_forms_noalloc(int64_t n, int64_t m, const double* d_v, const doubl
 void transformed_legendre_grid(int64_t n, double* omega, double* weight);
 void read_gw_input_h5(const std::string& path, int64_t* nmo, int64_t* nocc, double* fermi, double* mo, double* eri,
                       double* vxc);
+void read_gw_input_h5_slices(const std::string& path, const int64_t* states, int64_t nstates, int64_t* nmo,
+                             int64_t* nocc, double* fermi, double* mo, double* vph, double* panel, double* xdiag,
+                             double* vxc_diag);
 
 } // namespace gwb200

@@ -91,6 +91,26 @@ def read_gw_input_hdf5(path: str) -> GwInput:
     return GwInput(eri_mo=eri, mo_energy=mo, vxc_mo=vxc, nocc=nocc.value, fermi_energy=fermi.value)
 
 
+def read_gw_input_slices(path: str, states) -> GwSlices:
+    """Read from gw_input.h5 only what the screening path needs for `states` (V_ph, the states'
+    panel rows, the exchange and vxc diagonals, mo_energy), never the nmo^4 ERI tensor
+    (gwb200_read_input_h5_slices; the reference reads the whole tensor, src/hdf5_input.cpp:192-212).
+    The result equals gw_input.slices_from_input(read_gw_input_hdf5(path), states) bit for bit."""
+    st = np.ascontiguousarray(states, dtype=np.int64)
+    nmo, nocc, fermi = C.c_int64(), C.c_int64(), C.c_double()
+    check(lib.gwb200_read_input_h5_slices(path.encode(), None, 0, C.byref(nmo), C.byref(nocc), C.byref(fermi),
+                                          None, None, None, None, None))
+    m, o = nmo.value, nocc.value
+    n = o * (m - o)
+    mo, vph = np.zeros(m), np.zeros((n, n))
+    panel, xdiag, vxc_diag = np.zeros((st.shape[0] * m, n)), np.zeros((m, o)), np.zeros(m)
+    check(lib.gwb200_read_input_h5_slices(path.encode(), st.ctypes.data_as(_ip), st.shape[0], C.byref(nmo),
+                                          C.byref(nocc), C.byref(fermi), dptr(mo), dptr(vph), dptr(panel),
+                                          dptr(xdiag), dptr(vxc_diag)))
+    return GwSlices(mo_energy=mo, nocc=o, fermi_energy=fermi.value, states=st, vph=vph, panel=panel, xdiag=xdiag,
+                    vxc_diag=vxc_diag)
+
+
 def _precision_code(p: str | int) -> int:
     if p in ("fp64", FP64):
         return FP64
