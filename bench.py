@@ -245,8 +245,8 @@ def auto_pairs(wl) -> int:
 
 
 def reference_cpu_baseline(inp, wl, omegas, weights, threads: int, blas_pairs: int, omp_pairs: int) -> dict | None:
-    """The reference's CPU path in both modes (BASELINE plan: OpenMP frequency parallelism with one
-    BLAS thread per OpenMP thread, or threaded BLAS in serial mode), the faster one reported."""
+    """The reference's CPU path in both of its modes (OpenMP frequency parallelism with one BLAS
+    thread per OpenMP thread, or threaded BLAS in serial mode), the faster one reported."""
     blas = cpu_reference_sample(inp, wl, omegas, weights, blas_pairs, threads)
     if blas is None:
         return None
