@@ -41,6 +41,12 @@ def test_slices_reader_errors(tmp_path):
     with pytest.raises(GwB200Error) as e:
         read_gw_input_slices(str(tmp_path / "missing.h5"), [0])
     assert e.value.status == "GWB200_IO_ERROR"
+    # a file cut inside /eri_mo: the ranged reads stop at the end of the file
+    trunc = tmp_path / "trunc.h5"
+    trunc.write_bytes((GOLDEN / "h2o" / "gw_input.h5").read_bytes()[:400_000])
+    with pytest.raises(GwB200Error) as e:
+        read_gw_input_slices(str(trunc), [4])
+    assert e.value.status == "GWB200_IO_ERROR"
     # some but not all output arrays: refused before anything is read
     nmo, nocc, fermi = C.c_int64(), C.c_int64(), C.c_double()
     mo = np.zeros(18)
