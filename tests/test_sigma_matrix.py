@@ -70,6 +70,42 @@ def test_oracle_matrix_against_numpy_restatement(oracle_lib):
     assert np.abs(mat - ref).max() <= 1e-12 * np.abs(ref).max()
 
 
+def test_cross_forms_are_dot_products_of_the_solved_rows(oracle_lib):
+    """The identity the device path rests on: with eps = I + D^1/2 V D^1/2 = L L^T (D = -Pi0),
+    x_s^T W_c x_t = -(L^-1 D^1/2 x_s) . (L^-1 D^1/2 x_t) for the reference's W_c
+    (src/workspace/screening_workspace.cpp:21-66), so one factorisation and its solved rows give
+    every cross form; checked against the oracle's W_c at three frequencies."""
+    import ctypes as C
+
+    from minigw_b200.synthetic import make_input
+
+    def dp(a):
+        return a.ctypes.data_as(C.POINTER(C.c_double))
+
+    nmo, nocc = 20, 6
+    inp = make_input(nmo, nocc, seed=4)
+    eri = np.ascontiguousarray(inp.eri_mo)
+    _, _, delta = oracle_lib.ph_map(nmo, nocc, inp.mo_energy)
+    v = oracle_lib.vph(inp)
+    n = v.shape[0]
+    xs = np.zeros((2, n, nmo))
+    for s, p in enumerate((5, 8)):
+        oracle_lib.lib.gwo_panel(nmo, nocc, dp(eri), p, 0, nmo, dp(xs[s]))
+    for omega in (0.1, 1.0, 10.0):
+        pi0 = np.zeros(n, dtype=np.complex128)
+        oracle_lib.lib.gwo_pi0(0.0, omega, n, dp(delta), 0.0, dp(pi0))
+        wc = np.zeros((n, n), dtype=np.complex128)
+        assert oracle_lib.lib.gwo_w_c(n, dp(v), dp(pi0), dp(wc)) == 0
+        q_ref = np.einsum("ik,ij,jk->k", xs[0], wc, xs[1])
+        dh = np.sqrt(-pi0.real)
+        chol = np.linalg.cholesky(np.eye(n) + dh[:, None] * v * dh[None, :])
+        w0 = np.linalg.solve(chol, dh[:, None] * xs[0])
+        w1 = np.linalg.solve(chol, dh[:, None] * xs[1])
+        q = -np.sum(w0 * w1, axis=0)
+        assert np.abs(q_ref.imag).max() <= 1e-14 * np.abs(q_ref).max()
+        np.testing.assert_allclose(q, q_ref.real, rtol=1e-11, atol=1e-14 * np.abs(q_ref).max())
+
+
 def _check_against_oracle(be, oracle_lib, inp, nfreq, states):
     om, w = _grid(oracle_lib, nfreq)
     be.load_system(inp)
